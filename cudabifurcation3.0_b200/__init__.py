@@ -1,0 +1,423 @@
+"""B200 bifurcation engine -- Python host mirror of the C-ABI in include/cbf.h.
+
+The product is ``libcbf.so`` (CUDA kernels for sm_100a + the C-ABI + the C++
+drop-in facade with the reference's hostLibrary signatures).  This module only
+binds it with ctypes for Python callers, tests and the benchmark: every compute
+call runs on the GPU through that library.  There is no CPU fallback; if the
+library or a GPU is missing the calls raise.
+
+The function names and argument lists mirror the reference's host entry points
+(Library/hostLibrary.cuh): ``bifurcation1D``, ``bifurcation1DIC``,
+``bifurcation2DKDE``, ``bifurcation2DKDEIC``, ``bifurcation2DDBSCAN``,
+``bifurcation2DDBSCANIC``, ``LLE1D``, ``LLE1DIC``, ``LLE2D``, ``LLE2DIC``, with a
+``system=`` keyword (the reference compiles one ODE per build) and the results
+returned as numpy arrays instead of written to a CSV file.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "libcbf.so"
+
+SYS_MEMRISTIVE5, SYS_ROSSLER, SYS_LORENZ, SYS_CHEN = 0, 1, 2, 3
+SYSTEMS = {"memristive5": 0, "rossler": 1, "lorenz": 2, "chen": 3}
+TASK_PEAKS, TASK_KDE, TASK_DBSCAN, TASK_LLE, TASK_TRAJECTORY = 0, 1, 2, 3, 4
+FLAG_EXACT_GRID, FLAG_KDE_FIXED = 1, 2
+STATUS = {0: "ok", 1: "invalid argument", 2: "unknown system", 3: "CUDA error",
+          4: "out of device memory", 5: "no CUDA device", 6: "I/O error",
+          7: "device wait timed out", 8: "internal consistency check failed"}
+
+# Every symbol include/cbf.h declares (checked by the CPU test suite).
+EXPORTS = [
+    "cbf_abi_version", "cbf_status_string", "cbf_last_error", "cbf_kernel_launches",
+    "cbf_device_count", "cbf_set_device", "cbf_job_init", "cbf_record_length",
+    "cbf_peak_capacity", "cbf_job_points", "cbf_validate", "cbf_run",
+    "cbf_bifurcation1d", "cbf_bifurcation1d_ic", "cbf_bifurcation2d_kde",
+    "cbf_bifurcation2d_kde_ic", "cbf_bifurcation2d_dbscan", "cbf_bifurcation2d_dbscan_ic",
+    "cbf_lle1d", "cbf_lle1d_ic", "cbf_lle2d", "cbf_lle2d_ic", "cbf_run_host",
+    "cbf_grid_coordinates", "cbf_probe_fp64_peak", "cbf_probe_expf_zero",
+    "cbf_divergence_threshold", "cbf_csv_write_map", "cbf_csv_write_peaks", "cbf_csv_write_pairs",
+]
+
+
+class CbfError(RuntimeError):
+    def __init__(self, status: int, detail: str):
+        super().__init__(f"{STATUS.get(status, status)}: {detail}")
+        self.status = status
+        self.detail = detail
+
+
+class Job(C.Structure):
+    """Mirror of ``cbf_job`` (include/cbf.h)."""
+    _fields_ = [
+        ("ranges", C.c_double * 4),
+        ("ic", C.c_double * 8),
+        ("values", C.c_double * 16),
+        ("h", C.c_double),
+        ("tMax", C.c_double),
+        ("transientTime", C.c_double),
+        ("maxValue", C.c_double),
+        ("NT", C.c_double),
+        ("lleEps", C.c_double),
+        ("kdeI1", C.c_double),
+        ("kdeI2", C.c_double),
+        ("kdeH", C.c_double),
+        ("dbscanEps", C.c_double),
+        ("seedChunk", C.c_int64),
+        ("firstPoint", C.c_int64),
+        ("nPoints", C.c_int64),
+        ("task", C.c_int32),
+        ("system", C.c_int32),
+        ("sweepIC", C.c_int32),
+        ("dims", C.c_int32),
+        ("nPts", C.c_int32),
+        ("nIC", C.c_int32),
+        ("nV", C.c_int32),
+        ("idxMut", C.c_int32 * 2),
+        ("writableVar", C.c_int32),
+        ("preScaller", C.c_int32),
+        ("maxAmountOfPeaks", C.c_int32),
+        ("kdeSampling", C.c_int32),
+        ("flags", C.c_uint32),
+        ("peakCapacity", C.c_int32),
+    ]
+
+
+_lib = None
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+
+
+def lib():
+    """Load libcbf.so (build it first: ``python cudabifurcation3.0_b200/build.py``)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: build the CUDA library first")
+        L = C.CDLL(str(LIB_PATH))
+        L.cbf_abi_version.restype = C.c_int32
+        L.cbf_status_string.restype = C.c_char_p
+        L.cbf_status_string.argtypes = [C.c_int32]
+        L.cbf_last_error.restype = C.c_char_p
+        L.cbf_kernel_launches.restype = C.c_uint64
+        L.cbf_device_count.argtypes = [_ip]
+        L.cbf_set_device.argtypes = [C.c_int32]
+        L.cbf_job_init.restype = None
+        L.cbf_job_init.argtypes = [C.POINTER(Job)]
+        for f in ("cbf_record_length", "cbf_peak_capacity"):
+            getattr(L, f).restype = C.c_int32
+            getattr(L, f).argtypes = [C.POINTER(Job)]
+        L.cbf_job_points.restype = C.c_int64
+        L.cbf_job_points.argtypes = [C.POINTER(Job)]
+        L.cbf_validate.argtypes = [C.POINTER(Job)]
+        L.cbf_run.argtypes = [C.POINTER(Job), C.c_void_p, C.c_void_p, C.c_void_p]
+        L.cbf_run_host.argtypes = [C.POINTER(Job), C.c_void_p, C.c_void_p]
+        L.cbf_grid_coordinates.argtypes = [C.POINTER(Job), _dp]
+        L.cbf_probe_fp64_peak.argtypes = [C.c_double, _dp]
+        L.cbf_probe_expf_zero.argtypes = [C.c_float, C.POINTER(C.c_uint64)]
+        L.cbf_divergence_threshold.argtypes = [C.c_double, _ip, _dp]
+        bif1d = [C.c_int32, C.c_double, C.c_int32, C.c_double, C.c_int32, _dp, _dp, _ip,
+                 C.c_int32, C.c_double, C.c_double, _dp, C.c_int32, C.c_int32, _dp, C.c_int32, _ip]
+        L.cbf_bifurcation1d.argtypes = bif1d
+        L.cbf_bifurcation1d_ic.argtypes = bif1d
+        kde = [C.c_int32, C.c_double, C.c_int32, C.c_double, C.c_int32, _dp, _dp, _ip, C.c_int32,
+               C.c_double, C.c_int32, C.c_double, _dp, C.c_int32, C.c_int32, C.c_int32, C.c_double,
+               C.c_double, C.c_double, _ip]
+        L.cbf_bifurcation2d_kde.argtypes = kde
+        L.cbf_bifurcation2d_kde_ic.argtypes = kde
+        db = [C.c_int32, C.c_double, C.c_int32, C.c_double, C.c_int32, _dp, _dp, _ip, C.c_int32,
+              C.c_double, C.c_int32, C.c_double, _dp, C.c_int32, C.c_int32, C.c_double, _ip]
+        L.cbf_bifurcation2d_dbscan.argtypes = db
+        L.cbf_bifurcation2d_dbscan_ic.argtypes = db
+        lle = [C.c_int32, C.c_double, C.c_double, C.c_int32, C.c_double, C.c_double, _dp, C.c_int32,
+               _dp, _ip, C.c_int32, C.c_double, C.c_double, _dp, C.c_int32, C.c_int64, _dp]
+        for f in ("cbf_lle1d", "cbf_lle1d_ic", "cbf_lle2d", "cbf_lle2d_ic"):
+            getattr(L, f).argtypes = lle
+        for f in ("cbf_device_count", "cbf_set_device", "cbf_validate", "cbf_run", "cbf_run_host",
+                  "cbf_grid_coordinates", "cbf_probe_fp64_peak", "cbf_probe_expf_zero",
+                  "cbf_divergence_threshold", "cbf_bifurcation1d", "cbf_bifurcation1d_ic",
+                  "cbf_bifurcation2d_kde", "cbf_bifurcation2d_kde_ic", "cbf_bifurcation2d_dbscan",
+                  "cbf_bifurcation2d_dbscan_ic", "cbf_lle1d", "cbf_lle1d_ic", "cbf_lle2d",
+                  "cbf_lle2d_ic"):
+            getattr(L, f).restype = C.c_int32
+        L.cbf_csv_write_map.restype = C.c_int32
+        L.cbf_csv_write_map.argtypes = [C.c_char_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int32,
+                                        C.c_void_p, C.c_int32]
+        L.cbf_csv_write_peaks.restype = C.c_int32
+        L.cbf_csv_write_peaks.argtypes = [C.c_char_p, C.c_int32, C.c_void_p, C.c_int64, C.c_int64,
+                                          C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]
+        L.cbf_csv_write_pairs.restype = C.c_int32
+        L.cbf_csv_write_pairs.argtypes = [C.c_char_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64,
+                                          C.c_int32]
+        L.cbf_facade_set_system.argtypes = [C.c_int32]
+        L.cbf_facade_set_output_path.argtypes = [C.c_char_p]
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != 0:
+        raise CbfError(status, lib().cbf_last_error().decode(errors="replace"))
+
+
+def _sys(system) -> int:
+    return SYSTEMS[system] if isinstance(system, str) else int(system)
+
+
+def _d(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a, a.ctypes.data_as(_dp)
+
+
+def _i(a):
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    return a, a.ctypes.data_as(_ip)
+
+
+def make_job(*, task, system, nPts, ranges, idxMut, ic, values, h, tMax=0.0, transientTime=0.0,
+             maxValue=0.0, writableVar=0, preScaller=1, sweepIC=False, maxAmountOfPeaks=0,
+             kdeSampling=0, kdeI1=0.0, kdeI2=0.0, kdeH=0.0, dbscanEps=0.0, NT=0.0, lleEps=0.0,
+             seedChunk=0, firstPoint=0, nPoints=0, flags=0, peakCapacity=0) -> Job:
+    j = Job()
+    lib().cbf_job_init(C.byref(j))
+    dims = len(idxMut)
+    j.task, j.system, j.sweepIC, j.dims, j.nPts = task, _sys(system), int(bool(sweepIC)), dims, nPts
+    for i, r in enumerate(list(ranges)[: 2 * dims]):
+        j.ranges[i] = r
+    for i, m in enumerate(idxMut):
+        j.idxMut[i] = m
+    j.nIC = len(ic)
+    for i, v in enumerate(ic):
+        j.ic[i] = v
+    j.nV = len(values)
+    for i, v in enumerate(values):
+        j.values[i] = v
+    j.h, j.tMax, j.transientTime, j.maxValue = h, tMax, transientTime, maxValue
+    j.writableVar, j.preScaller = writableVar, preScaller
+    j.maxAmountOfPeaks, j.kdeSampling = maxAmountOfPeaks, kdeSampling
+    j.kdeI1, j.kdeI2, j.kdeH, j.dbscanEps = kdeI1, kdeI2, kdeH, dbscanEps
+    j.NT, j.lleEps, j.seedChunk = NT, lleEps, seedChunk
+    j.firstPoint, j.nPoints, j.flags, j.peakCapacity = firstPoint, nPoints, flags, peakCapacity
+    return j
+
+
+def run_host(job: Job):
+    """Run a job through the C-ABI with host buffers; returns (out, aux)."""
+    L = lib()
+    check(L.cbf_validate(C.byref(job)))
+    n = L.cbf_job_points(C.byref(job))
+    aux = None
+    if job.task == TASK_LLE:
+        out = np.zeros(n, np.float64)
+    elif job.task in (TASK_KDE, TASK_DBSCAN):
+        out = np.zeros(n, np.int32)
+    else:
+        if job.task == TASK_PEAKS:
+            cap = job.peakCapacity or L.cbf_peak_capacity(C.byref(job))
+        else:
+            cap = job.peakCapacity or L.cbf_record_length(C.byref(job))
+        job.peakCapacity = cap
+        out = np.zeros((n, cap), np.float64)
+        aux = np.zeros(n, np.int32)
+    check(L.cbf_run_host(C.byref(job), out.ctypes.data_as(C.c_void_p),
+                         None if aux is None else aux.ctypes.data_as(C.c_void_p)))
+    return out, aux
+
+
+def run_device(job: Job, d_out: int, d_aux: int = 0, stream: int = 0) -> None:
+    """Run a job on device buffers (raw pointers, e.g. torch tensor.data_ptr())."""
+    check(lib().cbf_run(C.byref(job), C.c_void_p(d_out), C.c_void_p(d_aux or None),
+                        C.c_void_p(stream or None)))
+
+
+def kernel_launches() -> int:
+    return int(lib().cbf_kernel_launches())
+
+
+def grid_coordinates(job: Job) -> np.ndarray:
+    n = lib().cbf_job_points(C.byref(job))
+    out = np.zeros((n, 2), np.float64)
+    check(lib().cbf_grid_coordinates(C.byref(job), out.ctypes.data_as(_dp)))
+    return out
+
+
+def probe_fp64_peak(ms: float = 200.0) -> float:
+    t = C.c_double(0.0)
+    check(lib().cbf_probe_fp64_peak(ms, C.byref(t)))
+    return t.value
+
+
+def probe_expf_zero(threshold: float) -> int:
+    c = C.c_uint64(0)
+    check(lib().cbf_probe_expf_zero(threshold, C.byref(c)))
+    return int(c.value)
+
+
+def divergence_threshold(max_value: float):
+    a = C.c_int32(0)
+    t = C.c_double(0.0)
+    check(lib().cbf_divergence_threshold(max_value, C.byref(a), C.byref(t)))
+    return bool(a.value), t.value
+
+
+def record_length(job: Job) -> int:
+    return int(lib().cbf_record_length(C.byref(job)))
+
+
+# ---------------------------------------------------------------------------
+# Reference-named entry points (hostLibrary.cuh), results as numpy arrays.
+
+def _bif1d(fn, system, tMax, nPts, h, amountOfInitialConditions, initialConditions, ranges,
+           indicesOfMutVars, writableVar, maxValue, transientTime, values, amountOfValues,
+           preScaller):
+    ic, icp = _d(initialConditions)
+    r, rp = _d(ranges)
+    ix, ixp = _i(indicesOfMutVars)
+    v, vp = _d(values)
+    rec = int(tMax / h / preScaller)
+    cap = max(rec // 2, 1)
+    peaks = np.zeros((nPts, cap), np.float64)
+    counts = np.zeros(nPts, np.int32)
+    check(fn(_sys(system), tMax, nPts, h, amountOfInitialConditions, icp, rp, ixp, writableVar,
+             maxValue, transientTime, vp, amountOfValues, preScaller,
+             peaks.ctypes.data_as(_dp), cap, counts.ctypes.data_as(_ip)))
+    return peaks, counts
+
+
+def bifurcation1D(tMax, nPts, h, amountOfInitialConditions, initialConditions, ranges,
+                  indicesOfMutVars, writableVar, maxValue, transientTime, values, amountOfValues,
+                  preScaller, *, system="memristive5"):
+    """hostLibrary.cuh:29-42.  Returns (peaks[nPts, cap], counts[nPts])."""
+    return _bif1d(lib().cbf_bifurcation1d, system, tMax, nPts, h, amountOfInitialConditions,
+                  initialConditions, ranges, indicesOfMutVars, writableVar, maxValue,
+                  transientTime, values, amountOfValues, preScaller)
+
+
+def bifurcation1DIC(tMax, nPts, h, amountOfInitialConditions, initialConditions, ranges,
+                    indicesOfMutVars, writableVar, maxValue, transientTime, values,
+                    amountOfValues, preScaller, *, system="memristive5"):
+    """hostLibrary.cuh:89-102."""
+    return _bif1d(lib().cbf_bifurcation1d_ic, system, tMax, nPts, h, amountOfInitialConditions,
+                  initialConditions, ranges, indicesOfMutVars, writableVar, maxValue,
+                  transientTime, values, amountOfValues, preScaller)
+
+
+def _kde(fn, system, tMax, nPts, h, nIC, icv, ranges, idx, wv, maxValue, maxPeaks, transient,
+         values, nV, preScaller, kdeSampling, i1, i2, smooth):
+    ic, icp = _d(icv)
+    r, rp = _d(ranges)
+    ix, ixp = _i(idx)
+    v, vp = _d(values)
+    out = np.zeros(nPts * nPts, np.int32)
+    check(fn(_sys(system), tMax, nPts, h, nIC, icp, rp, ixp, wv, maxValue, maxPeaks, transient,
+             vp, nV, preScaller, kdeSampling, i1, i2, smooth, out.ctypes.data_as(_ip)))
+    return out.reshape(nPts, nPts)
+
+
+def bifurcation2DKDE(tMax, nPts, h, amountOfInitialConditions, initialConditions, ranges,
+                     indicesOfMutVars, writableVar, maxValue, maxAmountOfPeaks, transientTime,
+                     values, amountOfValues, preScaller, in_kdeSampling, in_kdeSamplesInterval1,
+                     in_kdeSamplesInterval2, in_kdeSamplesSmooth, *, system="memristive5"):
+    """hostLibrary.cuh:129-147.  Returns the int32 map [row=axis1, col=axis0]."""
+    return _kde(lib().cbf_bifurcation2d_kde, system, tMax, nPts, h, amountOfInitialConditions,
+                initialConditions, ranges, indicesOfMutVars, writableVar, maxValue,
+                maxAmountOfPeaks, transientTime, values, amountOfValues, preScaller,
+                in_kdeSampling, in_kdeSamplesInterval1, in_kdeSamplesInterval2,
+                in_kdeSamplesSmooth)
+
+
+def bifurcation2DKDEIC(tMax, nPts, h, amountOfInitialConditions, initialConditions, ranges,
+                       indicesOfMutVars, writableVar, maxValue, maxAmountOfPeaks, transientTime,
+                       values, amountOfValues, preScaller, in_kdeSampling, in_kdeSamplesInterval1,
+                       in_kdeSamplesInterval2, in_kdeSamplesSmooth, *, system="memristive5"):
+    """hostLibrary.cuh:254-272."""
+    return _kde(lib().cbf_bifurcation2d_kde_ic, system, tMax, nPts, h, amountOfInitialConditions,
+                initialConditions, ranges, indicesOfMutVars, writableVar, maxValue,
+                maxAmountOfPeaks, transientTime, values, amountOfValues, preScaller,
+                in_kdeSampling, in_kdeSamplesInterval1, in_kdeSamplesInterval2,
+                in_kdeSamplesSmooth)
+
+
+def _db(fn, system, tMax, nPts, h, nIC, icv, ranges, idx, wv, maxValue, maxPeaks, transient,
+        values, nV, preScaller, eps):
+    ic, icp = _d(icv)
+    r, rp = _d(ranges)
+    ix, ixp = _i(idx)
+    v, vp = _d(values)
+    out = np.zeros(nPts * nPts, np.int32)
+    check(fn(_sys(system), tMax, nPts, h, nIC, icp, rp, ixp, wv, maxValue, maxPeaks, transient,
+             vp, nV, preScaller, eps, out.ctypes.data_as(_ip)))
+    return out.reshape(nPts, nPts)
+
+
+def bifurcation2DDBSCAN(tMax, nPts, h, amountOfInitialConditions, initialConditions, ranges,
+                        indicesOfMutVars, writableVar, maxValue, maxAmountOfPeaks, transientTime,
+                        values, amountOfValues, preScaller, eps, *, system="memristive5"):
+    """hostLibrary.cuh:171-186."""
+    return _db(lib().cbf_bifurcation2d_dbscan, system, tMax, nPts, h, amountOfInitialConditions,
+               initialConditions, ranges, indicesOfMutVars, writableVar, maxValue,
+               maxAmountOfPeaks, transientTime, values, amountOfValues, preScaller, eps)
+
+
+def bifurcation2DDBSCANIC(tMax, nPts, h, amountOfInitialConditions, initialConditions, ranges,
+                          indicesOfMutVars, writableVar, maxValue, maxAmountOfPeaks,
+                          transientTime, values, amountOfValues, preScaller, eps, *,
+                          system="memristive5"):
+    """hostLibrary.cuh:296-311."""
+    return _db(lib().cbf_bifurcation2d_dbscan_ic, system, tMax, nPts, h,
+               amountOfInitialConditions, initialConditions, ranges, indicesOfMutVars,
+               writableVar, maxValue, maxAmountOfPeaks, transientTime, values, amountOfValues,
+               preScaller, eps)
+
+
+def _lle(fn, dims, system, tMax, NT, nPts, h, eps, icv, nIC, ranges, idx, wv, maxValue,
+         transient, values, nV, seedChunk):
+    ic, icp = _d(icv)
+    r, rp = _d(ranges)
+    ix, ixp = _i(idx)
+    v, vp = _d(values)
+    n = nPts ** dims
+    out = np.zeros(n, np.float64)
+    check(fn(_sys(system), tMax, NT, nPts, h, eps, icp, nIC, rp, ixp, wv, maxValue, transient, vp,
+             nV, seedChunk, out.ctypes.data_as(_dp)))
+    return out.reshape((nPts, nPts) if dims == 2 else (nPts,))
+
+
+def LLE1D(tMax, NT, nPts, h, eps, initialConditions, amountOfInitialConditions, ranges,
+          indicesOfMutVars, writableVar, maxValue, transientTime, values, amountOfValues, *,
+          system="memristive5", seedChunk=0):
+    """hostLibrary.cuh:334-348."""
+    return _lle(lib().cbf_lle1d, 1, system, tMax, NT, nPts, h, eps, initialConditions,
+                amountOfInitialConditions, ranges, indicesOfMutVars, writableVar, maxValue,
+                transientTime, values, amountOfValues, seedChunk)
+
+
+def LLE1DIC(tMax, NT, nPts, h, eps, initialConditions, amountOfInitialConditions, ranges,
+            indicesOfMutVars, writableVar, maxValue, transientTime, values, amountOfValues, *,
+            system="memristive5", seedChunk=0):
+    """hostLibrary.cuh:371-385."""
+    return _lle(lib().cbf_lle1d_ic, 1, system, tMax, NT, nPts, h, eps, initialConditions,
+                amountOfInitialConditions, ranges, indicesOfMutVars, writableVar, maxValue,
+                transientTime, values, amountOfValues, seedChunk)
+
+
+def LLE2D(tMax, NT, nPts, h, eps, initialConditions, amountOfInitialConditions, ranges,
+          indicesOfMutVars, writableVar, maxValue, transientTime, values, amountOfValues, *,
+          system="memristive5", seedChunk=200000):
+    """hostLibrary.cuh:408-422 (seedChunk 200000: the reference's fixed chunk, :1552)."""
+    return _lle(lib().cbf_lle2d, 2, system, tMax, NT, nPts, h, eps, initialConditions,
+                amountOfInitialConditions, ranges, indicesOfMutVars, writableVar, maxValue,
+                transientTime, values, amountOfValues, seedChunk)
+
+
+def LLE2DIC(tMax, NT, nPts, h, eps, initialConditions, amountOfInitialConditions, ranges,
+            indicesOfMutVars, writableVar, maxValue, transientTime, values, amountOfValues, *,
+            system="memristive5", seedChunk=0):
+    """hostLibrary.cuh:445-459."""
+    return _lle(lib().cbf_lle2d_ic, 2, system, tMax, NT, nPts, h, eps, initialConditions,
+                amountOfInitialConditions, ranges, indicesOfMutVars, writableVar, maxValue,
+                transientTime, values, amountOfValues, seedChunk)

@@ -1,0 +1,117 @@
+// Internal definitions shared by the kernels and the C-ABI layer.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/cbf.h"
+#include "systems.cuh"
+
+namespace cbf {
+
+constexpr double kPeakIntervalUnit = 0.01;  // peakFinder's default h (cudaLibrary.cuh:204)
+
+// A validated job in the form the kernels consume (passed by value).
+struct DevJob {
+    double ranges[4];
+    double ic[CBF_MAX_DIM];
+    double values[CBF_MAX_VALUES];
+    double h;
+    double maxValue;
+    double divThresh;   // |x| >= divThresh  <=>  fabsf((float)x) > maxValue
+    double lleEps;
+    double tMax;
+    double kdeI1, kdeI2, kdeH;
+    double kdeSkip;     // terms with |peak - delta| > kdeSkip are exactly 0 (see kde epilogue)
+    double dbEps;
+    double dbSkip;      // pairs with |dx| or |dy| >= dbSkip are never neighbours
+    long long firstPoint;
+    long long nPoints;
+    long long seedChunk;
+    int nPts, dims, nIC, nV;
+    int idxMut0, idxMut1;
+    int writableVar, preScaller;
+    int nSkip;          // transient steps: (int)(transientTime / h)
+    int nRecord;        // recorded samples (int)(tMax/h/preScaller); LLE: (int)(tMax/NT)
+    int nNT;            // LLE steps per renormalisation (int)(size_t)(NT/h)
+    int checkDiv;       // maxValue != 0 and can ever fire
+    unsigned divHi;     // high word of divThresh (conservative fast check)
+    int exactGrid;
+    int maxPeaks;
+    int kdeSampling;
+    int kdeFixed;
+    int peakCap;        // peaks stored per point
+    int task;
+    int system;
+    int sweepIC;
+};
+
+// getValueByIdx (cudaLibrary.cu:210-216): `(int)idx / powf(nPts, v)` is a float
+// division, so above 2^24 the index is rounded; exactGrid uses integer math.
+__device__ __forceinline__ double grid_value(long long g, int nPts, double start, double finish,
+                                             int axis, bool exact)
+{
+    int cell;
+    if (!exact) {
+        float p = powf((float)nPts, (float)axis);
+        float q = (float)(int)g / p;
+        cell = ((int)q) % nPts;
+    } else {
+        long long d = (axis == 0) ? 1 : (long long)nPts;
+        cell = (int)((g / d) % nPts);
+    }
+    return start + (double)cell * ((double)(finish - start) / (double)(nPts - 1));
+}
+
+// Set up one point: ICs and values copied, swept entries overwritten
+// (cudaLibrary.cu:96-105; IC variant :183-192).  Fully unrolled so that the
+// arrays stay in registers even though the swept indices are runtime values.
+template <int DIM>
+__device__ __forceinline__ void setup_point(const DevJob& J, long long g, double (&x)[DIM],
+                                            double (&v)[CBF_MAX_VALUES])
+{
+    const bool exact = J.exactGrid != 0;
+    const double p0 = grid_value(g, J.nPts, J.ranges[0], J.ranges[1], 0, exact);
+    const double p1 = (J.dims > 1) ? grid_value(g, J.nPts, J.ranges[2], J.ranges[3], 1, exact) : 0.0;
+    const int m0 = J.idxMut0;
+    const int m1 = (J.dims > 1) ? J.idxMut1 : -1;
+#pragma unroll
+    for (int i = 0; i < DIM; ++i) {
+        double t = J.ic[i];
+        if (J.sweepIC) {
+            if (i == m0) t = p0;
+            if (i == m1) t = p1;
+        }
+        x[i] = t;
+    }
+#pragma unroll
+    for (int i = 0; i < CBF_MAX_VALUES; ++i) {
+        double t = J.values[i];
+        if (!J.sweepIC) {
+            if (i == m0) t = p0;
+            if (i == m1) t = p1;
+        }
+        v[i] = t;
+    }
+}
+
+__device__ __forceinline__ unsigned abs_hi(double v)
+{
+    return (unsigned)(__double_as_longlong(v) >> 32) & 0x7fffffffu;
+}
+
+// Exact divergence test of loopCalculateDiscreteModel (cudaLibrary.cu:69-71).
+__device__ __forceinline__ bool diverged(double v, double thresh)
+{
+    return fabs(v) >= thresh;
+}
+
+// Kernel launch bookkeeping (defined in capi.cu).
+void note_launch(unsigned n = 1);
+
+// Launchers (defined in lle.cu / bif.cu / probes.cu).  All return a CUDA error.
+cudaError_t launch_lle(const DevJob& J, double* d_out, cudaStream_t s);
+cudaError_t launch_bif(const DevJob& J, void* d_out, int* d_aux, cudaStream_t s);
+cudaError_t launch_grid_coords(const DevJob& J, double* d_out, cudaStream_t s);
+
+}  // namespace cbf

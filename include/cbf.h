@@ -1,0 +1,238 @@
+/*
+ * cbf.h -- C-ABI launch layer of the B200 bifurcation engine.
+ *
+ * Plain C types only (pointers, sizes, scalars).  Every function returns a
+ * cbf_status and never exits the process; cbf_last_error() gives the detail of
+ * the last failure on the calling thread.
+ *
+ * The reference library (CUDABifurcation3.0) exposes its hot path as C++
+ * __host__ functions in Library/hostLibrary.cuh that write a CSV file.  Each
+ * host-buffer entry point below replaces one of them: same argument meaning and
+ * order (plus a leading `system` id, because the reference hard-codes one ODE
+ * per build in Library/cudaLibrary.cu:2-44), results returned in caller buffers
+ * instead of a file.  The C++ drop-in facade with the reference's exact
+ * signatures and CSV output lives in hostLibrary.h and calls these functions.
+ *
+ * Semantics follow the reference exactly, including its documented quirks:
+ *   - grid value of point g on axis v: getValueByIdx (cudaLibrary.cu:210-216),
+ *     FP32 index division included (set CBF_FLAG_EXACT_GRID to opt out);
+ *   - peaks: first peak dropped, intervals in units of 0.01 (cudaLibrary.cu:220-284);
+ *   - KDE mode count (cudaLibrary.cu:356-441), DBSCAN cluster count
+ *     (cudaLibrary.cu:457-624), Benettin LLE (cudaLibrary.cu:666-908).
+ */
+#ifndef CBF_H
+#define CBF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CBF_ABI_VERSION 1
+
+typedef int32_t cbf_status;
+#define CBF_OK 0
+#define CBF_ERR_INVALID_ARG 1   /* bad size, index, range, unknown task */
+#define CBF_ERR_UNKNOWN_SYSTEM 2
+#define CBF_ERR_CUDA 3          /* a CUDA runtime call failed (detail in cbf_last_error) */
+#define CBF_ERR_OUT_OF_MEMORY 4
+#define CBF_ERR_NO_DEVICE 5
+#define CBF_ERR_IO 6            /* façade: output file could not be written */
+#define CBF_ERR_TIMEOUT 7       /* a bounded device-side wait gave up */
+#define CBF_ERR_INTERNAL 8      /* a device-side consistency check failed */
+
+/* ODE systems (the reference's calculateDiscreteModel is one per build). */
+#define CBF_SYS_MEMRISTIVE5 0   /* the 5-D model of cudaLibrary.cu:2-44, values[0..7] */
+#define CBF_SYS_ROSSLER 1       /* values = {s, a, b, c} */
+#define CBF_SYS_LORENZ 2        /* values = {s, sigma, rho, beta} */
+#define CBF_SYS_CHEN 3          /* values = {s, a, b, c} */
+#define CBF_NUM_SYSTEMS 4
+
+/* Tasks of the generic job interface. */
+#define CBF_TASK_PEAKS 0        /* 1-D diagram: all peaks per point (+counts) */
+#define CBF_TASK_KDE 1          /* KDE mode count per point (int32) */
+#define CBF_TASK_DBSCAN 2       /* DBSCAN cluster count per point (int32) */
+#define CBF_TASK_LLE 3          /* largest Lyapunov exponent per point (double) */
+#define CBF_TASK_TRAJECTORY 4   /* recorded x[writableVar] samples per point (+diverged flags) */
+
+/* Job flags. */
+#define CBF_FLAG_EXACT_GRID 1u  /* integer grid index instead of the FP32 quirk */
+#define CBF_FLAG_KDE_FIXED 2u   /* KDE with kdeSampling samples in total, not per peak */
+
+#define CBF_MAX_DIM 8
+#define CBF_MAX_VALUES 16
+
+/* One map computation.  Field meaning follows hostLibrary.cuh:29-459. */
+typedef struct cbf_job {
+    double ranges[4];               /* {start0, end0, start1, end1} */
+    double ic[CBF_MAX_DIM];         /* initial conditions */
+    double values[CBF_MAX_VALUES];  /* system parameters */
+    double h;                       /* integration step */
+    double tMax;                    /* record length (time units) */
+    double transientTime;
+    double maxValue;                /* divergence bound on |x[writableVar]|, 0 disables */
+    double NT;                      /* LLE: renormalisation interval */
+    double lleEps;                  /* LLE: initial offset */
+    double kdeI1, kdeI2, kdeH;      /* KDE sample interval and bandwidth */
+    double dbscanEps;
+    int64_t seedChunk;              /* LLE seed index = g mod seedChunk (0: g) */
+    int64_t firstPoint;             /* first linear grid index of this job */
+    int64_t nPoints;                /* points to compute (0: the whole grid) */
+    int32_t task;                   /* CBF_TASK_* */
+    int32_t system;                 /* CBF_SYS_* */
+    int32_t sweepIC;                /* 0: sweep values[], 1: sweep initial conditions */
+    int32_t dims;                   /* swept axes: 1 or 2 */
+    int32_t nPts;                   /* points per axis */
+    int32_t nIC;
+    int32_t nV;
+    int32_t idxMut[2];              /* swept entries of values[] (or ic[]) */
+    int32_t writableVar;            /* recorded / checked state variable */
+    int32_t preScaller;             /* steps per recorded sample */
+    int32_t maxAmountOfPeaks;
+    int32_t kdeSampling;
+    uint32_t flags;                 /* CBF_FLAG_* */
+    int32_t peakCapacity;           /* PEAKS/TRAJECTORY: row stride of d_out (0: derived) */
+} cbf_job;
+
+/* ---- library ---------------------------------------------------------- */
+int32_t cbf_abi_version(void);
+const char* cbf_status_string(cbf_status status);
+const char* cbf_last_error(void);
+/* Number of kernel launches issued by this library since load. */
+uint64_t cbf_kernel_launches(void);
+cbf_status cbf_device_count(int32_t* count);
+cbf_status cbf_set_device(int32_t device);
+/* Fill a job with the reference's defaults (s = 0.5 convention, preScaller 1). */
+void cbf_job_init(cbf_job* job);
+/* Derived sizes with the reference's int truncations (hostLibrary.cu:22-23,1286-1288). */
+int32_t cbf_record_length(const cbf_job* job);   /* (int)(tMax/h/preScaller) or LLE (int)(tMax/NT) */
+int32_t cbf_peak_capacity(const cbf_job* job);   /* peaks a PEAKS row can hold = record/2 */
+int64_t cbf_job_points(const cbf_job* job);      /* nPoints, or nPts^dims when 0 */
+cbf_status cbf_validate(const cbf_job* job);
+
+/* ---- device-resident interface --------------------------------------- */
+/* Run one job on `stream` (a cudaStream_t, NULL = legacy default stream).
+ * d_out: LLE double[n]; KDE/DBSCAN int32[n]; PEAKS double[n*cap];
+ *        TRAJECTORY double[n*record].
+ * d_aux: PEAKS int32[n] peak counts; TRAJECTORY int32[n] diverged flags; else unused.
+ * Scratch for KDE/DBSCAN is taken from the stream-ordered allocator. */
+cbf_status cbf_run(const cbf_job* job, void* d_out, void* d_aux, void* stream);
+
+/* ---- host-buffer entry points (drop-in for hostLibrary.cuh) ---------- */
+/* bifurcation1D, hostLibrary.cuh:29-42 / hostLibrary.cu:7-158.
+ * outPeaks[k*peakCapacity + j], outCounts[k]; peakCapacity >= record/2. */
+cbf_status cbf_bifurcation1d(int32_t system, double tMax, int32_t nPts, double h,
+                             int32_t amountOfInitialConditions, const double* initialConditions,
+                             const double* ranges, const int32_t* indicesOfMutVars,
+                             int32_t writableVar, double maxValue, double transientTime,
+                             const double* values, int32_t amountOfValues, int32_t preScaller,
+                             double* outPeaks, int32_t peakCapacity, int32_t* outCounts);
+/* bifurcation1DIC, hostLibrary.cuh:89-102 / hostLibrary.cu:243-393 */
+cbf_status cbf_bifurcation1d_ic(int32_t system, double tMax, int32_t nPts, double h,
+                                int32_t amountOfInitialConditions, const double* initialConditions,
+                                const double* ranges, const int32_t* indicesOfMutVars,
+                                int32_t writableVar, double maxValue, double transientTime,
+                                const double* values, int32_t amountOfValues, int32_t preScaller,
+                                double* outPeaks, int32_t peakCapacity, int32_t* outCounts);
+/* bifurcation2DKDE, hostLibrary.cuh:129-147 / hostLibrary.cu:397-567; out int32[nPts*nPts] */
+cbf_status cbf_bifurcation2d_kde(int32_t system, double tMax, int32_t nPts, double h,
+                                 int32_t amountOfInitialConditions, const double* initialConditions,
+                                 const double* ranges, const int32_t* indicesOfMutVars,
+                                 int32_t writableVar, double maxValue, int32_t maxAmountOfPeaks,
+                                 double transientTime, const double* values,
+                                 int32_t amountOfValues, int32_t preScaller, int32_t kdeSampling,
+                                 double kdeSamplesInterval1, double kdeSamplesInterval2,
+                                 double kdeSamplesSmooth, int32_t* out);
+/* bifurcation2DKDEIC, hostLibrary.cuh:254-272 / hostLibrary.cu:929-1090 */
+cbf_status cbf_bifurcation2d_kde_ic(int32_t system, double tMax, int32_t nPts, double h,
+                                    int32_t amountOfInitialConditions,
+                                    const double* initialConditions, const double* ranges,
+                                    const int32_t* indicesOfMutVars, int32_t writableVar,
+                                    double maxValue, int32_t maxAmountOfPeaks,
+                                    double transientTime, const double* values,
+                                    int32_t amountOfValues, int32_t preScaller,
+                                    int32_t kdeSampling, double kdeSamplesInterval1,
+                                    double kdeSamplesInterval2, double kdeSamplesSmooth,
+                                    int32_t* out);
+/* bifurcation2DDBSCAN, hostLibrary.cuh:171-186 / hostLibrary.cu:571-744 */
+cbf_status cbf_bifurcation2d_dbscan(int32_t system, double tMax, int32_t nPts, double h,
+                                    int32_t amountOfInitialConditions,
+                                    const double* initialConditions, const double* ranges,
+                                    const int32_t* indicesOfMutVars, int32_t writableVar,
+                                    double maxValue, int32_t maxAmountOfPeaks,
+                                    double transientTime, const double* values,
+                                    int32_t amountOfValues, int32_t preScaller, double eps,
+                                    int32_t* out);
+/* bifurcation2DDBSCANIC, hostLibrary.cuh:296-311 / hostLibrary.cu:1094-1266 */
+cbf_status cbf_bifurcation2d_dbscan_ic(int32_t system, double tMax, int32_t nPts, double h,
+                                       int32_t amountOfInitialConditions,
+                                       const double* initialConditions, const double* ranges,
+                                       const int32_t* indicesOfMutVars, int32_t writableVar,
+                                       double maxValue, int32_t maxAmountOfPeaks,
+                                       double transientTime, const double* values,
+                                       int32_t amountOfValues, int32_t preScaller, double eps,
+                                       int32_t* out);
+/* LLE1D / LLE1DIC / LLE2D / LLE2DIC, hostLibrary.cuh:334-459 / hostLibrary.cu:1270-1798.
+ * seedChunk reproduces the reference's chunk-local seed index (0: global index);
+ * the C++ facade computes it the way the reference does. out double[nPts^dims]. */
+cbf_status cbf_lle1d(int32_t system, double tMax, double NT, int32_t nPts, double h, double eps,
+                     const double* initialConditions, int32_t amountOfInitialConditions,
+                     const double* ranges, const int32_t* indicesOfMutVars, int32_t writableVar,
+                     double maxValue, double transientTime, const double* values,
+                     int32_t amountOfValues, int64_t seedChunk, double* out);
+cbf_status cbf_lle1d_ic(int32_t system, double tMax, double NT, int32_t nPts, double h,
+                        double eps, const double* initialConditions,
+                        int32_t amountOfInitialConditions, const double* ranges,
+                        const int32_t* indicesOfMutVars, int32_t writableVar, double maxValue,
+                        double transientTime, const double* values, int32_t amountOfValues,
+                        int64_t seedChunk, double* out);
+cbf_status cbf_lle2d(int32_t system, double tMax, double NT, int32_t nPts, double h, double eps,
+                     const double* initialConditions, int32_t amountOfInitialConditions,
+                     const double* ranges, const int32_t* indicesOfMutVars, int32_t writableVar,
+                     double maxValue, double transientTime, const double* values,
+                     int32_t amountOfValues, int64_t seedChunk, double* out);
+cbf_status cbf_lle2d_ic(int32_t system, double tMax, double NT, int32_t nPts, double h,
+                        double eps, const double* initialConditions,
+                        int32_t amountOfInitialConditions, const double* ranges,
+                        const int32_t* indicesOfMutVars, int32_t writableVar, double maxValue,
+                        double transientTime, const double* values, int32_t amountOfValues,
+                        int64_t seedChunk, double* out);
+
+/* Generic host-buffer form of cbf_run: copies results into host memory. */
+cbf_status cbf_run_host(const cbf_job* job, void* out, void* aux);
+
+/* ---- CSV output with the reference's byte layout ---------------------- */
+/* 2-D map (hostLibrary.cu:534-546): values in index order, ", " between values,
+ * "\n" before the first value of each new row of nPts, no final newline.
+ * headerRanges (4 doubles) adds the "r0 r1\nr2 r3\n" header (:476-480); NULL
+ * omits it.  isDouble selects double (%.*g) or int32 (%d) values. */
+cbf_status cbf_csv_write_map(const char* path, const void* values, int32_t isDouble, int64_t n,
+                             int32_t nPts, const double* headerRanges, int32_t precision);
+/* 1-D diagram rows "param, peak\n" at precision 12 (hostLibrary.cu:125-138) for
+ * points [firstPoint, firstPoint+nPoints); append != 0 appends to the file. */
+cbf_status cbf_csv_write_peaks(const char* path, int32_t nPts, const double* ranges,
+                               int64_t firstPoint, int64_t nPoints, const double* peaks,
+                               int32_t peakCapacity, const int32_t* counts, int32_t append);
+/* 1-D LLE rows "param, value\n" (hostLibrary.cu:1368-1378). */
+cbf_status cbf_csv_write_pairs(const char* path, int32_t nPts, const double* ranges,
+                               const double* values, int64_t n, int32_t precision);
+
+/* ---- probes used for measurement and self-checks --------------------- */
+/* Grid coordinates the kernels use for points [first, first+n): out[k*2+axis]. */
+cbf_status cbf_grid_coordinates(const cbf_job* job, double* out_host);
+/* FP64 FMA throughput of this GPU (TFLOP/s, 2 flops per FMA) over ~`ms` ms. */
+cbf_status cbf_probe_fp64_peak(double ms, double* tflops);
+/* Exhaustive device check that expf(x) == 0 for every float x <= threshold;
+ * *count receives the number of floats that violate it. */
+cbf_status cbf_probe_expf_zero(float threshold, uint64_t* count);
+/* The exact form of the reference's divergence test `fabsf(x) > maxValue`
+ * (cudaLibrary.cu:69-71) used by the kernels: fires iff fabs(x) >= *threshold,
+ * and only when *active is nonzero. */
+cbf_status cbf_divergence_threshold(double maxValue, int32_t* active, double* threshold);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CBF_H */

@@ -1,0 +1,583 @@
+/*
+ * CPU oracle -- TEST INFRASTRUCTURE ONLY (see oracle.h for the contract).
+ *
+ * Every function below restates one function of the reference library
+ * (CUDABifurcation3.0) in plain C, keeping the reference's expression order, its
+ * int/float/double conversions and its quirks.  The citation above each function
+ * names the reference lines it follows.  Compiled with -ffp-contract=off.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ------------------------------------------------------------------------- */
+/* Grid index -> parameter value.  cudaLibrary.cu:210-216.
+ * `(int)idx / powf((double)nPts, (double)valueNumber)` is a float division: the
+ * int index is converted to float (exact only below 2^24) and powf takes floats. */
+double orc_get_value_by_idx(int idx, int nPts, double startRange, double finishRange,
+                            int valueNumber)
+{
+    float p = powf((float)nPts, (float)valueNumber);
+    float q = (float)idx / p;
+    int cell = ((int)q) % nPts;
+    return startRange + (double)cell * ((double)(finishRange - startRange) / (double)(nPts - 1));
+}
+
+/* ------------------------------------------------------------------------- */
+/* Model steps.  One fixed-step CD (semi-implicit composition) step: an explicit
+ * half with k = h*s in reverse variable order, then a linearly implicit half with
+ * h1 = h*(1-s) in forward order (the scheme of cudaLibrary.cu:19-43).            */
+
+/* The model shipped in the reference, cudaLibrary.cu:2-44, restated literally.
+ * Quirks kept: `float y[5], k` truncates the explicit-half state snapshot and k to
+ * FP32 (:19-34); abs(x[4]) is the double overload (fabs) on the host build. */
+static void step_memristive5(double* x, const double* a, double h)
+{
+    float y[5], k;
+    k = (float)(h * a[7]);
+
+    x[4] = x[4] + (double)k * (x[0]);
+    x[3] = x[3] + (double)k * (-a[2] * x[1] - a[3] * x[3]);
+    x[2] = x[2] + (double)k * (a[1] * (x[1] - x[0] - x[2]));
+    x[1] = x[1] + (double)k * (-x[2] + x[3]);
+    x[0] = x[0] + (double)k * (a[0] * (x[2] - (a[4] + a[5] + a[6] * fabs(x[4])) * x[0]));
+
+    y[0] = (float)x[0];
+    y[1] = (float)x[1];
+    y[2] = (float)x[2];
+    y[3] = (float)x[3];
+    y[4] = (float)x[4];
+
+    double h1 = h * (1 - a[7]);
+
+    x[0] = ((double)y[0] + h1 * (a[0] * x[2])) / (1 + h1 * a[0] * (a[4] + a[5] + a[6] * fabs(x[4])));
+    x[1] = (double)y[1] + h1 * (-x[2] + x[3]);
+    x[2] = ((double)y[2] + h1 * (a[1] * (x[1] - x[0]))) / (1 + h1 * a[1]);
+    x[3] = ((double)y[3] + h1 * (-a[2] * x[1])) / (1 + h1 * a[3]);
+    x[4] = (double)y[4] + h1 * (x[0]);
+}
+
+/* Rossler x'=-y-z, y'=x+a*y, z'=b+z*(x-c); values = {s, a, b, c}. */
+static void step_rossler(double* X, const double* v, double h)
+{
+    const double s = v[0], a = v[1], b = v[2], c = v[3];
+    const double k = h * s;
+    const double h1 = h * (1.0 - s);
+    const double h1b = h1 * b;
+    const double r2 = 1.0 / (1.0 - h1 * a);
+    double x = X[0], y = X[1], z = X[2];
+    z = fma(k, fma(z, x - c, b), z);
+    y = fma(k, fma(a, y, x), y);
+    x = fma(-k, y + z, x);
+    x = fma(-h1, y + z, x);
+    y = fma(h1, x, y) * r2;
+    z = (z + h1b) / fma(-h1, x - c, 1.0);
+    X[0] = x; X[1] = y; X[2] = z;
+}
+
+/* Lorenz x'=sigma*(y-x), y'=x*(rho-z)-y, z'=x*y-beta*z; values = {s, sigma, rho, beta}. */
+static void step_lorenz(double* X, const double* v, double h)
+{
+    const double s = v[0], sg = v[1], rho = v[2], beta = v[3];
+    const double k = h * s;
+    const double h1 = h * (1.0 - s);
+    const double ks = k * sg;
+    const double h1s = h1 * sg;
+    const double r1 = 1.0 / (1.0 + h1s);
+    const double r2 = 1.0 / (1.0 + h1);
+    const double r3 = 1.0 / (1.0 + h1 * beta);
+    double x = X[0], y = X[1], z = X[2];
+    z = fma(k, fma(-beta, z, x * y), z);
+    y = fma(k, fma(x, rho - z, -y), y);
+    x = fma(ks, y - x, x);
+    x = fma(h1s, y, x) * r1;
+    y = fma(h1, x * (rho - z), y) * r2;
+    z = fma(h1, x * y, z) * r3;
+    X[0] = x; X[1] = y; X[2] = z;
+}
+
+/* Chen x'=a*(y-x), y'=(c-a)*x-x*z+c*y, z'=x*y-b*z; values = {s, a, b, c}. */
+static void step_chen(double* X, const double* v, double h)
+{
+    const double s = v[0], a = v[1], b = v[2], c = v[3];
+    const double k = h * s;
+    const double h1 = h * (1.0 - s);
+    const double cma = c - a;
+    const double ka = k * a;
+    const double h1a = h1 * a;
+    const double r1 = 1.0 / (1.0 + h1a);
+    const double r2 = 1.0 / (1.0 - h1 * c);
+    const double r3 = 1.0 / (1.0 + h1 * b);
+    double x = X[0], y = X[1], z = X[2];
+    z = fma(k, fma(-b, z, x * y), z);
+    y = fma(k, fma(x, cma - z, c * y), y);
+    x = fma(ka, y - x, x);
+    x = fma(h1a, y, x) * r1;
+    y = fma(h1, x * (cma - z), y) * r2;
+    z = fma(h1, x * y, z) * r3;
+    X[0] = x; X[1] = y; X[2] = z;
+}
+
+int orc_system_dim(int system)
+{
+    switch (system) {
+    case ORC_SYS_MEMRISTIVE5: return 5;
+    case ORC_SYS_ROSSLER:
+    case ORC_SYS_LORENZ:
+    case ORC_SYS_CHEN: return 3;
+    default: return -1;
+    }
+}
+
+void orc_model_step(int system, double* x, const double* a, double h)
+{
+    switch (system) {
+    case ORC_SYS_MEMRISTIVE5: step_memristive5(x, a, h); break;
+    case ORC_SYS_ROSSLER: step_rossler(x, a, h); break;
+    case ORC_SYS_LORENZ: step_lorenz(x, a, h); break;
+    case ORC_SYS_CHEN: step_chen(x, a, h); break;
+    default: break;
+    }
+}
+
+/* `if (maxValue != 0) if (fabsf(x[writableVar]) > maxValue)`: fabsf rounds the
+ * double to FP32, the comparison promotes back to double.  cudaLibrary.cu:69-71 */
+int orc_diverged(double v, double maxValue)
+{
+    return (maxValue != 0) && ((double)fabsf((float)v) > maxValue);
+}
+
+/* cudaLibrary.cu:55-74: store x[writableVar] BEFORE stepping, then preScaller
+ * steps, then the divergence check; returns false on the first violation. */
+int orc_loop(int system, double* x, const double* values, double h, int amountOfIterations,
+             int preScaller, int writableVar, double maxValue, double* data,
+             int64_t startDataIndex, int writeStep)
+{
+    for (int i = 0; i < amountOfIterations; ++i) {
+        if (data != NULL)
+            data[startDataIndex + (int64_t)i * writeStep] = x[writableVar];
+        for (int j = 0; j < preScaller - 1; ++j)
+            orc_model_step(system, x, values, h);
+        orc_model_step(system, x, values, h);
+        if (maxValue != 0)
+            if ((double)fabsf((float)x[writableVar]) > maxValue)
+                return 0;
+    }
+    return 1;
+}
+
+/* cudaLibrary.cu:220-266.  Quirks kept: a rising plateau sets i=j+1 and the loop's
+ * ++i skips sample j+1; after the scan the FIRST peak is dropped and intervals are
+ * (t[k+1]-t[k])*h.  Output may alias data (writes never pass the read cursor). */
+int orc_peak_finder(double* data, int64_t startDataIndex, int amountOfPoints,
+                    double* outPeaks, double* timeOfPeaks, double h)
+{
+    int amountOfPeaks = 0;
+    const int64_t s = startDataIndex;
+    for (int64_t i = s + 1; i < s + amountOfPoints - 1; ++i) {
+        if (data[i] > data[i - 1] && data[i] >= data[i + 1]) {
+            for (int64_t j = i; j < s + amountOfPoints - 1; ++j) {
+                if (data[j] < data[j + 1]) {
+                    i = j + 1;
+                    break;
+                }
+                if (data[j] > data[j + 1]) {
+                    if (outPeaks != NULL)
+                        outPeaks[s + amountOfPeaks] = data[j];
+                    if (timeOfPeaks != NULL)
+                        timeOfPeaks[s + amountOfPeaks] = (double)j;
+                    ++amountOfPeaks;
+                    i = j + 1;
+                    break;
+                }
+            }
+        }
+    }
+    if (amountOfPeaks > 1) {
+        for (int64_t i = 0; i < amountOfPeaks - 1; i++) {
+            if (outPeaks != NULL)
+                outPeaks[s + i] = outPeaks[s + i + 1];
+            if (timeOfPeaks != NULL)
+                timeOfPeaks[s + i] = (double)((timeOfPeaks[s + i + 1] - timeOfPeaks[s + i]) * h);
+        }
+        amountOfPeaks = amountOfPeaks - 1;
+    } else {
+        amountOfPeaks = 0;
+    }
+    return amountOfPeaks;
+}
+
+/* cudaLibrary.cu:356-422.  Gaussian KDE evaluated at k1-1 sample positions with
+ * FP32 expf and a double accumulator in peak order; strict local maxima counted
+ * with the `strangePeak` plateau state machine plus a rising tail. */
+int orc_kde(const double* data, int64_t startDataIndex, int amountOfPoints, int maxAmountOfPeaks,
+            int kdeSampling, double kdeSamplesInterval1, double kdeSamplesInterval2,
+            double kdeSmoothH)
+{
+    if (amountOfPoints == 0)
+        return 0;
+    if (amountOfPoints == 1 || amountOfPoints == 2)
+        return 1;
+    if (amountOfPoints > maxAmountOfPeaks)
+        return maxAmountOfPeaks;
+    return orc_kde_k1(data, startDataIndex, amountOfPoints, kdeSampling * amountOfPoints,
+                      kdeSamplesInterval1, kdeSamplesInterval2, kdeSmoothH);
+}
+
+/* The sampling and mode-counting body of kde() (cudaLibrary.cu:367-421) with the
+ * sample count k1 given directly; kde() uses k1 = kdeSampling * amountOfPoints.
+ * A fixed k1 is the library's fixed-sample extension of the same estimator. */
+int orc_kde_k1(const double* data, int64_t startDataIndex, int amountOfPoints, int k1i,
+               double kdeSamplesInterval1, double kdeSamplesInterval2, double kdeSmoothH)
+{
+    double k1 = k1i;
+    double k2 = (kdeSamplesInterval2 - kdeSamplesInterval1) / (k1 - 1);
+    double delt = 0;
+    double prevPrevData2 = 0;
+    double prevData2 = 0;
+    double data2 = 0;
+    int strangePeak = 0;
+    int resultKde = 0;
+
+    for (int w = 0; w < k1 - 1; ++w) {
+        delt = w * k2 + kdeSamplesInterval1;
+        prevPrevData2 = prevData2;
+        prevData2 = data2;
+        data2 = 0;
+        for (int m = 0; m < amountOfPoints; ++m) {
+            double tempData = (data[startDataIndex + m] - delt) / kdeSmoothH;
+            data2 += (double)expf((float)(-((tempData * tempData) / 2)));
+        }
+
+        if (w < 2)
+            continue;
+        if (strangePeak) {
+            if (prevData2 == data2)
+                continue;
+            else if (prevData2 < data2) {
+                strangePeak = 0;
+                continue;
+            } else if (prevData2 > data2) {
+                strangePeak = 0;
+                ++resultKde;
+                continue;
+            }
+        } else if (prevData2 > prevPrevData2 && prevData2 > data2) {
+            ++resultKde;
+            continue;
+        } else if (prevData2 > prevPrevData2 && prevData2 == data2) {
+            strangePeak = 1;
+            continue;
+        }
+    }
+    if (prevData2 < data2)
+        ++resultKde;
+    return resultKde;
+}
+
+/* cudaLibrary.cu:445-453: exact-equality shortcut, then FP32 hypotf of the
+ * double differences. */
+double orc_distance(double x1, double y1, double x2, double y2)
+{
+    if (x1 == x2 && y1 == y2)
+        return 0;
+    double dx = x2 - x1;
+    double dy = y2 - y1;
+    return (double)hypotf((float)dx, (float)dy);
+}
+
+/* cudaLibrary.cu:457-529, restated literally: labels at [start, start+n), the
+ * "stack" at start+n+k, popped from start+n+NumNeibor-1 into the loop variable;
+ * k only ranges over 0..n-2 (the last peak is never a neighbour); returns
+ * cluster-1. */
+int orc_dbscan(const double* data, const double* intervals, double* helpfulArray,
+               int64_t startDataIndex, int amountOfPeaks, int sizeOfHelpfulArray,
+               int maxAmountOfPeaks, double eps)
+{
+    if (amountOfPeaks <= 0)
+        return 0;
+    if (amountOfPeaks == 1)
+        return 1;
+    if (amountOfPeaks > maxAmountOfPeaks)
+        return 0;
+
+    const int64_t s = startDataIndex;
+    int cluster = 0;
+    int NumNeibor = 0;
+
+    for (int64_t i = s; i < s + sizeOfHelpfulArray; ++i)
+        helpfulArray[i] = 0;
+
+    for (int i = 0; i < amountOfPeaks; i++) {
+        if (NumNeibor >= 1) {
+            i = (int)helpfulArray[s + amountOfPeaks + NumNeibor - 1];
+            helpfulArray[s + amountOfPeaks + NumNeibor - 1] = 0;
+            NumNeibor = NumNeibor - 1;
+            for (int k = 0; k < amountOfPeaks - 1; k++) {
+                if (i != k && helpfulArray[s + k] == 0) {
+                    if (orc_distance(data[s + i], intervals[s + i], data[s + k], intervals[s + k]) < eps) {
+                        helpfulArray[s + k] = cluster;
+                        helpfulArray[s + amountOfPeaks + k] = k;
+                        ++NumNeibor;
+                    }
+                }
+            }
+        } else if (helpfulArray[s + i] == 0) {
+            NumNeibor = 0;
+            ++cluster;
+            helpfulArray[s + i] = cluster;
+            for (int k = 0; k < amountOfPeaks - 1; k++) {
+                if (i != k && helpfulArray[s + k] == 0) {
+                    if (orc_distance(data[s + i], intervals[s + i], data[s + k], intervals[s + k]) < eps) {
+                        helpfulArray[s + k] = cluster;
+                        helpfulArray[s + amountOfPeaks + k] = k;
+                        ++NumNeibor;
+                    }
+                }
+            }
+        }
+    }
+    return cluster - 1;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Per-point drivers                                                          */
+
+int orc_record_len(const orc_job* job)
+{
+    return (int)(job->tMax / job->h / (double)job->preScaller);
+}
+
+int orc_skip_len(const orc_job* job)
+{
+    return (int)(job->transientTime / job->h);
+}
+
+/* Per-thread set-up of calculateDiscreteModelCUDA (cudaLibrary.cu:96-105) and of
+ * its IC variant (:183-192): copy ICs and values, then overwrite the swept
+ * entries with getValueByIdx of the global point index. */
+static void setup_point(const orc_job* job, int64_t g, double* x, double* v)
+{
+    for (int i = 0; i < job->nIC; ++i)
+        x[i] = job->ic[i];
+    for (int i = 0; i < job->nV; ++i)
+        v[i] = job->values[i];
+    for (int i = 0; i < job->dims; ++i) {
+        double p = orc_get_value_by_idx((int)g, job->nPts, job->ranges[i * 2],
+                                        job->ranges[i * 2 + 1], i);
+        if (job->sweepIC)
+            x[job->idxMut[i]] = p;
+        else
+            v[job->idxMut[i]] = p;
+    }
+}
+
+/* cudaLibrary.cu:107-114 (and :194-201): unchecked transient, then the recorded
+ * loop with the divergence check on x[writableVar]. */
+int orc_trajectory_point(const orc_job* job, int64_t g, double* data)
+{
+    double x[8], v[16];
+    setup_point(job, g, x, v);
+    orc_loop(job->system, x, v, job->h, orc_skip_len(job), 1, 0, 0, NULL, 0, 1);
+    int ok = orc_loop(job->system, x, v, job->h, orc_record_len(job), job->preScaller,
+                      job->writableVar, job->maxValue, data, 0, 1);
+    return !ok;
+}
+
+/* LLEKernelCUDA, cudaLibrary.cu:666-785; IC variant LLEKernelICCUDA :789-908.
+ * Quirks kept: the seed uses the chunk-local thread index with int32 wrap (:723)
+ * or the IC formula (:846); every loop checks x[0] (writableVar hard-coded to 0)
+ * against maxValue and stops THAT integration early, but the LLE sum goes on and
+ * the final write overwrites the zero written on divergence (:750-754, :777). */
+double orc_lle_point(const orc_job* job, int64_t g)
+{
+    double x[8], y[8], z[8], v[16];
+    setup_point(job, g, x, v);
+
+    const int nIC = job->nIC;
+    const int idx = (int)(job->seedChunk > 0 ? (g % job->seedChunk) : g);
+    double zPower = 0;
+    for (int i = 0; i < nIC; ++i) {
+        if (!job->sweepIC) {
+            uint32_t u = (uint32_t)idx * ((uint32_t)i * (uint32_t)idx + 1u) + 1u;
+            int32_t arg = (int32_t)u;
+            z[i] = 0.5 * (double)sinf((float)arg);
+        } else {
+            double arg = 0.2171828 * (i + 1) + idx + (0.2171828 + i * idx);
+            z[i] = (double)sinf((float)arg) * 0.5;
+        }
+        zPower += z[i] * z[i];
+    }
+    zPower = sqrt(zPower);
+    for (int i = 0; i < nIC; i++)
+        z[i] /= zPower;
+
+    const int sys = job->system;
+    const double h = job->h;
+    const int skip = orc_skip_len(job);
+    const int nNT = (int)(size_t)(job->NT / h);
+    const int sizeOfBlock = (int)(job->tMax / job->NT);
+    const double eps = job->lleEps;
+
+    orc_loop(sys, x, v, h, skip, 1, 0, job->maxValue, NULL, 0, 1);
+
+    for (int i = 0; i < nIC; ++i)
+        y[i] = z[i] * eps + x[i];
+
+    double result = 0;
+    for (int i = 0; i < sizeOfBlock; ++i) {
+        orc_loop(sys, x, v, h, nNT, 1, 0, job->maxValue, NULL, 0, 1);
+        orc_loop(sys, y, v, h, nNT, 1, 0, job->maxValue, NULL, 0, 1);
+
+        double tempData = 0;
+        for (int l = 0; l < nIC; ++l)
+            tempData += (x[l] - y[l]) * (x[l] - y[l]);
+        tempData = sqrt(tempData) / eps;
+
+        result += log(tempData);
+
+        if (tempData != 0)
+            tempData = (1 / tempData);
+
+        for (int j = 0; j < nIC; ++j)
+            y[j] = (double)(x[j] - ((x[j] - y[j]) * tempData));
+    }
+    return result / job->tMax;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Map drivers                                                                */
+
+static int threads_or_default(int n)
+{
+#ifdef _OPENMP
+    return n > 0 ? n : omp_get_max_threads();
+#else
+    (void)n;
+    return 1;
+#endif
+}
+
+int orc_map_peaks(const orc_job* job, int64_t first, int64_t count, double* outPeaks,
+                  double* outIntervals, int32_t* counts, int64_t cap, int nThreads)
+{
+    const int rec = orc_record_len(job);
+    if (rec <= 0)
+        return -1;
+    int err = 0;
+#pragma omp parallel num_threads(threads_or_default(nThreads))
+    {
+        double* data = (double*)malloc(sizeof(double) * (size_t)rec);
+        double* peaks = (double*)malloc(sizeof(double) * (size_t)rec);
+        double* times = (double*)malloc(sizeof(double) * (size_t)rec);
+        if (!data || !peaks || !times) {
+#pragma omp atomic write
+            err = -2;
+        } else {
+#pragma omp for schedule(dynamic, 1)
+            for (int64_t k = 0; k < count; ++k) {
+                int diverged = orc_trajectory_point(job, first + k, data);
+                int n = 0;
+                if (!diverged)
+                    n = orc_peak_finder(data, 0, rec, peaks, times, 0.01);
+                counts[k] = n;
+                int64_t m = n < cap ? n : cap;
+                for (int64_t j = 0; j < m; ++j) {
+                    if (outPeaks)
+                        outPeaks[k * cap + j] = peaks[j];
+                    if (outIntervals)
+                        outIntervals[k * cap + j] = times[j];
+                }
+            }
+        }
+        free(data);
+        free(peaks);
+        free(times);
+    }
+    return err;
+}
+
+int orc_map_kde(const orc_job* job, int64_t first, int64_t count, int32_t* out, int nThreads)
+{
+    const int rec = orc_record_len(job);
+    if (rec <= 0)
+        return -1;
+    int err = 0;
+#pragma omp parallel num_threads(threads_or_default(nThreads))
+    {
+        double* data = (double*)malloc(sizeof(double) * (size_t)rec);
+        if (!data) {
+#pragma omp atomic write
+            err = -2;
+        } else {
+#pragma omp for schedule(dynamic, 1)
+            for (int64_t k = 0; k < count; ++k) {
+                int diverged = orc_trajectory_point(job, first + k, data);
+                int n = 0;
+                if (!diverged)
+                    n = orc_peak_finder(data, 0, rec, data, NULL, 0.01); /* in place, :514-515 */
+                out[k] = orc_kde(data, 0, n, job->maxAmountOfPeaks, job->kdeSampling,
+                                 job->kdeI1, job->kdeI2, job->kdeH);
+            }
+        }
+        free(data);
+    }
+    return err;
+}
+
+int orc_map_dbscan(const orc_job* job, int64_t first, int64_t count, int32_t* out, int nThreads)
+{
+    const int rec = orc_record_len(job);
+    if (rec <= 0)
+        return -1;
+    int err = 0;
+#pragma omp parallel num_threads(threads_or_default(nThreads))
+    {
+        double* data = (double*)malloc(sizeof(double) * (size_t)rec);
+        double* intervals = (double*)malloc(sizeof(double) * (size_t)rec);
+        double* helpful = (double*)malloc(sizeof(double) * (size_t)rec);
+        if (!data || !intervals || !helpful) {
+#pragma omp atomic write
+            err = -2;
+        } else {
+#pragma omp for schedule(dynamic, 1)
+            for (int64_t k = 0; k < count; ++k) {
+                int diverged = orc_trajectory_point(job, first + k, data);
+                int n = 0;
+                if (!diverged)
+                    n = orc_peak_finder(data, 0, rec, data, intervals, 0.01); /* :689-690 */
+                out[k] = orc_dbscan(data, intervals, helpful, 0, n, rec, job->maxAmountOfPeaks,
+                                    job->dbscanEps);
+            }
+        }
+        free(data);
+        free(intervals);
+        free(helpful);
+    }
+    return err;
+}
+
+int orc_map_lle(const orc_job* job, int64_t first, int64_t count, double* out, int nThreads)
+{
+    if ((int)(job->tMax / job->NT) <= 0 || job->nIC <= 0)
+        return -1;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads_or_default(nThreads))
+    for (int64_t k = 0; k < count; ++k)
+        out[k] = orc_lle_point(job, first + k);
+    return 0;
+}
+
+int orc_map_lle_list(const orc_job* job, const int64_t* idx, int64_t count, double* out, int nThreads)
+{
+    if ((int)(job->tMax / job->NT) <= 0 || job->nIC <= 0)
+        return -1;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads_or_default(nThreads))
+    for (int64_t k = 0; k < count; ++k)
+        out[k] = orc_lle_point(job, idx[k]);
+    return 0;
+}

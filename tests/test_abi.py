@@ -1,0 +1,206 @@
+"""C-ABI library checks that need no GPU: load, exports, validation, host logic."""
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+# The reference's hot-path entry points (Library/hostLibrary.cuh:29-459) by their
+# C++ mangled names: the facade must link in their place.
+REFERENCE_ENTRY_POINTS = [
+    "_Z13bifurcation1DdidiPKdS0_PKiiddS0_ii",
+    "_Z15bifurcation1DICdidiPKdS0_PKiiddS0_ii",
+    "_Z16bifurcation2DKDEdidiPKdS0_PKiididS0_iiiddd",
+    "_Z18bifurcation2DKDEICdidiPKdS0_PKiididS0_iiiddd",
+    "_Z19bifurcation2DDBSCANdidiPKdS0_PKiididS0_iid",
+    "_Z21bifurcation2DDBSCANICdidiPKdS0_PKiididS0_iid",
+    "_Z5LLE1DddiddPKdiS0_PKiiddS0_i",
+    "_Z7LLE1DICddiddPKdiS0_PKiiddS0_i",
+    "_Z5LLE2DddiddPKdiS0_PKiiddS0_i",
+    "_Z7LLE2DICddiddPKdiS0_PKiiddS0_i",
+]
+
+
+def _exports():
+    out = subprocess.run(["nm", "-D", "--defined-only", str(ROOT / "cudabifurcation3.0_b200" / "libcbf.so")],
+                         capture_output=True, text=True, check=True).stdout
+    return {line.split()[-1] for line in out.splitlines() if line.strip()}
+
+
+def _declared_in_headers():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = h.read_text()
+        names |= set(re.findall(r"\b(cbf_[a-z0-9_]+)\s*\(", text))
+    return names
+
+
+def test_library_loads_and_exports_every_declared_symbol(cbf):
+    L = cbf.lib()
+    assert L.cbf_abi_version() == 1
+    exported = _exports()
+    declared = _declared_in_headers()
+    assert declared, "no declarations found in include/*.h"
+    missing = sorted(declared - exported)
+    assert not missing, f"declared in include/*.h but not exported: {missing}"
+    assert not sorted(set(cbf.EXPORTS) - exported)
+
+
+def test_facade_links_as_the_reference_entry_points(cbf):
+    exported = _exports()
+    assert not [s for s in REFERENCE_ENTRY_POINTS if s not in exported]
+
+
+def test_facade_names_match_reference_header_when_available():
+    ref = Path("/root/reference/Library/hostLibrary.cuh")
+    if not ref.exists():
+        pytest.skip("reference sources not present")
+    text = ref.read_text()
+    for name in ("bifurcation1D", "bifurcation1DIC", "bifurcation2DKDE", "bifurcation2DKDEIC",
+                 "bifurcation2DDBSCAN", "bifurcation2DDBSCANIC", "LLE1D", "LLE1DIC", "LLE2D",
+                 "LLE2DIC"):
+        assert re.search(r"__host__ void " + name + r"\(", text), name
+
+
+def _job(cbf, **kw):
+    base = dict(task=cbf.TASK_LLE, system="chen", nPts=16, ranges=[30, 45, 20, 30], idxMut=[1, 3],
+                ic=[0.1, 0.1, 0.1], values=[0.5, 35, 3, 28], h=0.002, tMax=10, NT=0.5,
+                lleEps=1e-8, transientTime=1, maxValue=1e4)
+    base.update(kw)
+    return cbf.make_job(**base)
+
+
+@pytest.mark.parametrize("bad,code", [
+    (dict(system=9), 2),
+    (dict(ic=[0.1, 0.1]), 1),                 # wrong number of state variables
+    (dict(values=[0.5, 35, 3]), 1),           # too few parameters
+    (dict(idxMut=[1, 7]), 1),                 # swept index out of range
+    (dict(h=0.0), 1),
+    (dict(NT=0.0), 1),
+    (dict(task=9), 1),
+    (dict(task=1, preScaller=0, maxAmountOfPeaks=10), 1),
+    (dict(task=1, writableVar=5, maxAmountOfPeaks=10), 1),
+    (dict(nPts=0), 1),
+])
+def test_validation_errors(cbf, bad, code):
+    j = _job(cbf, **bad)
+    st = cbf.lib().cbf_validate(C.byref(j))
+    assert st == code
+    assert cbf.lib().cbf_last_error()  # a message is set
+
+
+def test_validation_accepts_reference_configs(cbf):
+    assert cbf.lib().cbf_validate(C.byref(_job(cbf))) == 0
+    # LLE ignores writableVar (the reference hard-codes x[0], cudaLibrary.cu:735)
+    assert cbf.lib().cbf_validate(C.byref(_job(cbf, writableVar=17))) == 0
+
+
+def test_derived_sizes_use_reference_truncations(cbf):
+    j = _job(cbf, task=cbf.TASK_KDE, tMax=200, h=0.005, maxAmountOfPeaks=10)
+    assert cbf.record_length(j) == int(200 / 0.005)
+    j = _job(cbf)
+    assert cbf.record_length(j) == int(10 / 0.5)
+    j = _job(cbf, task=cbf.TASK_PEAKS, tMax=500, h=0.01, preScaller=3, idxMut=[1], ranges=[0, 1])
+    assert cbf.record_length(j) == int(500 / 0.01 / 3)
+
+
+def test_divergence_threshold_is_exact(cbf, orc):
+    """fabs(x) >= T reproduces `fabsf(x) > maxValue` (cudaLibrary.cu:69-71) exactly."""
+    L = orc.lib()
+    rng = np.random.default_rng(3)
+    maxima = [1e4, 10.0, 6.0, 1000000.0, 1e7, 0.1, 1e-30, 3.4028234663852886e38, 1e300,
+              -1.0, 5e-45] + list(rng.uniform(0, 1e5, 60)) + list(10 ** rng.uniform(-40, 38, 60))
+    for m in maxima:
+        active, t = cbf.divergence_threshold(m)
+        assert active
+        probes = [t, np.nextafter(t, 0), np.nextafter(t, np.inf), m, -m, 0.0, np.inf, -np.inf,
+                  np.nextafter(m, 0), np.nextafter(m, np.inf)]
+        probes += list(t * (1 + rng.uniform(-1e-6, 1e-6, 20)))
+        for x in probes:
+            x = float(x)
+            if not np.isfinite(t) and not np.isfinite(x):
+                continue
+            want = bool(L.orc_diverged(x, m))
+            got = abs(x) >= t
+            assert want == got, (m, x, t)
+    assert cbf.divergence_threshold(0.0)[0] is False
+    assert cbf.divergence_threshold(float("inf"))[0] is False
+    assert cbf.divergence_threshold(float("nan"))[0] is False
+
+
+def _ref_map_csv(values, nPts, header, precision, is_double):
+    """The reference's ostream output (hostLibrary.cu:474-546), restated in Python."""
+    fmt = (lambda v: "%.*g" % (precision, v)) if is_double else (lambda v: "%d" % v)
+    s = []
+    if header is not None:
+        g = lambda v: "%.*g" % (precision, v)  # noqa: E731
+        s.append(f"{g(header[0])} {g(header[1])}\n{g(header[2])} {g(header[3])}\n")
+    cnt = 0
+    for v in values:
+        if cnt != 0:
+            s.append(", ")
+        if cnt == nPts:
+            s.append("\n")
+            cnt = 0
+        s.append(fmt(v))
+        cnt += 1
+    return "".join(s).encode()
+
+
+@pytest.mark.parametrize("nPts,precision,header,is_double", [
+    (4, 12, [0.05, 0.35, 0.05, 0.35], False),
+    (3, 6, [5, 20, 20, 200], False),
+    (5, 6, None, True),
+    (2, 6, [30, 45, 20, 30], True),
+])
+def test_csv_map_layout_is_byte_compatible(cbf, tmp_path, nPts, precision, header, is_double):
+    rng = np.random.default_rng(nPts)
+    if is_double:
+        vals = np.concatenate([rng.normal(size=nPts * nPts - 3) * 10.0 ** rng.integers(-8, 8, nPts * nPts - 3),
+                               [0.0, -0.0, 1.0 / 3.0]])
+        buf = np.ascontiguousarray(vals, np.float64)
+    else:
+        buf = np.ascontiguousarray(rng.integers(-1, 50, nPts * nPts), np.int32)
+    path = tmp_path / "m.csv"
+    hdr = None if header is None else np.array(header, np.float64)
+    st = cbf.lib().cbf_csv_write_map(str(path).encode(), buf.ctypes.data_as(C.c_void_p),
+                                     int(is_double), len(buf), nPts,
+                                     None if hdr is None else hdr.ctypes.data_as(C.c_void_p),
+                                     precision)
+    assert st == 0
+    assert path.read_bytes() == _ref_map_csv(buf.tolist(), nPts, header, precision, is_double)
+    text = path.read_text().split("\n")
+    if header is not None:
+        text = text[2:]
+    assert len(text) == nPts and all(r.endswith(", ") for r in text[:-1])
+
+
+def test_csv_peak_rows_layout(cbf, orc, tmp_path):
+    nPts, cap = 5, 4
+    ranges = np.array([0.05, 0.40], np.float64)
+    peaks = np.arange(nPts * cap, dtype=np.float64).reshape(nPts, cap) / 7.0
+    counts = np.array([0, 2, 4, 1, 3], np.int32)
+    path = tmp_path / "p.csv"
+    lib = cbf.lib()
+    lib.cbf_csv_write_peaks.argtypes = [C.c_char_p, C.c_int32, C.c_void_p, C.c_int64, C.c_int64,
+                                        C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]
+    assert lib.cbf_csv_write_peaks(str(path).encode(), nPts, ranges.ctypes.data, 0, nPts,
+                                   peaks.ctypes.data, cap, counts.ctypes.data, 0) == 0
+    want = []
+    for k in range(nPts):
+        par = orc.lib().orc_get_value_by_idx(k, nPts, 0.05, 0.40, 0)
+        for j in range(counts[k]):
+            want.append("%.12g, %.12g\n" % (par, peaks[k, j]))
+    assert path.read_text() == "".join(want)
+
+
+def test_csv_open_failure_is_reported(cbf, tmp_path):
+    buf = np.zeros(4, np.int32)
+    bad = tmp_path / "missing_dir" / "x.csv"
+    st = cbf.lib().cbf_csv_write_map(str(bad).encode(), buf.ctypes.data_as(C.c_void_p), 0, 4, 2,
+                                     None, 6)
+    assert st == 6  # CBF_ERR_IO

@@ -1,0 +1,238 @@
+"""GPU parity: the CUDA path (through the C-ABI) against the CPU oracle.
+
+Bar: bit-exact for integer outputs (peak counts, KDE and DBSCAN counts), for
+trajectories and for peak values/intervals; LLE within 1e-9 absolute (the LLE
+sum adds `log` terms, and the seed uses FP32 `sinf`, whose last bit may differ
+between CUDA and glibc).  Sizes are chosen so the oracle finishes in seconds.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+LLE_TOL = 1e-9
+
+# Parameter sets (values[0] = s = 0.5, the reference's CD symmetry convention).
+ROSSLER = dict(system="rossler", values=[0.5, 0.2, 0.2, 5.7], ic=[0.1, 0.1, 0.1])
+LORENZ = dict(system="lorenz", values=[0.5, 10.0, 28.0, 8.0 / 3.0], ic=[0.1, 0.1, 0.1])
+CHEN = dict(system="chen", values=[0.5, 35.0, 3.0, 28.0], ic=[0.1, 0.1, 0.1])
+MEMRISTIVE = dict(system="memristive5", values=[8, 35, 15, 0.01, -1.6676, 0.0676, 0.3682, 0.5],
+                  ic=[0.001, 0, 0, 0, 0])
+
+
+def both(cbf, orc, **kw):
+    """The same job for the product (cbf.Job) and the oracle (orc.OrcJob)."""
+    okw = {k: v for k, v in kw.items() if k not in ("task", "firstPoint", "nPoints", "flags",
+                                                    "peakCapacity")}
+    return cbf.make_job(**kw), orc.make_job(**okw)
+
+
+def test_expf_underflow_region_is_exactly_zero(cbf, gpu_ok):
+    # The KDE epilogue skips terms whose FP32 exponent argument is <= -128.
+    assert cbf.probe_expf_zero(-110.0) == 0
+    assert cbf.probe_expf_zero(-100.0) > 0  # the probe does see nonzero results
+
+
+@pytest.mark.parametrize("nPts,first,count", [(2048, 0, 4096), (2048, 4190000, 4304),
+                                               (8192, 16777000, 6000), (8192, 67100000, 8864)])
+def test_grid_coordinates_match_oracle(cbf, orc, gpu_ok, nPts, first, count):
+    j = cbf.make_job(task=cbf.TASK_LLE, system="chen", nPts=nPts, ranges=[30, 45, 20, 30],
+                     idxMut=[1, 3], ic=[0.1] * 3, values=[0.5, 35, 3, 28], h=0.002, tMax=1, NT=0.5,
+                     firstPoint=first, nPoints=count)
+    got = cbf.grid_coordinates(j)
+    L = orc.lib()
+    want0 = np.array([L.orc_get_value_by_idx(first + k, nPts, 30.0, 45.0, 0) for k in range(count)])
+    want1 = np.array([L.orc_get_value_by_idx(first + k, nPts, 20.0, 30.0, 1) for k in range(count)])
+    assert np.array_equal(got[:, 0], want0)
+    assert np.array_equal(got[:, 1], want1)
+
+
+@pytest.mark.parametrize("params,extra", [
+    (ROSSLER, dict(ranges=[0.05, 0.35, 0.05, 0.35], idxMut=[1, 2], h=0.01, writableVar=0)),
+    (LORENZ, dict(ranges=[5, 20, 20, 200], idxMut=[1, 2], h=0.005, writableVar=2)),
+    (CHEN, dict(ranges=[30, 45, 20, 30], idxMut=[1, 3], h=0.002, writableVar=1)),
+    (MEMRISTIVE, dict(ranges=[-6, 6, -15, 15], idxMut=[4, 3], h=0.005, writableVar=4)),
+])
+@pytest.mark.parametrize("sweepIC", [False, True])
+def test_trajectories_bit_exact(cbf, orc, gpu_ok, params, extra, sweepIC):
+    kw = dict(params, **extra)
+    if sweepIC:
+        kw["idxMut"] = [0, 1]
+        kw["ranges"] = [-2, 2, -3, 3]
+    j, o = both(cbf, orc, task=cbf.TASK_TRAJECTORY, nPts=5, tMax=20 * kw["h"] * 100,
+                transientTime=kw["h"] * 700, preScaller=2, maxValue=1e4, sweepIC=sweepIC, **kw)
+    traj, div = cbf.run_host(j)
+    rec = cbf.record_length(j)
+    for g in range(25):
+        want, wdiv = orc.trajectory(o, g)
+        assert bool(div[g]) == wdiv, g
+        got = traj[g, :rec]
+        if wdiv:
+            n_ok = np.argmax(~np.isfinite(got)) if not np.all(np.isfinite(got)) else rec
+            assert np.array_equal(got[:n_ok], want[:n_ok]), g
+        else:
+            assert np.array_equal(got, want), g
+
+
+def test_divergence_stops_trajectories_like_reference(cbf, orc, gpu_ok):
+    # maxValue far inside the attractor: most points diverge during the record.
+    j, o = both(cbf, orc, task=cbf.TASK_TRAJECTORY, nPts=6, tMax=5.0, transientTime=1.0,
+                preScaller=1, maxValue=12.0, ranges=[5, 20, 20, 200], idxMut=[1, 2], h=0.005,
+                writableVar=0, **LORENZ)
+    traj, div = cbf.run_host(j)
+    n_div = 0
+    for g in range(36):
+        want, wdiv = orc.trajectory(o, g)
+        assert bool(div[g]) == wdiv
+        n_div += wdiv
+    assert n_div > 0
+
+
+def test_bifurcation1d_rossler_bit_exact(cbf, orc, gpu_ok):
+    # The 1-D diagram configuration (Rossler a in [0.05, 0.40], 1000 t.u. transient,
+    # 500 t.u. record, h = 0.01) on 64 points.
+    kw = dict(nPts=64, ranges=[0.05, 0.40], idxMut=[1], h=0.01, tMax=500.0, transientTime=1000.0,
+              maxValue=1e4, writableVar=0, preScaller=1, **ROSSLER)
+    j, o = both(cbf, orc, task=cbf.TASK_PEAKS, **kw)
+    peaks, counts = cbf.run_host(j)
+    cap = peaks.shape[1]
+    wp, wt, wc = orc.map_peaks(o, 0, 64, cap)
+    assert np.array_equal(counts, wc)
+    for k in range(64):
+        assert np.array_equal(peaks[k, :counts[k]], wp[k, :wc[k]]), k
+    assert counts.sum() > 64
+
+
+def test_bifurcation1d_reference_api_matches_job_api(cbf, gpu_ok):
+    peaks, counts = cbf.bifurcation1D(100.0, 16, 0.01, 3, [0.1, 0.1, 0.1], [0.05, 0.35], [1], 0,
+                                      1e4, 200.0, [0.5, 0.2, 0.2, 5.7], 4, 1, system="rossler")
+    j = cbf.make_job(task=cbf.TASK_PEAKS, nPts=16, ranges=[0.05, 0.35], idxMut=[1], h=0.01,
+                     tMax=100.0, transientTime=200.0, maxValue=1e4, **ROSSLER)
+    p2, c2 = cbf.run_host(j)
+    assert np.array_equal(counts, c2) and np.array_equal(peaks, p2)
+
+
+LORENZ_MAP = dict(nPts=10, ranges=[5, 20, 20, 200], idxMut=[1, 2], h=0.005, tMax=60.0,
+                  transientTime=50.0, maxValue=1e4, writableVar=0, preScaller=1, **LORENZ)
+
+
+@pytest.mark.parametrize("maxPeaks,samp,i1,i2,hh,flags", [
+    (10000, 10, -20.0, 60.0, 0.05, 0),
+    (10000, 4, -30.0, 60.0, 0.5, 0),
+    (40, 10, -20.0, 60.0, 0.05, 0),          # some points exceed maxAmountOfPeaks
+    (10000, 256, -20.0, 60.0, 0.05, 2),      # fixed 256-sample extension
+])
+def test_kde_map_bit_exact(cbf, orc, gpu_ok, maxPeaks, samp, i1, i2, hh, flags):
+    kw = dict(LORENZ_MAP, maxAmountOfPeaks=maxPeaks, kdeSampling=samp, kdeI1=i1, kdeI2=i2, kdeH=hh)
+    j, o = both(cbf, orc, task=cbf.TASK_KDE, flags=flags, **kw)
+    got, _ = cbf.run_host(j)
+    n = kw["nPts"] ** 2
+    if flags & cbf.FLAG_KDE_FIXED:
+        # oracle: the same kde() with k1 = 256 fixed, i.e. kdeSampling = 256 / n per point
+        peaks, _, counts = orc.map_peaks(o, 0, n, cbf.lib().cbf_peak_capacity(C.byref(j)))
+        want = []
+        for k in range(n):
+            want.append(orc.kde_fixed(peaks[k, :counts[k]], maxPeaks, samp, i1, i2, hh))
+        want = np.array(want, np.int32)
+    else:
+        want = orc.map_kde(o, 0, n)
+    assert np.array_equal(got, want), np.nonzero(got != want)
+
+
+@pytest.mark.parametrize("maxPeaks,eps", [(10000, 1e-3), (10000, 0.05), (10000, 2.0), (30, 0.05)])
+def test_dbscan_map_bit_exact(cbf, orc, gpu_ok, maxPeaks, eps):
+    kw = dict(LORENZ_MAP, maxAmountOfPeaks=maxPeaks, dbscanEps=eps)
+    j, o = both(cbf, orc, task=cbf.TASK_DBSCAN, **kw)
+    got, _ = cbf.run_host(j)
+    want = orc.map_dbscan(o, 0, kw["nPts"] ** 2)
+    assert np.array_equal(got, want), np.nonzero(got != want)
+
+
+def test_kde_dbscan_ic_sweep_and_divergence(cbf, orc, gpu_ok):
+    kw = dict(LORENZ_MAP, sweepIC=True, idxMut=[0, 1], ranges=[-16, 16, -16, 16], maxValue=30.0,
+              maxAmountOfPeaks=10000)
+    j, o = both(cbf, orc, task=cbf.TASK_DBSCAN, dbscanEps=0.05, **kw)
+    got, _ = cbf.run_host(j)
+    assert np.array_equal(got, orc.map_dbscan(o, 0, 100))
+    j, o = both(cbf, orc, task=cbf.TASK_KDE, kdeSampling=10, kdeI1=-20.0, kdeI2=60.0, kdeH=0.05,
+                **kw)
+    got, _ = cbf.run_host(j)
+    assert np.array_equal(got, orc.map_kde(o, 0, 100))
+
+
+CHEN_LLE = dict(nPts=8, ranges=[30, 45, 20, 30], idxMut=[1, 3], h=0.002, NT=0.5, tMax=40.0,
+                transientTime=10.0, lleEps=1e-8, maxValue=1e4, **CHEN)
+
+
+@pytest.mark.parametrize("extra", [
+    dict(),
+    dict(seedChunk=37),                                     # chunk-local seed index
+    dict(maxValue=20.0),                                    # early exits every interval
+    dict(sweepIC=True, idxMut=[0, 2], ranges=[-16, 16, 5, 30]),
+    dict(dims=1),
+])
+def test_lle_map_matches_oracle(cbf, orc, gpu_ok, extra):
+    kw = dict(CHEN_LLE)
+    dims = extra.pop("dims", 2)
+    kw.update(extra)
+    if dims == 1:
+        kw["idxMut"] = kw["idxMut"][:1]
+        kw["ranges"] = kw["ranges"][:2]
+        kw["nPts"] = 40
+    j, o = both(cbf, orc, task=cbf.TASK_LLE, **kw)
+    got, _ = cbf.run_host(j)
+    want = orc.map_lle(o, 0, kw["nPts"] ** dims)
+    err = np.abs(got - want)
+    assert np.all(err <= LLE_TOL), (err.max(), np.argmax(err))
+    assert np.isfinite(want).all()
+
+
+@pytest.mark.parametrize("params,extra", [
+    (LORENZ, dict(ranges=[5, 20, 20, 200], idxMut=[1, 2], h=0.005)),
+    (ROSSLER, dict(ranges=[0.05, 0.35, 0.05, 0.35], idxMut=[1, 2], h=0.01)),
+    (MEMRISTIVE, dict(ranges=[-6, 6, -15, 15], idxMut=[4, 3], h=0.005, maxValue=1e7)),
+])
+def test_lle_other_systems(cbf, orc, gpu_ok, params, extra):
+    kw = dict(nPts=6, NT=0.4, tMax=20.0, transientTime=5.0, lleEps=1e-6, maxValue=1e4)
+    kw.update(params)
+    kw.update(extra)
+    j, o = both(cbf, orc, task=cbf.TASK_LLE, **kw)
+    got, _ = cbf.run_host(j)
+    want = orc.map_lle(o, 0, 36)
+    assert np.all(np.abs(got - want) <= LLE_TOL), np.abs(got - want).max()
+
+
+def test_reference_named_lle2d(cbf, orc, gpu_ok):
+    got = cbf.LLE2D(40.0, 0.5, 8, 0.002, 1e-8, [0.1, 0.1, 0.1], 3, [30, 45, 20, 30], [1, 3], 0,
+                    1e4, 10.0, [0.5, 35, 3, 28], 4, system="chen")
+    o = orc.make_job(nPts=8, ranges=[30, 45, 20, 30], idxMut=[1, 3], h=0.002, NT=0.5, tMax=40.0,
+                     transientTime=10.0, lleEps=1e-8, maxValue=1e4, seedChunk=200000, **CHEN)
+    want = orc.map_lle(o, 0, 64).reshape(8, 8)
+    assert np.all(np.abs(got - want) <= LLE_TOL)
+
+
+def test_device_api_with_torch_stream(cbf, gpu_ok):
+    torch = pytest.importorskip("torch")
+    j = cbf.make_job(task=cbf.TASK_LLE, **CHEN_LLE)
+    n = 64
+    out = torch.empty(n, dtype=torch.float64, device="cuda")
+    s = torch.cuda.Stream()
+    before = cbf.kernel_launches()
+    with torch.cuda.stream(s):
+        cbf.run_device(j, out.data_ptr(), 0, s.cuda_stream)
+    s.synchronize()
+    assert cbf.kernel_launches() == before + 1
+    host, _ = cbf.run_host(cbf.make_job(task=cbf.TASK_LLE, **CHEN_LLE))
+    assert np.array_equal(out.cpu().numpy(), host)
+
+
+def test_exact_grid_flag(cbf, orc, gpu_ok):
+    j = cbf.make_job(task=cbf.TASK_LLE, system="chen", nPts=8192, ranges=[0, 8191, 0, 8191],
+                     idxMut=[1, 3], ic=[0.1] * 3, values=[0.5, 35, 3, 28], h=0.002, tMax=1, NT=0.5,
+                     firstPoint=16777216, nPoints=2048, flags=cbf.FLAG_EXACT_GRID)
+    got = cbf.grid_coordinates(j)
+    g = np.arange(16777216, 16777216 + 2048)
+    assert np.array_equal(got[:, 0], (g % 8192).astype(float))
+    assert np.array_equal(got[:, 1], (g // 8192).astype(float))

@@ -1,0 +1,132 @@
+"""Pin the CPU oracle to the reference's own code (CPU only).
+
+tests/golden/reference_vectors.npz holds outputs of the reference's
+getValueByIdx, peakFinder, kde, distance, dbscan and its shipped model through
+loopCalculateDiscreteModel, computed by compiling those functions from the
+reference sources (tests/golden/make_golden.py).  The oracle must reproduce all
+of them bit for bit.  When oracle/_ref/libcbf_ref.so is present the same
+checks also run live on fresh random inputs.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+GOLDEN = Path(__file__).resolve().parent / "golden" / "reference_vectors.npz"
+
+
+@pytest.fixture(scope="module")
+def G():
+    return np.load(GOLDEN)
+
+
+def test_grid_index_matches_reference(G, orc):
+    L = orc.lib()
+    got = np.array([L.orc_get_value_by_idx(int(i), int(p), float(a), float(b), int(v))
+                    for i, p, a, b, v in zip(G["grid_idx"], G["grid_npts"], G["grid_lo"],
+                                             G["grid_hi"], G["grid_axis"])])
+    assert np.array_equal(got.view(np.int64), G["grid_val"].view(np.int64))
+
+
+def test_grid_index_float_quirk_is_real(orc):
+    # 8192^2 grid: the float division rounds the index above 2^24 (cudaLibrary.cu:214).
+    L = orc.lib()
+    idx = 16777217  # 2^24 + 1 -> (float) rounds to 2^24
+    quirk = L.orc_get_value_by_idx(idx, 8192, 0.0, 8191.0, 0)
+    assert quirk == float((idx - 1) % 8192)
+
+
+def test_peak_finder_matches_reference(G, orc):
+    flat, offs = G["pf_flat"], G["pf_offs"]
+    want_n = G["pf_counts"]
+    pk_off = np.concatenate([[0], np.cumsum(want_n)])
+    for i in range(len(want_n)):
+        seq = flat[offs[i]:offs[i + 1]]
+        p, t = orc.peak_finder(seq) if len(seq) else (np.zeros(0), np.zeros(0))
+        assert len(p) == want_n[i], i
+        assert np.array_equal(p, G["pf_peaks"][pk_off[i]:pk_off[i + 1]]), i
+        assert np.array_equal(t, G["pf_times"][pk_off[i]:pk_off[i + 1]]), i
+
+
+def test_peak_finder_quirks(orc):
+    # rising plateau: the sample after the plateau is skipped (cudaLibrary.cu:231-234)
+    d = [0, 2, 2, 3, 1, 0, 5, 0, 4, 0]
+    p, t = orc.peak_finder(d)
+    # detected peaks at 6 and 8 (3 at index 3 is skipped); first one is dropped
+    assert list(p) == [4.0] and np.allclose(t, [0.02])
+    # fewer than two detected peaks -> zero
+    assert len(orc.peak_finder([0, 1, 0])[0]) == 0
+
+
+def test_kde_matches_reference(G, orc):
+    offs = G["kde_offs"]
+    for i, (maxp, samp, i1, i2, hh) in enumerate(G["kde_params"]):
+        p = G["kde_flat"][offs[i]:offs[i + 1]]
+        got = orc.kde(p, int(maxp), int(samp), i1, i2, hh)
+        assert got == G["kde_res"][i], i
+
+
+def test_kde_special_cases(orc):
+    assert orc.kde([], 10, 5, -1, 1, 0.1) == 0
+    assert orc.kde([1.0], 10, 5, -1, 1, 0.1) == 1
+    assert orc.kde([1.0, 2.0], 10, 5, -1, 1, 0.1) == 1
+    assert orc.kde([1.0, 2.0, 3.0, 4.0], 3, 5, -1, 1, 0.1) == 3  # > max -> max
+
+
+def test_distance_matches_reference(G, orc):
+    L = orc.lib()
+    got = np.array([L.orc_distance(*map(float, r)) for r in G["dist_in"]])
+    assert np.array_equal(got, G["dist_out"])
+
+
+def test_dbscan_matches_reference(G, orc):
+    offs = G["db_offs"]
+    for i, (maxp, eps) in enumerate(G["db_params"]):
+        p = G["db_p"][offs[i]:offs[i + 1]]
+        t = G["db_t"][offs[i]:offs[i + 1]]
+        assert orc.dbscan(p, t, int(maxp), eps) == G["db_res"][i], i
+
+
+def test_dbscan_special_cases(orc):
+    assert orc.dbscan([], [], 10, 0.1) == 0
+    assert orc.dbscan([1.0], [0.1], 10, 0.1) == 1
+    assert orc.dbscan([1.0, 2.0, 3.0], [0.1] * 3, 2, 0.1) == 0  # > max -> 0
+    # the last peak is never anyone's neighbour and the result is cluster-1
+    assert orc.dbscan([1.0, 1.0, 1.0], [0.1] * 3, 10, 0.5) == 1
+
+
+def test_shipped_model_matches_reference(G, orc):
+    L = orc.lib()
+    vals = G["m5_vals"]
+    steps = int(G["m5_steps"])
+    for r in range(len(G["m5_x0"])):
+        x = G["m5_x0"][r].copy()
+        d = np.zeros(steps)
+        ok = L.orc_loop(0, x, vals, 0.005, steps, int(G["m5_pre"][r]), int(G["m5_wv"][r]),
+                        float(G["m5_max"][r]), d.ctypes.data, 0, 1)
+        assert ok == G["m5_ok"][r], r
+        assert np.array_equal(x, G["m5_x"][r]), r
+        assert np.array_equal(d, G["m5_data"][r]), r
+
+
+@pytest.mark.skipif(not (Path(__file__).resolve().parents[1] / "oracle" / "_ref" /
+                         "libcbf_ref.so").exists(), reason="reference shim not built")
+def test_live_random_against_reference(orc):
+    R = orc.ref()
+    L = orc.lib()
+    rng = np.random.default_rng(7)
+    for _ in range(300):
+        n = int(rng.integers(3, 50))
+        s = rng.integers(0, 3, n).astype(float)
+        a, b = s.copy(), s.copy()
+        pa, ta, pb, tb = (np.zeros(n) for _ in range(4))
+        ca = R.ref_peakFinder(a, 0, n, pa.ctypes.data, ta.ctypes.data, 0.01)
+        cb = L.orc_peak_finder(b, 0, n, pb.ctypes.data, tb.ctypes.data, 0.01)
+        assert ca == cb and np.array_equal(pa[:ca], pb[:cb]) and np.array_equal(ta[:ca], tb[:cb])
+        p = np.round(rng.normal(size=n), 2)
+        t = rng.integers(1, 3, n) * 0.01
+        ha, hb = np.zeros(2 * n + 2), np.zeros(2 * n + 2)
+        assert R.ref_dbscan(p.copy(), t.copy(), ha, 0, n, len(ha), 60, 0.05) == \
+            L.orc_dbscan(p.copy(), t.copy(), hb, 0, n, len(hb), 60, 0.05)
+        assert R.ref_kde(p.copy(), 0, n, 60, 4, -3.0, 3.0, 0.1) == \
+            L.orc_kde(p.copy(), 0, n, 60, 4, -3.0, 3.0, 0.1)
