@@ -318,7 +318,7 @@ def main(argv=None) -> int:
     if dist:
         dist.all_reduce(e2e_total, op=dist.ReduceOp.MAX)
     e2e_value = world * n * len(e2e_times) / float(e2e_total.item())
-    assert np.array_equal(res, out.cpu().numpy()), "host API and device API maps differ"
+    assert np.array_equal(res, out.cpu().numpy(), equal_nan=True), "host and device API maps differ"
 
     flops_per_launch = float(n) * spp * CHEN_FLOPS_PER_STEP
     achieved = flops_per_launch / (ms_per_step / 1e3) / 1e12 if world == 1 else \

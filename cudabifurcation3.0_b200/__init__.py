@@ -40,7 +40,7 @@ EXPORTS = [
     "cbf_bifurcation2d_kde_ic", "cbf_bifurcation2d_dbscan", "cbf_bifurcation2d_dbscan_ic",
     "cbf_lle1d", "cbf_lle1d_ic", "cbf_lle2d", "cbf_lle2d_ic", "cbf_run_host",
     "cbf_grid_coordinates", "cbf_probe_fp64_peak", "cbf_probe_expf_zero",
-    "cbf_divergence_threshold", "cbf_csv_write_map", "cbf_csv_write_peaks", "cbf_csv_write_pairs",
+    "cbf_divergence_threshold", "cbf_lle_seeds", "cbf_csv_write_map", "cbf_csv_write_peaks", "cbf_csv_write_pairs",
 ]
 
 
@@ -117,6 +117,8 @@ def lib():
         L.cbf_run.argtypes = [C.POINTER(Job), C.c_void_p, C.c_void_p, C.c_void_p]
         L.cbf_run_host.argtypes = [C.POINTER(Job), C.c_void_p, C.c_void_p]
         L.cbf_grid_coordinates.argtypes = [C.POINTER(Job), _dp]
+        L.cbf_lle_seeds.argtypes = [C.POINTER(Job), _dp]
+        L.cbf_lle_seeds.restype = C.c_int32
         L.cbf_probe_fp64_peak.argtypes = [C.c_double, _dp]
         L.cbf_probe_expf_zero.argtypes = [C.c_float, C.POINTER(C.c_uint64)]
         L.cbf_divergence_threshold.argtypes = [C.c_double, _ip, _dp]
@@ -242,6 +244,14 @@ def grid_coordinates(job: Job) -> np.ndarray:
     n = lib().cbf_job_points(C.byref(job))
     out = np.zeros((n, 2), np.float64)
     check(lib().cbf_grid_coordinates(C.byref(job), out.ctypes.data_as(_dp)))
+    return out
+
+
+def lle_seeds(job: Job) -> np.ndarray:
+    """Device-computed LLE perturbation vectors, shape (points, nIC)."""
+    n = lib().cbf_job_points(C.byref(job))
+    out = np.zeros((n, job.nIC), np.float64)
+    check(lib().cbf_lle_seeds(C.byref(job), out.ctypes.data_as(_dp)))
     return out
 
 

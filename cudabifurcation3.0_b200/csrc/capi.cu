@@ -622,6 +622,27 @@ cbf_status cbf_grid_coordinates(const cbf_job* job, double* out_host)
     return CBF_OK;
 }
 
+cbf_status cbf_lle_seeds(const cbf_job* job, double* out_host)
+{
+    DevJob d;
+    cbf_status st = lower_job(job, &d);
+    if (st != CBF_OK) return st;
+    if (d.task != CBF_TASK_LLE) return fail(CBF_ERR_INVALID_ARG, "cbf_lle_seeds needs an LLE job");
+    if (!out_host) return fail(CBF_ERR_INVALID_ARG, "null output");
+    if (d.nPoints == 0) return CBF_OK;
+    cudaStream_t s;
+    if ((st = library_stream(&s)) != CBF_OK) return st;
+    double* dd = nullptr;
+    const size_t bytes = (size_t)d.nPoints * d.nIC * sizeof(double);
+    CBF_CUDA(cudaMallocAsync((void**)&dd, bytes, s));
+    cudaError_t e = launch_lle_seeds(d, dd, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out_host, dd, bytes, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFreeAsync(dd, s);
+    if (e != cudaSuccess) return cuda_fail(e, "lle seeds");
+    return CBF_OK;
+}
+
 cbf_status cbf_probe_fp64_peak(double ms, double* tflops)
 {
     if (!tflops || !(ms > 0)) return fail(CBF_ERR_INVALID_ARG, "bad probe arguments");

@@ -106,6 +106,29 @@ __device__ __forceinline__ bool diverged(double v, double thresh)
     return fabs(v) >= thresh;
 }
 
+// Deterministic LLE perturbation direction from the chunk-local thread index
+// (cudaLibrary.cu:720-732; IC variant :843-855), normalised in double.
+template <int D, bool IC>
+__device__ __forceinline__ void lle_seed(long long g, long long seedChunk, double (&z)[D])
+{
+    const int idx = (int)(seedChunk > 0 ? (g % seedChunk) : g);
+    double zPower = 0;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        if (!IC) {
+            const unsigned u = (unsigned)idx * ((unsigned)i * (unsigned)idx + 1u) + 1u;
+            z[i] = 0.5 * (double)sinf((float)(int)u);
+        } else {
+            const double arg = 0.2171828 * (i + 1) + idx + (0.2171828 + i * idx);
+            z[i] = (double)sinf((float)arg) * 0.5;
+        }
+        zPower += z[i] * z[i];
+    }
+    zPower = sqrt(zPower);
+#pragma unroll
+    for (int i = 0; i < D; ++i) z[i] /= zPower;
+}
+
 // Kernel launch bookkeeping (defined in capi.cu).
 void note_launch(unsigned n = 1);
 
@@ -113,5 +136,6 @@ void note_launch(unsigned n = 1);
 cudaError_t launch_lle(const DevJob& J, double* d_out, cudaStream_t s);
 cudaError_t launch_bif(const DevJob& J, void* d_out, int* d_aux, cudaStream_t s);
 cudaError_t launch_grid_coords(const DevJob& J, double* d_out, cudaStream_t s);
+cudaError_t launch_lle_seeds(const DevJob& J, double* d_out, cudaStream_t s);
 
 }  // namespace cbf

@@ -114,25 +114,8 @@ __global__ void __launch_bounds__(kLleThreads) lle_kernel(const DevJob J, double
         setup_point<D>(J, g, x, v);
         const typename S::Coef c = S::prep(v, J.h);
 
-        // Deterministic perturbation direction from the chunk-local thread index
-        // (cudaLibrary.cu:720-732; IC variant :843-855).
-        const int idx = (int)(J.seedChunk > 0 ? (g % J.seedChunk) : g);
         double z[D];
-        double zPower = 0;
-#pragma unroll
-        for (int i = 0; i < D; ++i) {
-            if (!IC) {
-                const unsigned u = (unsigned)idx * ((unsigned)i * (unsigned)idx + 1u) + 1u;
-                z[i] = 0.5 * (double)sinf((float)(int)u);
-            } else {
-                const double arg = 0.2171828 * (i + 1) + idx + (0.2171828 + i * idx);
-                z[i] = (double)sinf((float)arg) * 0.5;
-            }
-            zPower += z[i] * z[i];
-        }
-        zPower = sqrt(zPower);
-#pragma unroll
-        for (int i = 0; i < D; ++i) z[i] /= zPower;
+        lle_seed<D, IC>(g, J.seedChunk, z);
 
         run_checked<S>(x, c, J.nSkip, J);
 
@@ -154,6 +137,30 @@ __global__ void __launch_bounds__(kLleThreads) lle_kernel(const DevJob J, double
         }
         out[p] = result / J.tMax;
     }
+}
+
+template <int D, bool IC>
+__global__ void lle_seed_kernel(const DevJob J, double* __restrict__ out)
+{
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= J.nPoints) return;
+    double z[D];
+    lle_seed<D, IC>(J.firstPoint + p, J.seedChunk, z);
+#pragma unroll
+    for (int i = 0; i < D; ++i) out[p * D + i] = z[i];
+}
+
+template <int D>
+cudaError_t launch_seeds_d(const DevJob& J, double* d_out, cudaStream_t s)
+{
+    const long long blocks = (J.nPoints + 127) / 128;
+    if (blocks == 0) return cudaSuccess;
+    if (J.sweepIC)
+        lle_seed_kernel<D, true><<<(unsigned)blocks, 128, 0, s>>>(J, d_out);
+    else
+        lle_seed_kernel<D, false><<<(unsigned)blocks, 128, 0, s>>>(J, d_out);
+    note_launch();
+    return cudaGetLastError();
 }
 
 template <class S, bool IC>
@@ -182,6 +189,17 @@ cudaError_t launch_lle(const DevJob& J, double* d_out, cudaStream_t s)
     case CBF_SYS_ROSSLER: return launch_lle_s<Rossler>(J, d_out, s);
     case CBF_SYS_LORENZ: return launch_lle_s<Lorenz>(J, d_out, s);
     case CBF_SYS_CHEN: return launch_lle_s<Chen>(J, d_out, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_lle_seeds(const DevJob& J, double* d_out, cudaStream_t s)
+{
+    switch (J.system) {
+    case CBF_SYS_MEMRISTIVE5: return launch_seeds_d<Memristive5::DIM>(J, d_out, s);
+    case CBF_SYS_ROSSLER: return launch_seeds_d<Rossler::DIM>(J, d_out, s);
+    case CBF_SYS_LORENZ: return launch_seeds_d<Lorenz::DIM>(J, d_out, s);
+    case CBF_SYS_CHEN: return launch_seeds_d<Chen::DIM>(J, d_out, s);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -222,6 +222,10 @@ cbf_status cbf_csv_write_pairs(const char* path, int32_t nPts, const double* ran
 /* ---- probes used for measurement and self-checks --------------------- */
 /* Grid coordinates the kernels use for points [first, first+n): out[k*2+axis]. */
 cbf_status cbf_grid_coordinates(const cbf_job* job, double* out_host);
+/* The normalised LLE perturbation vectors z (nIC per point) the LLE kernels
+ * start from for points [first, first+n) (cudaLibrary.cu:720-732, :843-855);
+ * out_host[k*nIC + i].  Lets a checker isolate the FP32 sinf of the seed. */
+cbf_status cbf_lle_seeds(const cbf_job* job, double* out_host);
 /* FP64 FMA throughput of this GPU (TFLOP/s, 2 flops per FMA) over ~`ms` ms. */
 cbf_status cbf_probe_fp64_peak(double ms, double* tflops);
 /* Exhaustive device check that expf(x) == 0 for every float x <= threshold;

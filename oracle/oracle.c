@@ -394,11 +394,8 @@ int orc_trajectory_point(const orc_job* job, int64_t g, double* data)
  * or the IC formula (:846); every loop checks x[0] (writableVar hard-coded to 0)
  * against maxValue and stops THAT integration early, but the LLE sum goes on and
  * the final write overwrites the zero written on divergence (:750-754, :777). */
-double orc_lle_point(const orc_job* job, int64_t g)
+void orc_lle_seed(const orc_job* job, int64_t g, double* z)
 {
-    double x[8], y[8], z[8], v[16];
-    setup_point(job, g, x, v);
-
     const int nIC = job->nIC;
     const int idx = (int)(job->seedChunk > 0 ? (g % job->seedChunk) : g);
     double zPower = 0;
@@ -416,6 +413,26 @@ double orc_lle_point(const orc_job* job, int64_t g)
     zPower = sqrt(zPower);
     for (int i = 0; i < nIC; i++)
         z[i] /= zPower;
+}
+
+double orc_lle_point(const orc_job* job, int64_t g)
+{
+    return orc_lle_point_seeded(job, g, NULL);
+}
+
+/* zIn: the normalised perturbation to start from (NULL: orc_lle_seed). */
+double orc_lle_point_seeded(const orc_job* job, int64_t g, const double* zIn)
+{
+    double x[8], y[8], z[8], v[16];
+    setup_point(job, g, x, v);
+
+    const int nIC = job->nIC;
+    if (zIn) {
+        for (int i = 0; i < nIC; ++i)
+            z[i] = zIn[i];
+    } else {
+        orc_lle_seed(job, g, z);
+    }
 
     const int sys = job->system;
     const double h = job->h;
@@ -569,6 +586,17 @@ int orc_map_lle(const orc_job* job, int64_t first, int64_t count, double* out, i
 #pragma omp parallel for schedule(dynamic, 1) num_threads(threads_or_default(nThreads))
     for (int64_t k = 0; k < count; ++k)
         out[k] = orc_lle_point(job, first + k);
+    return 0;
+}
+
+int orc_map_lle_seeded(const orc_job* job, int64_t first, int64_t count, const double* z,
+                       double* out, int nThreads)
+{
+    if ((int)(job->tMax / job->NT) <= 0 || job->nIC <= 0)
+        return -1;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads_or_default(nThreads))
+    for (int64_t k = 0; k < count; ++k)
+        out[k] = orc_lle_point_seeded(job, first + k, z + k * job->nIC);
     return 0;
 }
 

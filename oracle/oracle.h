@@ -98,6 +98,12 @@ int orc_skip_len(const orc_job* job);     /* (int)(transientTime / h) */
 int orc_trajectory_point(const orc_job* job, int64_t g, double* data);
 /* Per point: Benettin LLE (cudaLibrary.cu:666-785, IC variant :789-908). */
 double orc_lle_point(const orc_job* job, int64_t g);
+/* The same from a given normalised perturbation z (NULL: the seed below).  Lets
+ * a check feed the device's FP32 sinf seed so that only the LLE arithmetic is
+ * compared. */
+double orc_lle_point_seeded(const orc_job* job, int64_t g, const double* z);
+/* The seed of cudaLibrary.cu:720-732 (IC variant :843-855) with glibc sinf. */
+void orc_lle_seed(const orc_job* job, int64_t g, double* z);
 
 /* Map-level drivers over global points [first, first+count), OpenMP over points.
  * Peaks: outPeaks[k*cap + j], outIntervals likewise (may be NULL), counts[k]
@@ -110,6 +116,9 @@ int orc_map_kde(const orc_job* job, int64_t first, int64_t count, int32_t* out, 
 int orc_map_dbscan(const orc_job* job, int64_t first, int64_t count, int32_t* out, int nThreads);
 /* LLEKernelCUDA path (hostLibrary.cu:1598-1623) */
 int orc_map_lle(const orc_job* job, int64_t first, int64_t count, double* out, int nThreads);
+/* Same with per-point seeds z[k*nIC + i]. */
+int orc_map_lle_seeded(const orc_job* job, int64_t first, int64_t count, const double* z,
+                       double* out, int nThreads);
 /* Same, over an explicit list of global indices (strided samples for the CPU baseline). */
 int orc_map_lle_list(const orc_job* job, const int64_t* idx, int64_t count, double* out, int nThreads);
 

@@ -143,6 +143,12 @@ def lib():
         L.orc_map_dbscan.argtypes = [C.POINTER(OrcJob), C.c_int64, C.c_int64, _ip, C.c_int]
         L.orc_map_lle.restype = C.c_int
         L.orc_map_lle.argtypes = [C.POINTER(OrcJob), C.c_int64, C.c_int64, _dp, C.c_int]
+        L.orc_lle_point_seeded.restype = C.c_double
+        L.orc_lle_point_seeded.argtypes = [C.POINTER(OrcJob), C.c_int64, C.c_void_p]
+        L.orc_lle_seed.restype = None
+        L.orc_lle_seed.argtypes = [C.POINTER(OrcJob), C.c_int64, _dp]
+        L.orc_map_lle_seeded.restype = C.c_int
+        L.orc_map_lle_seeded.argtypes = [C.POINTER(OrcJob), C.c_int64, C.c_int64, _dp, _dp, C.c_int]
         L.orc_map_lle_list.restype = C.c_int
         L.orc_map_lle_list.argtypes = [C.POINTER(OrcJob), _lp, C.c_int64, _dp, C.c_int]
         _lib = L
@@ -266,6 +272,25 @@ def map_lle(job: OrcJob, first: int, count: int, threads: int = 0):
     rc = lib().orc_map_lle(C.byref(job), first, count, out, threads)
     if rc != 0:
         raise RuntimeError(f"orc_map_lle failed: {rc}")
+    return out
+
+
+def map_lle_seeded(job: OrcJob, first: int, count: int, z, threads: int = 0):
+    """LLE map started from the given perturbations z[count, nIC]."""
+    z = np.ascontiguousarray(z, dtype=np.float64)
+    out = np.zeros(count, np.float64)
+    rc = lib().orc_map_lle_seeded(C.byref(job), first, count, z, out, threads)
+    if rc != 0:
+        raise RuntimeError(f"orc_map_lle_seeded failed: {rc}")
+    return out
+
+
+def lle_seeds(job: OrcJob, first: int, count: int):
+    out = np.zeros((count, job.nIC), np.float64)
+    row = np.zeros(job.nIC, np.float64)
+    for k in range(count):
+        lib().orc_lle_seed(C.byref(job), first + k, row)
+        out[k] = row
     return out
 
 

@@ -1,9 +1,12 @@
 """GPU parity: the CUDA path (through the C-ABI) against the CPU oracle.
 
 Bar: bit-exact for integer outputs (peak counts, KDE and DBSCAN counts), for
-trajectories and for peak values/intervals; LLE within 1e-9 absolute (the LLE
-sum adds `log` terms, and the seed uses FP32 `sinf`, whose last bit may differ
-between CUDA and glibc).  Sizes are chosen so the oracle finishes in seconds.
+trajectories and for peak values/intervals; LLE within 1e-9 absolute.  The LLE
+seed is FP32 `sinf` of an integer, whose last bit differs between CUDA and glibc
+for some arguments, so the LLE comparisons start the oracle from the device's
+seed vectors (cbf_lle_seeds) and a separate test bounds the seed difference;
+what remains is CUDA vs glibc `log` in the sum.  Sizes are chosen so the oracle
+finishes in seconds.
 """
 import ctypes as C
 
@@ -20,6 +23,20 @@ LORENZ = dict(system="lorenz", values=[0.5, 10.0, 28.0, 8.0 / 3.0], ic=[0.1, 0.1
 CHEN = dict(system="chen", values=[0.5, 35.0, 3.0, 28.0], ic=[0.1, 0.1, 0.1])
 MEMRISTIVE = dict(system="memristive5", values=[8, 35, 15, 0.01, -1.6676, 0.0676, 0.3682, 0.5],
                   ic=[0.001, 0, 0, 0, 0])
+
+
+def assert_lle_close(got, want, tol=LLE_TOL):
+    """Same non-finite values (-inf when a trajectory lands exactly on a fixed
+    point and log(0) enters the sum, NaN after inf-inf) at the same positions;
+    finite values within tol."""
+    got = np.asarray(got)
+    want = np.asarray(want)
+    fin = np.isfinite(want)
+    assert np.array_equal(fin, np.isfinite(got))
+    assert np.array_equal(np.isnan(got), np.isnan(want))
+    assert np.array_equal(got[np.isinf(want)], want[np.isinf(want)])
+    err = np.abs(got[fin] - want[fin])
+    assert err.size == 0 or err.max() <= tol, (err.max(), np.argmax(err))
 
 
 def both(cbf, orc, **kw):
@@ -111,7 +128,9 @@ def test_bifurcation1d_reference_api_matches_job_api(cbf, gpu_ok):
     j = cbf.make_job(task=cbf.TASK_PEAKS, nPts=16, ranges=[0.05, 0.35], idxMut=[1], h=0.01,
                      tMax=100.0, transientTime=200.0, maxValue=1e4, **ROSSLER)
     p2, c2 = cbf.run_host(j)
-    assert np.array_equal(counts, c2) and np.array_equal(peaks, p2)
+    assert np.array_equal(counts, c2)
+    for k in range(16):  # entries past the count are unspecified, as in the reference
+        assert np.array_equal(peaks[k, :counts[k]], p2[k, :c2[k]])
 
 
 LORENZ_MAP = dict(nPts=10, ranges=[5, 20, 20, 200], idxMut=[1, 2], h=0.005, tMax=60.0,
@@ -183,10 +202,10 @@ def test_lle_map_matches_oracle(cbf, orc, gpu_ok, extra):
         kw["nPts"] = 40
     j, o = both(cbf, orc, task=cbf.TASK_LLE, **kw)
     got, _ = cbf.run_host(j)
-    want = orc.map_lle(o, 0, kw["nPts"] ** dims)
-    err = np.abs(got - want)
-    assert np.all(err <= LLE_TOL), (err.max(), np.argmax(err))
-    assert np.isfinite(want).all()
+    n = kw["nPts"] ** dims
+    want = orc.map_lle_seeded(o, 0, n, cbf.lle_seeds(j))
+    assert_lle_close(got, want)
+    assert np.isfinite(want).mean() > 0.9
 
 
 @pytest.mark.parametrize("params,extra", [
@@ -200,8 +219,8 @@ def test_lle_other_systems(cbf, orc, gpu_ok, params, extra):
     kw.update(extra)
     j, o = both(cbf, orc, task=cbf.TASK_LLE, **kw)
     got, _ = cbf.run_host(j)
-    want = orc.map_lle(o, 0, 36)
-    assert np.all(np.abs(got - want) <= LLE_TOL), np.abs(got - want).max()
+    want = orc.map_lle_seeded(o, 0, 36, cbf.lle_seeds(j))
+    assert_lle_close(got, want)
 
 
 def test_reference_named_lle2d(cbf, orc, gpu_ok):
@@ -209,8 +228,35 @@ def test_reference_named_lle2d(cbf, orc, gpu_ok):
                     1e4, 10.0, [0.5, 35, 3, 28], 4, system="chen")
     o = orc.make_job(nPts=8, ranges=[30, 45, 20, 30], idxMut=[1, 3], h=0.002, NT=0.5, tMax=40.0,
                      transientTime=10.0, lleEps=1e-8, maxValue=1e4, seedChunk=200000, **CHEN)
-    want = orc.map_lle(o, 0, 64).reshape(8, 8)
-    assert np.all(np.abs(got - want) <= LLE_TOL)
+    j = cbf.make_job(task=cbf.TASK_LLE, seedChunk=200000, **CHEN_LLE)
+    want = orc.map_lle_seeded(o, 0, 64, cbf.lle_seeds(j)).reshape(8, 8)
+    assert_lle_close(got, want)
+
+
+@pytest.mark.parametrize("sweepIC,chunk", [(False, 0), (False, 200000), (False, 37), (True, 0)])
+def test_lle_seeds_match_glibc_within_ulps(cbf, orc, gpu_ok, sweepIC, chunk):
+    """The seed is 0.5*sinf(int) normalised (cudaLibrary.cu:720-732, :843-855):
+    CUDA's and glibc's sinf agree to a few float ulps, i.e. ~1e-7 relative."""
+    kw = dict(CHEN_LLE, nPts=64, seedChunk=chunk)
+    if sweepIC:
+        kw.update(sweepIC=True, idxMut=[0, 2], ranges=[-16, 16, 5, 30])
+    j, o = both(cbf, orc, task=cbf.TASK_LLE, **kw)
+    dev = cbf.lle_seeds(j)
+    host = orc.lle_seeds(o, 0, 64 * 64)
+    assert np.all(np.abs(dev - host) <= 1e-6), np.abs(dev - host).max()
+    assert np.allclose(np.linalg.norm(dev, axis=1), 1.0, atol=1e-15)
+    frac_exact = np.mean(np.all(dev == host, axis=1))
+    assert frac_exact > 0.3  # most seeds are bit-identical
+
+
+def test_lle_long_run_seed_sensitivity_is_small(cbf, orc, gpu_ok):
+    """With the oracle's own glibc seeds, the LLE still agrees once the
+    perturbation has aligned (long record): the libm difference washes out."""
+    kw = dict(CHEN_LLE, nPts=4, tMax=200.0, transientTime=20.0)
+    j, o = both(cbf, orc, task=cbf.TASK_LLE, **kw)
+    got, _ = cbf.run_host(j)
+    want = orc.map_lle(o, 0, 16)
+    assert_lle_close(got, want, 1e-5)
 
 
 def test_device_api_with_torch_stream(cbf, gpu_ok):
@@ -225,7 +271,7 @@ def test_device_api_with_torch_stream(cbf, gpu_ok):
     s.synchronize()
     assert cbf.kernel_launches() == before + 1
     host, _ = cbf.run_host(cbf.make_job(task=cbf.TASK_LLE, **CHEN_LLE))
-    assert np.array_equal(out.cpu().numpy(), host)
+    assert np.array_equal(out.cpu().numpy(), host, equal_nan=True)
 
 
 def test_exact_grid_flag(cbf, orc, gpu_ok):
