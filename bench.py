@@ -8,6 +8,7 @@ reference, seed chunk 200000).  FP64 throughout.  Inputs are synthetic by
 nature: the grid itself.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py --workload lorenz-dbscan-1024|lorenz-kde256-1024|lorenz-kde-1024|rossler-bif1d-1000
 
 Multi-GPU (torchrun, one rank per GPU): every rank computes its own 2048x2048 map
 of one c-stripe (weak scaling, no data-path collective); time = max over ranks.
@@ -16,8 +17,9 @@ The JSON line reports:
            launching stream around each map, L2 flushed between maps;
   e2e      the same through the public host API (cbf_lle2d: host output buffer,
            device allocation, launch, D2H copy inside the timed region);
-  roofline achieved FP64 flops of the LLE kernel vs the FP64 FMA peak measured on
-           the same GPU by the library's probe kernel;
+  roofline achieved FP64 flops of the LLE kernel vs the FP64 peak (the larger of
+           the nominal 64 lanes/SM x 2 x clock and the library's FMA probe), plus
+           the FP64-pipe instruction utilisation;
   cpu_baseline the CPU oracle (restatement of the reference per-point code) on a
            strided sample, all host threads.
 """
@@ -43,8 +45,32 @@ PKG_DIR = ROOT / "cudabifurcation3.0_b200"
 WORKLOAD = dict(system="chen", nPts=2048, ranges=[30.0, 45.0, 20.0, 30.0], idxMut=[1, 3],
                 ic=[0.1, 0.1, 0.1], values=[0.5, 35.0, 3.0, 28.0], h=0.002, NT=0.5, tMax=1000.0,
                 transientTime=500.0, lleEps=1e-8, maxValue=1e4, seedChunk=200000)
-CHEN_FLOPS_PER_STEP = 26   # FP64 flops of one Chen CD step, FMA = 2 (systems.cuh)
 METRIC = "grid points/s, 2D LLE map (plain FP64)"
+# FP64 work of one CD step of each system (csrc/systems.cuh; FMA = 2 flops)
+FLOPS_PER_STEP = {"chen": 19, "lorenz": 19, "rossler": 17, "memristive5": 66}
+FP64_INSTR_PER_STEP = {"chen": 14, "lorenz": 14, "rossler": 10, "memristive5": 52}
+FP64_LANES_PER_SM = 64
+
+# The other measured configurations (printed as their own JSON lines with
+# --workload NAME; the default run is the LLE map above).
+_LORENZ = dict(system="lorenz", nPts=1024, ranges=[5.0, 20.0, 20.0, 200.0], idxMut=[1, 2],
+               ic=[0.1, 0.1, 0.1], values=[0.5, 10.0, 28.0, 8.0 / 3.0], h=0.005, tMax=200.0,
+               transientTime=500.0, maxValue=1e4, writableVar=0, preScaller=1,
+               maxAmountOfPeaks=10000)
+SECONDARY = {
+    # 2-D DBSCAN cluster-count map, Lorenz (sigma, rho) 1024^2, eps 1e-3
+    "lorenz-dbscan-1024": dict(_LORENZ, task=2, dbscanEps=1e-3),
+    # 2-D KDE mode-count map with 256 samples per point (fixed-sample mode)
+    "lorenz-kde256-1024": dict(_LORENZ, task=1, kdeSampling=256, flags=2, kdeI1=-60.0,
+                               kdeI2=60.0, kdeH=1.0),
+    # the same with the reference's per-peak sampling (k1 = 4 * peaks)
+    "lorenz-kde-1024": dict(_LORENZ, task=1, kdeSampling=4, kdeI1=-60.0, kdeI2=60.0, kdeH=0.5),
+    # 1-D bifurcation diagram, Rossler a in [0.05, 0.40], 1000 points
+    "rossler-bif1d-1000": dict(system="rossler", nPts=1000, ranges=[0.05, 0.40], idxMut=[1],
+                               ic=[0.1, 0.1, 0.1], values=[0.5, 0.2, 0.2, 5.7], h=0.01,
+                               tMax=500.0, transientTime=1000.0, maxValue=1e4, writableVar=0,
+                               preScaller=1, task=0),
+}
 
 
 def load_cbf():
@@ -131,42 +157,61 @@ class ClockSampler:
                 "reasons": sorted(reasons)}
 
 
+def fp64_roofline(torch, device: int, system: str, n_points: int, spp: int, mean_ms: float,
+                  clocks: dict, probe_tflops: float) -> dict:
+    """FP64 roofline of one map: algorithmic flops and FP64-pipe instructions."""
+    props = torch.cuda.get_device_properties(device)
+    max_mhz = clocks.get("sm_max_mhz") or 1965.0
+    nominal = props.multi_processor_count * FP64_LANES_PER_SM * 2 * max_mhz * 1e6 / 1e12
+    peak = max(nominal, probe_tflops)
+    flops = float(n_points) * spp * FLOPS_PER_STEP[system]
+    achieved = flops / (mean_ms / 1e3) / 1e12
+    sm_mhz = clocks.get("sm_mhz") or max_mhz
+    instr = float(n_points) * spp * FP64_INSTR_PER_STEP[system]
+    pipe = instr / (mean_ms / 1e3) / (props.multi_processor_count * FP64_LANES_PER_SM * sm_mhz * 1e6)
+    return {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak,
+            "peak_source": "max(nominal SMs x 64 FP64 lanes x 2 flops x max SM clock, FP64 FMA "
+                           "probe measured in this run); MEASURED_PEAKS.json has no FP64 figure",
+            "peak_nominal": nominal, "peak_probe": probe_tflops, "flops_per_launch": flops,
+            "flops_per_step": FLOPS_PER_STEP[system],
+            "fp64_instr_per_step": FP64_INSTR_PER_STEP[system],
+            "fp64_pipe_frac": pipe}
+
+
 def cpu_baseline(w: dict, target_s: float = 15.0) -> dict:
     """Oracle port of the reference per-point code on a strided sample, all threads."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
     threads = O.host_threads()
-    job = O.make_job(**{k: v for k, v in w.items()})
+    job = O.make_job(**w)
     n_total = w["nPts"] ** 2
-    # calibrate: one point per thread
     probe = np.arange(threads, dtype=np.int64) * (n_total // max(threads, 1))
     t0 = time.perf_counter()
     O.map_lle_list(job, probe, threads)
-    dt = time.perf_counter() - t0
-    per_round = max(dt, 1e-3)
-    rounds = max(1, int(target_s / per_round))
-    count = rounds * threads
+    per_round = max(time.perf_counter() - t0, 1e-3)
+    count = max(1, int(target_s / per_round)) * threads
     stride = max(1, n_total // count)
     idx = (np.arange(count, dtype=np.int64) * stride) % n_total
     t0 = time.perf_counter()
     O.map_lle_list(job, idx, threads)
     dt = time.perf_counter() - t0
     return {"value": count / dt, "unit": "points/s", "cores": threads, "kind": "port",
-            "sample": f"{count} of {n_total} points (every {stride}th), full 1.25e6 steps each",
-            "seconds": dt}
+            "sample": f"{count} of {n_total} points (every {stride}th), "
+                      f"{steps_per_point(w)} steps each"}
 
 
 def traffic_from_profiles():
     """Per-launch DRAM bytes of the LLE kernel from the committed ncu summary, if any."""
-    p = ROOT / "profiles" / "lle_chen_2048_ncu.json"
+    p = ROOT / "profiles" / "lle_chen_2048_traffic.json"
     try:
-        d = json.loads(p.read_text())
-        return d.get("dram_bytes_per_full_launch")
+        return json.loads(p.read_text()).get("dram_bytes_per_full_launch")
     except (OSError, ValueError):
         return None
 
 
 def run_reference(args) -> int:
+    """The reference's per-point code (oracle port) on the host cores."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -213,8 +258,88 @@ def run_reference(args) -> int:
     return 0
 
 
+def run_secondary(args, name: str) -> int:
+    """One of the other configurations: device-resident points/s, oracle sample."""
+    import torch
+    torch.cuda.set_device(0)
+    cbf = load_cbf()
+    w = dict(SECONDARY[name])
+    if args.nPts:
+        w["nPts"] = args.nPts
+    task = w.pop("task")
+    job = cbf.make_job(task=task, **w)
+    dims = len(w["idxMut"])
+    n = w["nPts"] ** dims
+    rec = cbf.record_length(job)
+    spp = int(w["transientTime"] / w["h"]) + rec * w["preScaller"]
+    if task == cbf.TASK_PEAKS:
+        cap = cbf.lib().cbf_peak_capacity(C.byref(job))
+        job.peakCapacity = cap
+        out = torch.empty(n * cap, dtype=torch.float64, device="cuda")
+        aux = torch.empty(n, dtype=torch.int32, device="cuda")
+        aux_ptr = aux.data_ptr()
+    else:
+        out = torch.empty(n, dtype=torch.int32, device="cuda")
+        aux_ptr = 0
+    stream = torch.cuda.Stream()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        cbf.run_device(job, out.data_ptr(), aux_ptr, stream.cuda_stream)
+    stream.synchronize()
+    sampler = ClockSampler(0)
+    torch.cuda.synchronize()
+    sampler.start()
+    launches0 = cbf.kernel_launches()
+    ms = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        cbf.run_device(job, out.data_ptr(), aux_ptr, stream.cuda_stream)
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        stream.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    launches = cbf.kernel_launches() - launches0
+    clocks = sampler.stop()
+    t = statistics.mean(ms)
+    probe = cbf.probe_fp64_peak(300.0)
+    roof = fp64_roofline(torch, 0, w["system"], n, spp, t, clocks, probe)
+    roof["traffic"] = None
+    roof["note"] = "integration flops only; the peak/KDE/DBSCAN work is on top"
+    # oracle on a small contiguous sample
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    threads = O.host_threads()
+    oj = O.make_job(**{k: v for k, v in w.items() if k != "flags"})
+    cnt = min(n, threads * 2)
+    t0 = time.perf_counter()
+    if task == cbf.TASK_DBSCAN:
+        O.map_dbscan(oj, n // 2, cnt, threads)
+    elif task == cbf.TASK_KDE and not (w.get("flags", 0) & 2):
+        O.map_kde(oj, n // 2, cnt, threads)
+    else:
+        O.map_peaks(oj, n // 2, cnt, max(rec // 2, 1), threads)
+    cpu_pps = cnt / (time.perf_counter() - t0)
+    line = {"metric": f"grid points/s, {name}", "value": n / (t / 1e3), "unit": "points/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (the parameter grid is the input)",
+            "config": {"workload": name, "grid": f"{w['nPts']}^{dims}", "steps_per_point": spp,
+                       "record": rec, "cache": "L2 flushed before every timed map"},
+            "roofline": roof,
+            "cpu_baseline": {"value": cpu_pps, "unit": "points/s", "cores": threads,
+                             "kind": "port", "sample": f"{cnt} contiguous points"},
+            "gpu_launches": int(launches), "clocks": clocks, "kernel_ms": ms}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(argv=None) -> int:
-    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap = argparse.ArgumentParser(description=__doc__,
+                                 formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
@@ -222,24 +347,26 @@ def main(argv=None) -> int:
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--nPts", type=int, default=None, help="override the grid side (testing)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="chen-lle2d-2048",
+                    choices=["chen-lle2d-2048", *SECONDARY])
     args = ap.parse_args(argv)
 
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "chen-lle2d-2048":
+        return run_secondary(args, args.workload)
 
     import torch
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     dist = None
+    torch.cuda.set_device(local)
     if world > 1:
         import datetime
         import torch.distributed as dist
-        torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
-    else:
-        torch.cuda.set_device(local)
 
     cbf = load_cbf()
     cbf.check(cbf.lib().cbf_set_device(local))
@@ -250,7 +377,7 @@ def main(argv=None) -> int:
     job = cbf.make_job(task=cbf.TASK_LLE, **w)
     spp = steps_per_point(w)
 
-    fp64_peak = cbf.probe_fp64_peak(300.0)  # TFLOP/s, FMA = 2 flops
+    probe = cbf.probe_fp64_peak(300.0)  # TFLOP/s, FMA = 2 flops
 
     stream = torch.cuda.Stream()
     out = torch.empty(n, dtype=torch.float64, device="cuda")
@@ -287,8 +414,7 @@ def main(argv=None) -> int:
     launches = cbf.kernel_launches() - launches0
     clocks = sampler.stop()
     kernel_ms = [a.elapsed_time(b) for a, b in evs]
-    total_ms = sum(kernel_ms)
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    t = torch.tensor([sum(kernel_ms)], dtype=torch.float64, device="cuda")
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     total_ms = float(t.item())
@@ -318,18 +444,16 @@ def main(argv=None) -> int:
     if dist:
         dist.all_reduce(e2e_total, op=dist.ReduceOp.MAX)
     e2e_value = world * n * len(e2e_times) / float(e2e_total.item())
-    assert np.array_equal(res, out.cpu().numpy(), equal_nan=True), "host and device API maps differ"
+    same = np.array_equal(res, out.cpu().numpy(), equal_nan=True)
 
-    flops_per_launch = float(n) * spp * CHEN_FLOPS_PER_STEP
-    achieved = flops_per_launch / (ms_per_step / 1e3) / 1e12 if world == 1 else \
-        flops_per_launch / (statistics.mean(kernel_ms) / 1e3) / 1e12
-    traffic = traffic_from_profiles()
+    roof = fp64_roofline(torch, local, w["system"], n, spp, statistics.mean(kernel_ms),
+                         clocks, probe)
+    roof["traffic"] = traffic_from_profiles()
 
     if rank == 0:
         base = None
         if world == 1 and not args.no_cpu_baseline:
             base = cpu_baseline(w)
-            base.pop("seconds", None)
         line = {
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -342,14 +466,8 @@ def main(argv=None) -> int:
                        "cache": "L2 flushed (256 MB write) before every timed map; inputs are scalars",
                        "parallelism": f"{world} independent c-stripes, one per GPU"},
             "e2e": {"value": e2e_value, "unit": "points/s", "h2d_bytes_per_step": C.sizeof(cbf.Job),
-                    "d2h_bytes_per_step": n * 8},
-            "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak,
-                         "unit": "TFLOP/s", "frac": achieved / fp64_peak,
-                         "traffic": traffic,
-                         "peak_source": "FP64 FMA-chain probe kernel on this GPU, same run "
-                                        "(MEASURED_PEAKS.json has no FP64 figure)",
-                         "flops_per_launch": flops_per_launch,
-                         "flops_per_step": CHEN_FLOPS_PER_STEP},
+                    "d2h_bytes_per_step": n * 8, "matches_device_api": bool(same)},
+            "roofline": roof,
             "cpu_baseline": base,
             "gpu_launches": int(launches),
             "clocks": clocks,
@@ -359,7 +477,7 @@ def main(argv=None) -> int:
     if dist:
         dist.barrier()
         dist.destroy_process_group()
-    return 0
+    return 0 if same else 1
 
 
 if __name__ == "__main__":

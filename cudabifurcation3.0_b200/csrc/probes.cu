@@ -13,13 +13,14 @@ namespace cbf {
 
 namespace {
 
-constexpr int kChains = 8;
+constexpr int kChains = 16;
 
 __global__ void __launch_bounds__(256) fp64_fma_kernel(double* out, int iters, double a, double b)
 {
     double r[kChains];
 #pragma unroll
     for (int c = 0; c < kChains; ++c) r[c] = (threadIdx.x + c) * 1e-6;
+#pragma unroll 4
     for (int i = 0; i < iters; ++i) {
 #pragma unroll
         for (int c = 0; c < kChains; ++c) r[c] = fma(r[c], a, b);

@@ -62,22 +62,62 @@ static void step_memristive5(double* x, const double* a, double h)
     x[4] = (double)y[4] + h1 * (x[0]);
 }
 
+/* The library's Rossler, Lorenz and Chen CD steps.  Specification (shared with
+ * the CUDA kernels, which must match it operation for operation): with k = h*s,
+ * h1 = h*(1-s), the explicit half (reverse variable order) and the linearly
+ * implicit half (forward order) multiplied out, parameter-only factors hoisted.
+ * Coefficients are recomputed here on every step (same values every time). */
+
 /* Rossler x'=-y-z, y'=x+a*y, z'=b+z*(x-c); values = {s, a, b, c}. */
 static void step_rossler(double* X, const double* v, double h)
 {
     const double s = v[0], a = v[1], b = v[2], c = v[3];
     const double k = h * s;
     const double h1 = h * (1.0 - s);
-    const double h1b = h1 * b;
+    const double c1 = 1.0 - k * c;
+    const double kb = k * b;
+    const double bq = 1.0 + k * a;
+    const double hs = k + h1;
     const double r2 = 1.0 / (1.0 - h1 * a);
-    double x = X[0], y = X[1], z = X[2];
-    z = fma(k, fma(z, x - c, b), z);
-    y = fma(k, fma(a, y, x), y);
-    x = fma(-k, y + z, x);
-    x = fma(-h1, y + z, x);
-    y = fma(h1, x, y) * r2;
-    z = (z + h1b) / fma(-h1, x - c, 1.0);
-    X[0] = x; X[1] = y; X[2] = z;
+    const double g = h1 * r2;
+    const double h1b = h1 * b;
+    const double c2 = 1.0 + h1 * c;
+    const double x = X[0], y = X[1], z = X[2];
+    const double z1 = fma(z, fma(k, x, c1), kb);       /* z + k*(b + z*(x-c)) */
+    const double y1 = fma(bq, y, k * x);               /* y + k*(x + a*y) */
+    const double x2 = fma(-hs, y1 + z1, x);            /* x - k*(y1+z1) - h1*(y1+z1) */
+    const double y2 = fma(g, x2, r2 * y1);             /* (y1 + h1*x2)/(1 - h1*a) */
+    const double z2 = (z1 + h1b) / fma(-h1, x2, c2);   /* (z1 + h1*b)/(1 - h1*(x2-c)) */
+    X[0] = x2; X[1] = y2; X[2] = z2;
+}
+
+/* Chen x'=a*(y-x), y'=(c-a)*x-x*z+c*y, z'=x*y-b*z; values = {s, a, b, c}. */
+static void step_chen(double* X, const double* v, double h)
+{
+    const double s = v[0], a = v[1], b = v[2], c = v[3];
+    const double k = h * s;
+    const double h1 = h * (1.0 - s);
+    const double ka = k * a;
+    const double h1a = h1 * a;
+    const double ca = 1.0 - k * b;
+    const double cb = 1.0 + k * c;
+    const double cma = c - a;
+    const double r1 = 1.0 / (1.0 + h1a);
+    const double d = (1.0 - ka) * r1;
+    const double e = (ka + h1a) * r1;
+    const double r2 = 1.0 / (1.0 - h1 * c);
+    const double g = h1 * r2;
+    const double r3 = 1.0 / (1.0 + h1 * b);
+    const double hh = h1 * r3;
+    const double x = X[0], y = X[1], z = X[2];
+    const double kx = k * x;
+    const double z1 = fma(kx, y, ca * z);        /* z + k*(x*y - b*z) */
+    const double w = cma - z1;
+    const double y1 = fma(kx, w, cb * y);        /* y + k*((c-a)*x - x*z1 + c*y) */
+    const double x2 = fma(d, x, e * y1);         /* explicit + implicit x half-steps */
+    const double y2 = fma(g * x2, w, r2 * y1);   /* (y1 + h1*x2*((c-a)-z1))/(1 - h1*c) */
+    const double z2 = fma(hh * x2, y2, r3 * z1); /* (z1 + h1*x2*y2)/(1 + h1*b) */
+    X[0] = x2; X[1] = y2; X[2] = z2;
 }
 
 /* Lorenz x'=sigma*(y-x), y'=x*(rho-z)-y, z'=x*y-beta*z; values = {s, sigma, rho, beta}. */
@@ -88,39 +128,24 @@ static void step_lorenz(double* X, const double* v, double h)
     const double h1 = h * (1.0 - s);
     const double ks = k * sg;
     const double h1s = h1 * sg;
+    const double ca = 1.0 - k * beta;
+    const double cb = 1.0 - k;
     const double r1 = 1.0 / (1.0 + h1s);
+    const double d = (1.0 - ks) * r1;
+    const double e = (ks + h1s) * r1;
     const double r2 = 1.0 / (1.0 + h1);
+    const double g = h1 * r2;
     const double r3 = 1.0 / (1.0 + h1 * beta);
-    double x = X[0], y = X[1], z = X[2];
-    z = fma(k, fma(-beta, z, x * y), z);
-    y = fma(k, fma(x, rho - z, -y), y);
-    x = fma(ks, y - x, x);
-    x = fma(h1s, y, x) * r1;
-    y = fma(h1, x * (rho - z), y) * r2;
-    z = fma(h1, x * y, z) * r3;
-    X[0] = x; X[1] = y; X[2] = z;
-}
-
-/* Chen x'=a*(y-x), y'=(c-a)*x-x*z+c*y, z'=x*y-b*z; values = {s, a, b, c}. */
-static void step_chen(double* X, const double* v, double h)
-{
-    const double s = v[0], a = v[1], b = v[2], c = v[3];
-    const double k = h * s;
-    const double h1 = h * (1.0 - s);
-    const double cma = c - a;
-    const double ka = k * a;
-    const double h1a = h1 * a;
-    const double r1 = 1.0 / (1.0 + h1a);
-    const double r2 = 1.0 / (1.0 - h1 * c);
-    const double r3 = 1.0 / (1.0 + h1 * b);
-    double x = X[0], y = X[1], z = X[2];
-    z = fma(k, fma(-b, z, x * y), z);
-    y = fma(k, fma(x, cma - z, c * y), y);
-    x = fma(ka, y - x, x);
-    x = fma(h1a, y, x) * r1;
-    y = fma(h1, x * (cma - z), y) * r2;
-    z = fma(h1, x * y, z) * r3;
-    X[0] = x; X[1] = y; X[2] = z;
+    const double hh = h1 * r3;
+    const double x = X[0], y = X[1], z = X[2];
+    const double kx = k * x;
+    const double z1 = fma(kx, y, ca * z);
+    const double w = rho - z1;
+    const double y1 = fma(kx, w, cb * y);
+    const double x2 = fma(d, x, e * y1);
+    const double y2 = fma(g * x2, w, r2 * y1);
+    const double z2 = fma(hh * x2, y2, r3 * z1);
+    X[0] = x2; X[1] = y2; X[2] = z2;
 }
 
 int orc_system_dim(int system)
