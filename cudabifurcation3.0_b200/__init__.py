@@ -40,7 +40,8 @@ EXPORTS = [
     "cbf_bifurcation2d_kde_ic", "cbf_bifurcation2d_dbscan", "cbf_bifurcation2d_dbscan_ic",
     "cbf_lle1d", "cbf_lle1d_ic", "cbf_lle2d", "cbf_lle2d_ic", "cbf_run_host",
     "cbf_grid_coordinates", "cbf_probe_fp64_peak", "cbf_probe_expf_zero",
-    "cbf_divergence_threshold", "cbf_lle_seeds", "cbf_csv_write_map", "cbf_csv_write_peaks", "cbf_csv_write_pairs",
+    "cbf_divergence_threshold", "cbf_lle_seeds", "cbf_bifurcation2d_dbscan_noalloc",
+    "cbf_csv_write_map", "cbf_csv_write_peaks", "cbf_csv_write_pairs",
 ]
 
 
@@ -135,6 +136,8 @@ def lib():
               C.c_double, C.c_int32, C.c_double, _dp, C.c_int32, C.c_int32, C.c_double, _ip]
         L.cbf_bifurcation2d_dbscan.argtypes = db
         L.cbf_bifurcation2d_dbscan_ic.argtypes = db
+        L.cbf_bifurcation2d_dbscan_noalloc.argtypes = db[:-1] + [C.c_void_p, C.c_void_p]
+        L.cbf_bifurcation2d_dbscan_noalloc.restype = C.c_int32
         lle = [C.c_int32, C.c_double, C.c_double, C.c_int32, C.c_double, C.c_double, _dp, C.c_int32,
                _dp, _ip, C.c_int32, C.c_double, C.c_double, _dp, C.c_int32, C.c_int64, _dp]
         for f in ("cbf_lle1d", "cbf_lle1d_ic", "cbf_lle2d", "cbf_lle2d_ic"):

@@ -430,7 +430,70 @@ cudaError_t launch_bif_s(const DevJob& J, void* d_out, int* d_aux, cudaStream_t 
     }
 }
 
+template <class S, int TASK>
+cudaError_t launch_bif_prealloc_t(const DevJob& J, void* d_out, double* scratch, size_t scratchBytes,
+                                  int* err, cudaStream_t s)
+{
+    const long long nTiles = (J.nPoints + 31) / 32;
+    if (nTiles == 0) return cudaSuccess;
+    const int bitWords = (TASK == CBF_TASK_DBSCAN) ? (J.peakCap + 31) / 32 : 0;
+    const size_t smemBytes = (size_t)kBifWarps * 2 * bitWords * sizeof(unsigned);
+    auto kern = bif_kernel<S, TASK>;
+    cudaError_t e;
+    if (smemBytes > 48 * 1024) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBytes);
+        if (e != cudaSuccess) return e;
+    }
+    int dev = 0, sms = 0, perSm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, kBifThreads, smemBytes)) != cudaSuccess)
+        return e;
+    if (perSm < 1) return cudaErrorInvalidConfiguration;
+    const size_t perBlock = (size_t)kBifThreads * J.peakCap * sizeof(double) *
+                            (TASK == CBF_TASK_DBSCAN ? 2 : 1);
+    long long blocks = (nTiles + kBifWarps - 1) / kBifWarps;
+    const long long resident = (long long)sms * perSm;
+    if (blocks > resident) blocks = resident;
+    const long long fit = (long long)(scratchBytes / perBlock);
+    if (fit < 1) return cudaErrorInvalidValue;
+    if (blocks > fit) blocks = fit;
+    double* scrInt = (TASK == CBF_TASK_DBSCAN) ? scratch + (size_t)blocks * kBifThreads * J.peakCap : nullptr;
+    kern<<<(unsigned)blocks, kBifThreads, smemBytes, s>>>(J, d_out, nullptr, scratch, scrInt, bitWords, err);
+    note_launch();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    int hostErr = 0;
+    if ((e = cudaMemcpyAsync(&hostErr, err, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+    return hostErr ? cudaErrorAssert : cudaSuccess;
+}
+
+template <class S>
+cudaError_t launch_bif_prealloc_s(const DevJob& J, void* d_out, double* scratch, size_t scratchBytes,
+                                  int* err, cudaStream_t s)
+{
+    switch (J.task) {
+    case CBF_TASK_KDE: return launch_bif_prealloc_t<S, CBF_TASK_KDE>(J, d_out, scratch, scratchBytes, err, s);
+    case CBF_TASK_DBSCAN: return launch_bif_prealloc_t<S, CBF_TASK_DBSCAN>(J, d_out, scratch, scratchBytes, err, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+static_assert(kBifThreads == kBifBlockThreads, "block size shared with other translation units");
+
 }  // namespace
+
+cudaError_t launch_bif_prealloc(const DevJob& J, void* d_out, double* scratch, size_t scratchBytes,
+                                int* err, cudaStream_t s)
+{
+    switch (J.system) {
+    case CBF_SYS_MEMRISTIVE5: return launch_bif_prealloc_s<Memristive5>(J, d_out, scratch, scratchBytes, err, s);
+    case CBF_SYS_ROSSLER: return launch_bif_prealloc_s<Rossler>(J, d_out, scratch, scratchBytes, err, s);
+    case CBF_SYS_LORENZ: return launch_bif_prealloc_s<Lorenz>(J, d_out, scratch, scratchBytes, err, s);
+    case CBF_SYS_CHEN: return launch_bif_prealloc_s<Chen>(J, d_out, scratch, scratchBytes, err, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
 
 cudaError_t launch_bif(const DevJob& J, void* d_out, int* d_aux, cudaStream_t s)
 {

@@ -400,6 +400,11 @@ cbf_status lle(bool ic_sweep, int dims, int32_t system, double tMax, double NT, 
 }
 
 }  // namespace
+
+cbf_status lower_job_for(const cbf_job* job, DevJob* d) { return lower_job(job, d); }
+cbf_status report_error(cbf_status st, const char* message) { return fail(st, "%s", message); }
+cbf_status report_cuda_error(cudaError_t e, const char* where) { return cuda_fail(e, where); }
+
 }  // namespace cbf
 
 using namespace cbf;

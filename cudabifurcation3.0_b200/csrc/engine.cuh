@@ -132,10 +132,23 @@ __device__ __forceinline__ void lle_seed(long long g, long long seedChunk, doubl
 // Kernel launch bookkeeping (defined in capi.cu).
 void note_launch(unsigned n = 1);
 
+// Threads per block of the fused bifurcation kernel (bif.cu).
+constexpr int kBifBlockThreads = 128;
+
 // Launchers (defined in lle.cu / bif.cu / probes.cu).  All return a CUDA error.
 cudaError_t launch_lle(const DevJob& J, double* d_out, cudaStream_t s);
 cudaError_t launch_bif(const DevJob& J, void* d_out, int* d_aux, cudaStream_t s);
 cudaError_t launch_grid_coords(const DevJob& J, double* d_out, cudaStream_t s);
 cudaError_t launch_lle_seeds(const DevJob& J, double* d_out, cudaStream_t s);
+// KDE/DBSCAN with caller-provided scratch (no allocation): `scratch` holds
+// `scratchBytes` of peak buffers, `err` one int that must be zero on entry.
+// Synchronises `s` to read `err`.
+cudaError_t launch_bif_prealloc(const DevJob& J, void* d_out, double* scratch, size_t scratchBytes,
+                                int* err, cudaStream_t s);
+
+// Job lowering and error reporting shared with other translation units (capi.cu).
+cbf_status lower_job_for(const cbf_job* job, DevJob* d);
+cbf_status report_error(cbf_status st, const char* message);
+cbf_status report_cuda_error(cudaError_t e, const char* where);
 
 }  // namespace cbf

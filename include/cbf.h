@@ -200,6 +200,28 @@ cbf_status cbf_lle2d_ic(int32_t system, double tMax, double NT, int32_t nPts, do
                         double transientTime, const double* values, int32_t amountOfValues,
                         int64_t seedChunk, double* out);
 
+/* DBSCAN cluster-count map that allocates no device memory.  No counterpart in
+ * the reference.  For callers that cannot call cudaMalloc: programs whose device
+ * memory belongs to another allocator (a framework's pool, a fixed budget), and
+ * latency-critical loops that cannot afford an allocation's implicit
+ * synchronisation or an out-of-memory failure mid-run.  Arguments as
+ * cbf_bifurcation2d_dbscan (ic/ranges/indices/values are host arrays); d_out is
+ * caller-owned device memory of nPts*nPts int32; runs on `stream` and returns
+ * when the map is complete.  Scratch: a fixed 64 MiB device array inside the
+ * library (held by every GPU that loads it until exit); maps whose
+ * min(maxAmountOfPeaks, record/2) exceeds 32 767 peaks per point are rejected with
+ * CBF_ERR_INVALID_ARG.  The first call on a device looks up the array's device
+ * address, so make it before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller. */
+cbf_status cbf_bifurcation2d_dbscan_noalloc(int32_t system, double tMax, int32_t nPts, double h,
+                                            int32_t amountOfInitialConditions,
+                                            const double* initialConditions, const double* ranges,
+                                            const int32_t* indicesOfMutVars, int32_t writableVar,
+                                            double maxValue, int32_t maxAmountOfPeaks,
+                                            double transientTime, const double* values,
+                                            int32_t amountOfValues, int32_t preScaller, double eps,
+                                            int32_t* d_out, void* stream);
+
 /* Generic host-buffer form of cbf_run: copies results into host memory. */
 cbf_status cbf_run_host(const cbf_job* job, void* out, void* aux);
 
