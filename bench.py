@@ -378,6 +378,7 @@ def main(argv=None) -> int:
     spp = steps_per_point(w)
 
     probe = cbf.probe_fp64_peak(300.0)  # TFLOP/s, FMA = 2 flops
+    variant, trial_ms = cbf.autotune(job)  # picks the LLE kernel shape for this device
 
     stream = torch.cuda.Stream()
     out = torch.empty(n, dtype=torch.float64, device="cuda")
@@ -464,7 +465,9 @@ def main(argv=None) -> int:
                        "transient": w["transientTime"], "eps": w["lleEps"],
                        "steps_per_point": spp, "points_per_rank": n,
                        "cache": "L2 flushed (256 MB write) before every timed map; inputs are scalars",
-                       "parallelism": f"{world} independent c-stripes, one per GPU"},
+                       "parallelism": f"{world} independent c-stripes, one per GPU",
+                       "lle_kernel_variant": variant,
+                       "autotune_trial_ms": [round(float(x), 3) for x in trial_ms]},
             "e2e": {"value": e2e_value, "unit": "points/s", "h2d_bytes_per_step": C.sizeof(cbf.Job),
                     "d2h_bytes_per_step": n * 8, "matches_device_api": bool(same)},
             "roofline": roof,

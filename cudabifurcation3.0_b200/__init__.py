@@ -40,7 +40,8 @@ EXPORTS = [
     "cbf_bifurcation2d_kde_ic", "cbf_bifurcation2d_dbscan", "cbf_bifurcation2d_dbscan_ic",
     "cbf_lle1d", "cbf_lle1d_ic", "cbf_lle2d", "cbf_lle2d_ic", "cbf_run_host",
     "cbf_grid_coordinates", "cbf_probe_fp64_peak", "cbf_probe_expf_zero",
-    "cbf_divergence_threshold", "cbf_lle_seeds", "cbf_bifurcation2d_dbscan_noalloc",
+    "cbf_divergence_threshold", "cbf_lle_seeds", "cbf_autotune", "cbf_set_lle_variant",
+    "cbf_get_lle_variant", "cbf_bifurcation2d_dbscan_noalloc",
     "cbf_csv_write_map", "cbf_csv_write_peaks", "cbf_csv_write_pairs",
 ]
 
@@ -118,6 +119,12 @@ def lib():
         L.cbf_run.argtypes = [C.POINTER(Job), C.c_void_p, C.c_void_p, C.c_void_p]
         L.cbf_run_host.argtypes = [C.POINTER(Job), C.c_void_p, C.c_void_p]
         L.cbf_grid_coordinates.argtypes = [C.POINTER(Job), _dp]
+        L.cbf_autotune.argtypes = [C.POINTER(Job), _ip, _dp]
+        L.cbf_autotune.restype = C.c_int32
+        L.cbf_set_lle_variant.argtypes = [C.c_int32, C.c_int32]
+        L.cbf_set_lle_variant.restype = C.c_int32
+        L.cbf_get_lle_variant.argtypes = [C.c_int32]
+        L.cbf_get_lle_variant.restype = C.c_int32
         L.cbf_lle_seeds.argtypes = [C.POINTER(Job), _dp]
         L.cbf_lle_seeds.restype = C.c_int32
         L.cbf_probe_fp64_peak.argtypes = [C.c_double, _dp]
@@ -248,6 +255,21 @@ def grid_coordinates(job: Job) -> np.ndarray:
     out = np.zeros((n, 2), np.float64)
     check(lib().cbf_grid_coordinates(C.byref(job), out.ctypes.data_as(_dp)))
     return out
+
+
+NUM_LLE_VARIANTS = 5
+
+
+def autotune(job: Job):
+    """Time every LLE kernel shape on a short copy of `job`; returns (chosen, ms[])."""
+    chosen = C.c_int32(0)
+    ms = np.zeros(NUM_LLE_VARIANTS, np.float64)
+    check(lib().cbf_autotune(C.byref(job), C.byref(chosen), ms.ctypes.data_as(_dp)))
+    return int(chosen.value), ms
+
+
+def set_lle_variant(system, variant: int) -> None:
+    check(lib().cbf_set_lle_variant(_sys(system), variant))
 
 
 def lle_seeds(job: Job) -> np.ndarray:

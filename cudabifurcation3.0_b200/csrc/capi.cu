@@ -98,7 +98,27 @@ cbf_status library_stream(cudaStream_t* s)
     return CBF_OK;
 }
 
+// Chosen LLE kernel shape per device and system (-1: default shape 0).
+std::atomic<int> g_lle_variant[64][CBF_NUM_SYSTEMS];
+std::once_flag g_variant_init;
+
+void init_variants()
+{
+    for (int d = 0; d < 64; ++d)
+        for (int k = 0; k < CBF_NUM_SYSTEMS; ++k) g_lle_variant[d][k].store(-1);
+}
+
 }  // namespace
+
+int lle_variant_for(int system)
+{
+    std::call_once(g_variant_init, init_variants);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    if (system < 0 || system >= CBF_NUM_SYSTEMS) return 0;
+    const int v = g_lle_variant[dev][system].load();
+    return v < 0 ? 0 : v;
+}
 
 void note_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
@@ -624,6 +644,76 @@ cbf_status cbf_grid_coordinates(const cbf_job* job, double* out_host)
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     cudaFreeAsync(dd, s);
     if (e != cudaSuccess) return cuda_fail(e, "grid coordinates");
+    return CBF_OK;
+}
+
+cbf_status cbf_set_lle_variant(int32_t system, int32_t variant)
+{
+    std::call_once(g_variant_init, init_variants);
+    if (system < 0 || system >= CBF_NUM_SYSTEMS) return fail(CBF_ERR_UNKNOWN_SYSTEM, "unknown system %d", system);
+    if (variant < -1 || variant >= kNumLleVariants) return fail(CBF_ERR_INVALID_ARG, "variant %d out of range", variant);
+    int dev = 0;
+    CBF_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(CBF_ERR_INVALID_ARG, "device %d out of range", dev);
+    g_lle_variant[dev][system].store(variant);
+    return CBF_OK;
+}
+
+int32_t cbf_get_lle_variant(int32_t system) { return lle_variant_for(system); }
+
+// Times every LLE kernel shape on a shortened copy of the job: the job's first
+// points (two full waves of the most occupying shape), its transient cut to 1024
+// steps, 8 renormalisation intervals of at most 1000 steps.  Per-step cost does
+// not depend on where in the trajectory a step falls, so the ranking carries over.
+cbf_status cbf_autotune(const cbf_job* job, int32_t* chosen, double* msPerVariant)
+{
+    std::call_once(g_variant_init, init_variants);
+    DevJob d;
+    cbf_status st = lower_job(job, &d);
+    if (st != CBF_OK) return st;
+    if (d.task != CBF_TASK_LLE) return fail(CBF_ERR_INVALID_ARG, "cbf_autotune tunes LLE jobs");
+    int dev = 0, sms = 0;
+    CBF_CUDA(cudaGetDevice(&dev));
+    CBF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    DevJob t = d;
+    const long long trial = (long long)sms * 2048 * 2 * 2;
+    if (t.nPoints > trial) t.nPoints = trial;
+    if (t.nSkip > 1024) t.nSkip = 1024;
+    if (t.nRecord > 8) t.nRecord = 8;
+    if (t.nRecord < 1) t.nRecord = 1;
+    if (t.nNT > 1000) t.nNT = 1000;
+    if (t.nNT < 1) t.nNT = 1;
+    cudaStream_t s;
+    if ((st = library_stream(&s)) != CBF_OK) return st;
+    double* out = nullptr;
+    CBF_CUDA(cudaMallocAsync((void**)&out, (size_t)t.nPoints * sizeof(double), s));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 0.f;
+    int bestV = 0;
+    cudaError_t e = cudaSuccess;
+    for (int v = 0; v < kNumLleVariants && e == cudaSuccess; ++v) {
+        e = launch_lle_variant(t, out, s, v);  // warm-up (module load, caches)
+        if (e != cudaSuccess) break;
+        cudaEventRecord(e0, s);
+        e = launch_lle_variant(t, out, s, v);
+        cudaEventRecord(e1, s);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+        if (msPerVariant) msPerVariant[v] = ms;
+        if (v == 0 || ms < best) {
+            best = ms;
+            bestV = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFreeAsync(out, s);
+    if (e != cudaSuccess) return cuda_fail(e, "autotune");
+    if (dev >= 0 && dev < 64) g_lle_variant[dev][d.system].store(bestV);
+    if (chosen) *chosen = bestV;
     return CBF_OK;
 }
 

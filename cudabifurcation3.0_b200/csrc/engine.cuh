@@ -137,6 +137,11 @@ constexpr int kBifBlockThreads = 128;
 
 // Launchers (defined in lle.cu / bif.cu / probes.cu).  All return a CUDA error.
 cudaError_t launch_lle(const DevJob& J, double* d_out, cudaStream_t s);
+// LLE kernel shapes (lle.cu): the autotuner's search space.
+constexpr int kNumLleVariants = 5;
+cudaError_t launch_lle_variant(const DevJob& J, double* d_out, cudaStream_t s, int variant);
+// The shape cbf_run uses for `system` on the current device (capi.cu).
+int lle_variant_for(int system);
 cudaError_t launch_bif(const DevJob& J, void* d_out, int* d_aux, cudaStream_t s);
 cudaError_t launch_grid_coords(const DevJob& J, double* d_out, cudaStream_t s);
 cudaError_t launch_lle_seeds(const DevJob& J, double* d_out, cudaStream_t s);

@@ -1,11 +1,14 @@
 // Largest Lyapunov exponent maps (Benettin two-trajectory method).
 //
 // Semantics: LLEKernelCUDA / LLEKernelICCUDA, Library/cudaLibrary.cu:666-908.
-// Design (B200): one thread owns one grid point for its whole life; the base
-// trajectory x and the perturbed trajectory y live in registers and are advanced
-// in the same loop body, giving the scheduler two independent FP64 dependency
-// chains per thread (the reference integrates x for NT/h steps, then y, each from
-// shared memory).  Parameter-only quantities are hoisted once per point.
+// Design (B200): a thread owns PPT grid points (1 or 2) for their whole life;
+// for each point the base trajectory x and the perturbed trajectory y live in
+// registers and are advanced in the same loop body, giving the scheduler 2*PPT
+// independent FP64 dependency chains per thread (the reference integrates x for
+// NT/h steps, then y, each from shared memory).  Parameter-only quantities are
+// hoisted once per point.  The kernel is instantiated in a few shapes (points per
+// thread, block size, register cap); the autotuner in capi.cu times them on the
+// device and picks one per system.
 //
 // Divergence: the reference checks |x[0]| against maxValue after EVERY step and
 // stops that integration at the first violation (loopCalculateDiscreteModel,
@@ -21,121 +24,176 @@ namespace cbf {
 
 namespace {
 
-constexpr int kLleThreads = 128;
 constexpr int kTransientChunk = 512;
 
-template <class S>
-__device__ __forceinline__ void copy_state(double (&d)[S::DIM], const double (&s)[S::DIM])
+template <int D>
+__device__ __forceinline__ void copy_state(double (&d)[D], const double (&s)[D])
 {
 #pragma unroll
-    for (int i = 0; i < S::DIM; ++i) d[i] = s[i];
+    for (int i = 0; i < D; ++i) d[i] = s[i];
 }
 
-// loopCalculateDiscreteModel(x, values, h, n, 1, 0, maxValue, nullptr) for one
-// trajectory: n steps, stop after the first step with |x[0]| past the bound.
-template <class S>
-__device__ __forceinline__ void run_checked(double (&x)[S::DIM], const typename S::Coef& c,
-                                            int n, const DevJob& J)
+// loopCalculateDiscreteModel(x, values, h, n, 1, 0, maxValue, nullptr) for PPT
+// independent points: n steps each, a point stops after its first step with
+// |x[0]| past the bound and stays stopped for the rest of the call.
+template <class S, int PPT>
+__device__ __forceinline__ void run_checked(double (&x)[PPT][S::DIM],
+                                            const typename S::Coef (&c)[PPT], int n,
+                                            const DevJob& J)
 {
     if (!J.checkDiv) {
-#pragma unroll 4
-        for (int i = 0; i < n; ++i) S::step(x, c);
+#pragma unroll 2
+        for (int i = 0; i < n; ++i) {
+#pragma unroll
+            for (int j = 0; j < PPT; ++j) S::step(x[j], c[j]);
+        }
         return;
     }
+    bool alive[PPT];
+#pragma unroll
+    for (int j = 0; j < PPT; ++j) alive[j] = true;
     for (int done = 0; done < n; done += kTransientChunk) {
         const int m = min(kTransientChunk, n - done);
-        double x0[S::DIM];
-        copy_state<S>(x0, x);
-        unsigned mx = 0;
-#pragma unroll 4
-        for (int i = 0; i < m; ++i) {
-            S::step(x, c);
-            mx = max(mx, abs_hi(x[0]));
+        double x0[PPT][S::DIM];
+        unsigned mx[PPT];
+#pragma unroll
+        for (int j = 0; j < PPT; ++j) {
+            copy_state<S::DIM>(x0[j], x[j]);
+            mx[j] = 0;
         }
-        if (mx >= J.divHi) {
-            copy_state<S>(x, x0);
-            for (int i = 0; i < m; ++i) {
-                S::step(x, c);
-                if (diverged(x[0], J.divThresh)) return;
+#pragma unroll 2
+        for (int i = 0; i < m; ++i) {
+#pragma unroll
+            for (int j = 0; j < PPT; ++j) {
+                S::step(x[j], c[j]);
+                mx[j] = max(mx[j], abs_hi(x[j][0]));
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < PPT; ++j) {
+            if (!alive[j]) {
+                copy_state<S::DIM>(x[j], x0[j]);  // stopped earlier: state frozen
+            } else if (mx[j] >= J.divHi) {
+                copy_state<S::DIM>(x[j], x0[j]);
+                for (int i = 0; i < m; ++i) {
+                    S::step(x[j], c[j]);
+                    if (diverged(x[j][0], J.divThresh)) {
+                        alive[j] = false;
+                        break;
+                    }
+                }
             }
         }
     }
 }
 
 // The two NT-interval integrations of one renormalisation block
-// (cudaLibrary.cu:748-754), interleaved; each stops at its own first violation.
-template <class S>
-__device__ __forceinline__ void run_pair(double (&x)[S::DIM], double (&y)[S::DIM],
-                                         const typename S::Coef& c, int n, const DevJob& J)
+// (cudaLibrary.cu:748-754) for PPT points, interleaved; each trajectory stops at
+// its own first violation within the interval.
+template <class S, int PPT>
+__device__ __forceinline__ void run_pair(double (&x)[PPT][S::DIM], double (&y)[PPT][S::DIM],
+                                         const typename S::Coef (&c)[PPT], int n, const DevJob& J)
 {
     if (!J.checkDiv) {
 #pragma unroll 2
         for (int i = 0; i < n; ++i) {
-            S::step(x, c);
-            S::step(y, c);
+#pragma unroll
+            for (int j = 0; j < PPT; ++j) {
+                S::step(x[j], c[j]);
+                S::step(y[j], c[j]);
+            }
         }
         return;
     }
-    double x0[S::DIM], y0[S::DIM];
-    copy_state<S>(x0, x);
-    copy_state<S>(y0, y);
-    unsigned mx = 0, my = 0;
+    double x0[PPT][S::DIM], y0[PPT][S::DIM];
+    unsigned mx[PPT], my[PPT];
+#pragma unroll
+    for (int j = 0; j < PPT; ++j) {
+        copy_state<S::DIM>(x0[j], x[j]);
+        copy_state<S::DIM>(y0[j], y[j]);
+        mx[j] = my[j] = 0;
+    }
 #pragma unroll 2
     for (int i = 0; i < n; ++i) {
-        S::step(x, c);
-        S::step(y, c);
-        mx = max(mx, abs_hi(x[0]));
-        my = max(my, abs_hi(y[0]));
-    }
-    if (mx >= J.divHi) {
-        copy_state<S>(x, x0);
-        for (int i = 0; i < n; ++i) {
-            S::step(x, c);
-            if (diverged(x[0], J.divThresh)) break;
+#pragma unroll
+        for (int j = 0; j < PPT; ++j) {
+            S::step(x[j], c[j]);
+            S::step(y[j], c[j]);
+            mx[j] = max(mx[j], abs_hi(x[j][0]));
+            my[j] = max(my[j], abs_hi(y[j][0]));
         }
     }
-    if (my >= J.divHi) {
-        copy_state<S>(y, y0);
-        for (int i = 0; i < n; ++i) {
-            S::step(y, c);
-            if (diverged(y[0], J.divThresh)) break;
+#pragma unroll
+    for (int j = 0; j < PPT; ++j) {
+        if (mx[j] >= J.divHi) {
+            copy_state<S::DIM>(x[j], x0[j]);
+            for (int i = 0; i < n; ++i) {
+                S::step(x[j], c[j]);
+                if (diverged(x[j][0], J.divThresh)) break;
+            }
+        }
+        if (my[j] >= J.divHi) {
+            copy_state<S::DIM>(y[j], y0[j]);
+            for (int i = 0; i < n; ++i) {
+                S::step(y[j], c[j]);
+                if (diverged(y[j][0], J.divThresh)) break;
+            }
         }
     }
 }
 
-template <class S, bool IC>
-__global__ void __launch_bounds__(kLleThreads) lle_kernel(const DevJob J, double* __restrict__ out)
+template <class S, bool IC, int PPT, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) lle_kernel(const DevJob J, double* __restrict__ out)
 {
     constexpr int D = S::DIM;
+    const long long nq = (J.nPoints + PPT - 1) / PPT;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < J.nPoints; p += stride) {
-        const long long g = J.firstPoint + p;
-        double x[D], v[CBF_MAX_VALUES];
-        setup_point<D>(J, g, x, v);
-        const typename S::Coef c = S::prep(v, J.h);
-
-        double z[D];
-        lle_seed<D, IC>(g, J.seedChunk, z);
-
-        run_checked<S>(x, c, J.nSkip, J);
-
-        double y[D];
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += stride) {
+        double x[PPT][D], y[PPT][D];
+        typename S::Coef c[PPT];
 #pragma unroll
-        for (int i = 0; i < D; ++i) y[i] = z[i] * J.lleEps + x[i];
-
-        double result = 0;
-        for (int b = 0; b < J.nRecord; ++b) {
-            run_pair<S>(x, y, c, J.nNT, J);
-            double t = 0;
-#pragma unroll
-            for (int l = 0; l < D; ++l) t += (x[l] - y[l]) * (x[l] - y[l]);
-            t = sqrt(t) / J.lleEps;
-            result += log(t);
-            if (t != 0) t = (1 / t);
-#pragma unroll
-            for (int j = 0; j < D; ++j) y[j] = x[j] - ((x[j] - y[j]) * t);
+        for (int j = 0; j < PPT; ++j) {
+            long long p = q * PPT + j;
+            if (p >= J.nPoints) p = J.nPoints - 1;  // tail lane repeats a point, never stores it
+            double v[CBF_MAX_VALUES];
+            setup_point<D>(J, J.firstPoint + p, x[j], v);
+            c[j] = S::prep(v, J.h);
         }
-        out[p] = result / J.tMax;
+
+        run_checked<S, PPT>(x, c, J.nSkip, J);
+
+#pragma unroll
+        for (int j = 0; j < PPT; ++j) {
+            long long p = q * PPT + j;
+            if (p >= J.nPoints) p = J.nPoints - 1;
+            double z[D];
+            lle_seed<D, IC>(J.firstPoint + p, J.seedChunk, z);
+#pragma unroll
+            for (int i = 0; i < D; ++i) y[j][i] = z[i] * J.lleEps + x[j][i];
+        }
+
+        double result[PPT];
+#pragma unroll
+        for (int j = 0; j < PPT; ++j) result[j] = 0;
+        for (int b = 0; b < J.nRecord; ++b) {
+            run_pair<S, PPT>(x, y, c, J.nNT, J);
+#pragma unroll
+            for (int j = 0; j < PPT; ++j) {
+                double t = 0;
+#pragma unroll
+                for (int l = 0; l < D; ++l) t += (x[j][l] - y[j][l]) * (x[j][l] - y[j][l]);
+                t = sqrt(t) / J.lleEps;
+                result[j] += log(t);
+                if (t != 0) t = (1 / t);
+#pragma unroll
+                for (int i = 0; i < D; ++i) y[j][i] = x[j][i] - ((x[j][i] - y[j][i]) * t);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < PPT; ++j) {
+            const long long p = q * PPT + j;
+            if (p < J.nPoints) out[p] = result[j] / J.tMax;
+        }
     }
 }
 
@@ -163,34 +221,60 @@ cudaError_t launch_seeds_d(const DevJob& J, double* d_out, cudaStream_t s)
     return cudaGetLastError();
 }
 
-template <class S, bool IC>
-cudaError_t launch_lle_t(const DevJob& J, double* d_out, cudaStream_t s)
+template <class S, bool IC, int PPT, int THREADS, int MINB>
+cudaError_t launch_variant(const DevJob& J, double* d_out, cudaStream_t s)
 {
-    const long long blocks = (J.nPoints + kLleThreads - 1) / kLleThreads;
+    const long long nq = (J.nPoints + PPT - 1) / PPT;
+    const long long blocks = (nq + THREADS - 1) / THREADS;
     const unsigned grid = (unsigned)(blocks < (1ll << 30) ? blocks : (1ll << 30));
     if (grid == 0) return cudaSuccess;
-    lle_kernel<S, IC><<<grid, kLleThreads, 0, s>>>(J, d_out);
+    lle_kernel<S, IC, PPT, THREADS, MINB><<<grid, THREADS, 0, s>>>(J, d_out);
     note_launch();
     return cudaGetLastError();
 }
 
-template <class S>
-cudaError_t launch_lle_s(const DevJob& J, double* d_out, cudaStream_t s)
+// The kernel shapes the autotuner chooses from: {points per thread, threads per
+// block, minimum resident blocks per SM (a register cap for the compiler)}.
+//   0: 1 pt, 128 thr, >= 8 blocks/SM  (<= 64 registers, 32 warps/SM)  default
+//   1: 1 pt, 128 thr, no cap
+//   2: 1 pt, 256 thr, >= 4 blocks/SM  (<= 64 registers)
+//   3: 2 pt, 128 thr, >= 4 blocks/SM  (<= 128 registers, 4 chains per thread)
+//   4: 2 pt, 128 thr, >= 3 blocks/SM  (<= 170 registers)
+template <class S, bool IC>
+cudaError_t launch_lle_v(const DevJob& J, double* d_out, cudaStream_t s, int variant)
 {
-    return J.sweepIC ? launch_lle_t<S, true>(J, d_out, s) : launch_lle_t<S, false>(J, d_out, s);
+    switch (variant) {
+    case 1: return launch_variant<S, IC, 1, 128, 1>(J, d_out, s);
+    case 2: return launch_variant<S, IC, 1, 256, 4>(J, d_out, s);
+    case 3: return launch_variant<S, IC, 2, 128, 4>(J, d_out, s);
+    case 4: return launch_variant<S, IC, 2, 128, 3>(J, d_out, s);
+    default: return launch_variant<S, IC, 1, 128, 8>(J, d_out, s);
+    }
+}
+
+template <class S>
+cudaError_t launch_lle_s(const DevJob& J, double* d_out, cudaStream_t s, int variant)
+{
+    return J.sweepIC ? launch_lle_v<S, true>(J, d_out, s, variant)
+                     : launch_lle_v<S, false>(J, d_out, s, variant);
 }
 
 }  // namespace
 
-cudaError_t launch_lle(const DevJob& J, double* d_out, cudaStream_t s)
+cudaError_t launch_lle_variant(const DevJob& J, double* d_out, cudaStream_t s, int variant)
 {
     switch (J.system) {
-    case CBF_SYS_MEMRISTIVE5: return launch_lle_s<Memristive5>(J, d_out, s);
-    case CBF_SYS_ROSSLER: return launch_lle_s<Rossler>(J, d_out, s);
-    case CBF_SYS_LORENZ: return launch_lle_s<Lorenz>(J, d_out, s);
-    case CBF_SYS_CHEN: return launch_lle_s<Chen>(J, d_out, s);
+    case CBF_SYS_MEMRISTIVE5: return launch_lle_s<Memristive5>(J, d_out, s, variant);
+    case CBF_SYS_ROSSLER: return launch_lle_s<Rossler>(J, d_out, s, variant);
+    case CBF_SYS_LORENZ: return launch_lle_s<Lorenz>(J, d_out, s, variant);
+    case CBF_SYS_CHEN: return launch_lle_s<Chen>(J, d_out, s, variant);
     default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t launch_lle(const DevJob& J, double* d_out, cudaStream_t s)
+{
+    return launch_lle_variant(J, d_out, s, lle_variant_for(J.system));
 }
 
 cudaError_t launch_lle_seeds(const DevJob& J, double* d_out, cudaStream_t s)

@@ -120,6 +120,18 @@ cbf_status cbf_validate(const cbf_job* job);
  * Scratch for KDE/DBSCAN is taken from the stream-ordered allocator. */
 cbf_status cbf_run(const cbf_job* job, void* d_out, void* d_aux, void* stream);
 
+/* ---- autotuning ------------------------------------------------------ */
+/* The LLE kernel exists in CBF_NUM_LLE_VARIANTS shapes (points per thread 1|2,
+ * threads per block, register cap).  cbf_autotune times all of them on a
+ * shortened copy of `job` on the current device and makes the fastest the one
+ * cbf_run (and every LLE entry point) uses for job->system on this device.
+ * msPerVariant (optional) receives each shape's trial time. */
+#define CBF_NUM_LLE_VARIANTS 5
+cbf_status cbf_autotune(const cbf_job* job, int32_t* chosenVariant, double* msPerVariant);
+/* Set (variant >= 0) or reset to the default (-1) the shape for a system. */
+cbf_status cbf_set_lle_variant(int32_t system, int32_t variant);
+int32_t cbf_get_lle_variant(int32_t system);
+
 /* ---- host-buffer entry points (drop-in for hostLibrary.cuh) ---------- */
 /* bifurcation1D, hostLibrary.cuh:29-42 / hostLibrary.cu:7-158.
  * outPeaks[k*peakCapacity + j], outCounts[k]; peakCapacity >= record/2. */
