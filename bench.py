@@ -8,7 +8,7 @@ reference, seed chunk 200000).  FP64 throughout.  Inputs are synthetic by
 nature: the grid itself.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-    python bench.py --workload lorenz-dbscan-1024|lorenz-kde256-1024|lorenz-kde-1024|rossler-bif1d-1000
+    python bench.py --workload lorenz-dbscan-1024|lorenz-kde256-1024|lorenz-kde-1024|rossler-bif1d-1000|batch64
 
 Multi-GPU (torchrun, one rank per GPU): every rank computes its own 2048x2048 map
 of one c-stripe (weak scaling, no data-path collective); time = max over ranks.
@@ -71,6 +71,115 @@ SECONDARY = {
                                tMax=500.0, transientTime=1000.0, maxValue=1e4, writableVar=0,
                                preScaller=1, task=0),
 }
+
+
+BATCH_SEED = 20240101
+_BATCH_SYSTEMS = {
+    "rossler": dict(values=[0.5, 0.2, 0.2, 5.7], idxMut=[1, 2], ranges=[0.05, 0.35, 0.05, 0.35]),
+    "lorenz": dict(values=[0.5, 10.0, 28.0, 8.0 / 3.0], idxMut=[1, 2], ranges=[5.0, 20.0, 20.0, 200.0]),
+    "chen": dict(values=[0.5, 35.0, 3.0, 28.0], idxMut=[1, 3], ranges=[30.0, 45.0, 20.0, 30.0]),
+}
+
+
+def batch_specs(seed: int = BATCH_SEED, n: int = 64):
+    """The ragged-batch configuration: n jobs drawn from `seed` -- system in
+    {Rossler, Lorenz, Chen}, task in {2-D KDE, 2-D DBSCAN, 2-D LLE}, grid side
+    U{64..1024}, record U[200, 5000] time units, h U[0.001, 0.01], transient 100."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for _ in range(n):
+        system = ["rossler", "lorenz", "chen"][rng.integers(0, 3)]
+        task = ["kde", "dbscan", "lle"][rng.integers(0, 3)]
+        side = int(rng.integers(64, 1025))
+        record = float(rng.uniform(200.0, 5000.0))
+        h = float(rng.uniform(0.001, 0.01))
+        spec = dict(system=system, nPts=side, ic=[0.1, 0.1, 0.1], h=h, tMax=record,
+                    transientTime=100.0, maxValue=1e4, **_BATCH_SYSTEMS[system])
+        if task == "lle":
+            spec.update(task=3, NT=0.5, lleEps=1e-8)
+        elif task == "kde":
+            spec.update(task=1, maxAmountOfPeaks=1000, kdeSampling=4, kdeI1=-60.0, kdeI2=60.0,
+                        kdeH=0.5)
+        else:
+            spec.update(task=2, maxAmountOfPeaks=1000, dbscanEps=0.05)
+        specs.append(spec)
+    return specs
+
+
+def run_batch(args) -> int:
+    """Ragged batch: the seeded 64 jobs in one persistent launch (CUDA graph) vs one by one."""
+    import torch
+    torch.cuda.set_device(0)
+    cbf = load_cbf()
+    specs = batch_specs()
+    jobs, outs = [], []
+    for sp in specs:
+        sp = dict(sp)
+        task = sp.pop("task")
+        jobs.append(cbf.make_job(task=task, **sp))
+        n = sp["nPts"] ** 2
+        outs.append(torch.empty(n, dtype=torch.float64 if task == cbf.TASK_LLE else torch.int32,
+                                device="cuda"))
+    batch = cbf.Batch(jobs, [o.data_ptr() for o in outs])
+    stream = torch.cuda.Stream()
+    s = stream.cuda_stream
+    bps, tune_ms = batch.autotune(s)
+    batch.capture(s)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        batch.launch(s)
+    stream.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    launches0 = cbf.kernel_launches()
+    ms = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        batch.launch(s)
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        stream.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    launches = cbf.kernel_launches() - launches0
+    clocks = sampler.stop()
+    batch.check()
+    got = [o.cpu().numpy().copy() for o in outs]
+    # the same jobs one by one (per-job kernels), timed the same way
+    with torch.cuda.stream(stream):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+    batch.run_sequential(s)
+    with torch.cuda.stream(stream):
+        e1.record(stream)
+    stream.synchronize()
+    seq_ms = e0.elapsed_time(e1)
+    same = all(np.array_equal(a, o.cpu().numpy(), equal_nan=True) for a, o in zip(got, outs))
+    t = statistics.mean(ms)
+    pts = batch.points()
+    line = {"metric": "grid points/s, ragged batch of 64 jobs in one persistent launch",
+            "value": pts / (t / 1e3), "unit": "points/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded job mix)",
+            "config": {"workload": "batch64", "seed": BATCH_SEED, "jobs": len(specs),
+                       "points": pts,
+                       "tasks": {k: sum(1 for sp in specs if sp["task"] == v)
+                                 for k, v in (("lle", 3), ("kde", 1), ("dbscan", 2))},
+                       "cache": "L2 flushed before every timed run",
+                       "blocks_per_sm": bps, "autotune_trial_ms": [round(float(x), 3) for x in tune_ms],
+                       "launch": "one CUDA graph (queue reset + persistent kernel)"},
+            "one_by_one": {"value": pts / (seq_ms / 1e3), "ms": seq_ms,
+                           "speedup_batch_over_one_by_one": seq_ms / t,
+                           "results_identical": bool(same)},
+            "gpu_launches": int(launches), "clocks": clocks, "kernel_ms": ms}
+    print(json.dumps(line), flush=True)
+    batch.close()
+    return 0 if same else 1
 
 
 def load_cbf():
@@ -348,11 +457,13 @@ def main(argv=None) -> int:
     ap.add_argument("--nPts", type=int, default=None, help="override the grid side (testing)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="chen-lle2d-2048",
-                    choices=["chen-lle2d-2048", *SECONDARY])
+                    choices=["chen-lle2d-2048", "batch64", *SECONDARY])
     args = ap.parse_args(argv)
 
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch64":
+        return run_batch(args)
     if args.workload != "chen-lle2d-2048":
         return run_secondary(args, args.workload)
 

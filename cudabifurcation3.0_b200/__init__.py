@@ -41,7 +41,9 @@ EXPORTS = [
     "cbf_lle1d", "cbf_lle1d_ic", "cbf_lle2d", "cbf_lle2d_ic", "cbf_run_host",
     "cbf_grid_coordinates", "cbf_probe_fp64_peak", "cbf_probe_expf_zero",
     "cbf_divergence_threshold", "cbf_lle_seeds", "cbf_autotune", "cbf_set_lle_variant",
-    "cbf_get_lle_variant", "cbf_bifurcation2d_dbscan_noalloc",
+    "cbf_get_lle_variant", "cbf_batch_create", "cbf_batch_destroy", "cbf_batch_points",
+    "cbf_batch_blocks_per_sm", "cbf_batch_run", "cbf_batch_capture", "cbf_batch_launch",
+    "cbf_batch_run_sequential", "cbf_batch_check", "cbf_batch_autotune", "cbf_bifurcation2d_dbscan_noalloc",
     "cbf_csv_write_map", "cbf_csv_write_peaks", "cbf_csv_write_pairs",
 ]
 
@@ -125,6 +127,22 @@ def lib():
         L.cbf_set_lle_variant.restype = C.c_int32
         L.cbf_get_lle_variant.argtypes = [C.c_int32]
         L.cbf_get_lle_variant.restype = C.c_int32
+        L.cbf_batch_create.argtypes = [C.POINTER(Job), C.c_int32, C.POINTER(C.c_void_p),
+                                       C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
+        L.cbf_batch_create.restype = C.c_int32
+        L.cbf_batch_destroy.argtypes = [C.c_void_p]
+        L.cbf_batch_destroy.restype = None
+        L.cbf_batch_points.argtypes = [C.c_void_p]
+        L.cbf_batch_points.restype = C.c_int64
+        L.cbf_batch_blocks_per_sm.argtypes = [C.c_void_p]
+        L.cbf_batch_blocks_per_sm.restype = C.c_int32
+        for f in ("cbf_batch_run", "cbf_batch_capture", "cbf_batch_launch", "cbf_batch_run_sequential"):
+            getattr(L, f).argtypes = [C.c_void_p, C.c_void_p]
+            getattr(L, f).restype = C.c_int32
+        L.cbf_batch_check.argtypes = [C.c_void_p]
+        L.cbf_batch_check.restype = C.c_int32
+        L.cbf_batch_autotune.argtypes = [C.c_void_p, C.c_void_p, _ip, _dp]
+        L.cbf_batch_autotune.restype = C.c_int32
         L.cbf_lle_seeds.argtypes = [C.POINTER(Job), _dp]
         L.cbf_lle_seeds.restype = C.c_int32
         L.cbf_probe_fp64_peak.argtypes = [C.c_double, _dp]
@@ -266,6 +284,60 @@ def autotune(job: Job):
     ms = np.zeros(NUM_LLE_VARIANTS, np.float64)
     check(lib().cbf_autotune(C.byref(job), C.byref(chosen), ms.ctypes.data_as(_dp)))
     return int(chosen.value), ms
+
+
+class Batch:
+    """Many jobs in one persistent launch (cbf_batch_*); outputs are device pointers."""
+
+    def __init__(self, jobs, d_outs, d_auxs=None):
+        n = len(jobs)
+        arr = (Job * n)(*jobs)
+        outs = (C.c_void_p * n)(*[C.c_void_p(p) for p in d_outs])
+        auxs = None
+        if d_auxs is not None:
+            auxs = (C.c_void_p * n)(*[C.c_void_p(p or None) for p in d_auxs])
+        h = C.c_void_p()
+        check(lib().cbf_batch_create(arr, n, outs, auxs, C.byref(h)))
+        self.handle = h
+
+    def points(self) -> int:
+        return int(lib().cbf_batch_points(self.handle))
+
+    def blocks_per_sm(self) -> int:
+        return int(lib().cbf_batch_blocks_per_sm(self.handle))
+
+    def run(self, stream: int = 0):
+        check(lib().cbf_batch_run(self.handle, C.c_void_p(stream or None)))
+
+    def capture(self, stream: int = 0):
+        check(lib().cbf_batch_capture(self.handle, C.c_void_p(stream or None)))
+
+    def launch(self, stream: int = 0):
+        check(lib().cbf_batch_launch(self.handle, C.c_void_p(stream or None)))
+
+    def run_sequential(self, stream: int = 0):
+        check(lib().cbf_batch_run_sequential(self.handle, C.c_void_p(stream or None)))
+
+    def check(self):
+        check(lib().cbf_batch_check(self.handle))
+
+    def autotune(self, stream: int = 0):
+        chosen = C.c_int32(0)
+        ms = np.zeros(8, np.float64)
+        check(lib().cbf_batch_autotune(self.handle, C.c_void_p(stream or None), C.byref(chosen),
+                                       ms.ctypes.data_as(_dp)))
+        return int(chosen.value), ms
+
+    def close(self):
+        if self.handle:
+            lib().cbf_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def set_lle_variant(system, variant: int) -> None:

@@ -422,6 +422,11 @@ cbf_status lle(bool ic_sweep, int dims, int32_t system, double tMax, double NT, 
 }  // namespace
 
 cbf_status lower_job_for(const cbf_job* job, DevJob* d) { return lower_job(job, d); }
+cbf_status run_job_lowered(const DevJob& d, void* d_out, void* d_aux, cudaStream_t s)
+{
+    return run_lowered(d, d_out, d_aux, s);
+}
+cbf_status library_stream_for_batch(cudaStream_t* s) { return library_stream(s); }
 cbf_status report_error(cbf_status st, const char* message) { return fail(st, "%s", message); }
 cbf_status report_cuda_error(cudaError_t e, const char* where) { return cuda_fail(e, where); }
 

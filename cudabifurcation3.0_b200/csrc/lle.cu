@@ -18,129 +18,11 @@
 // word of the exact threshold is the interval replayed from a register snapshot
 // with the exact per-step check.  Results are identical; the common case pays
 // two integer ops per step.
-#include "engine.cuh"
+#include "lle_device.cuh"
 
 namespace cbf {
 
 namespace {
-
-constexpr int kTransientChunk = 512;
-
-template <int D>
-__device__ __forceinline__ void copy_state(double (&d)[D], const double (&s)[D])
-{
-#pragma unroll
-    for (int i = 0; i < D; ++i) d[i] = s[i];
-}
-
-// loopCalculateDiscreteModel(x, values, h, n, 1, 0, maxValue, nullptr) for PPT
-// independent points: n steps each, a point stops after its first step with
-// |x[0]| past the bound and stays stopped for the rest of the call.
-template <class S, int PPT>
-__device__ __forceinline__ void run_checked(double (&x)[PPT][S::DIM],
-                                            const typename S::Coef (&c)[PPT], int n,
-                                            const DevJob& J)
-{
-    if (!J.checkDiv) {
-#pragma unroll 2
-        for (int i = 0; i < n; ++i) {
-#pragma unroll
-            for (int j = 0; j < PPT; ++j) S::step(x[j], c[j]);
-        }
-        return;
-    }
-    bool alive[PPT];
-#pragma unroll
-    for (int j = 0; j < PPT; ++j) alive[j] = true;
-    for (int done = 0; done < n; done += kTransientChunk) {
-        const int m = min(kTransientChunk, n - done);
-        double x0[PPT][S::DIM];
-        unsigned mx[PPT];
-#pragma unroll
-        for (int j = 0; j < PPT; ++j) {
-            copy_state<S::DIM>(x0[j], x[j]);
-            mx[j] = 0;
-        }
-#pragma unroll 2
-        for (int i = 0; i < m; ++i) {
-#pragma unroll
-            for (int j = 0; j < PPT; ++j) {
-                S::step(x[j], c[j]);
-                mx[j] = max(mx[j], abs_hi(x[j][0]));
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < PPT; ++j) {
-            if (!alive[j]) {
-                copy_state<S::DIM>(x[j], x0[j]);  // stopped earlier: state frozen
-            } else if (mx[j] >= J.divHi) {
-                copy_state<S::DIM>(x[j], x0[j]);
-                for (int i = 0; i < m; ++i) {
-                    S::step(x[j], c[j]);
-                    if (diverged(x[j][0], J.divThresh)) {
-                        alive[j] = false;
-                        break;
-                    }
-                }
-            }
-        }
-    }
-}
-
-// The two NT-interval integrations of one renormalisation block
-// (cudaLibrary.cu:748-754) for PPT points, interleaved; each trajectory stops at
-// its own first violation within the interval.
-template <class S, int PPT>
-__device__ __forceinline__ void run_pair(double (&x)[PPT][S::DIM], double (&y)[PPT][S::DIM],
-                                         const typename S::Coef (&c)[PPT], int n, const DevJob& J)
-{
-    if (!J.checkDiv) {
-#pragma unroll 2
-        for (int i = 0; i < n; ++i) {
-#pragma unroll
-            for (int j = 0; j < PPT; ++j) {
-                S::step(x[j], c[j]);
-                S::step(y[j], c[j]);
-            }
-        }
-        return;
-    }
-    double x0[PPT][S::DIM], y0[PPT][S::DIM];
-    unsigned mx[PPT], my[PPT];
-#pragma unroll
-    for (int j = 0; j < PPT; ++j) {
-        copy_state<S::DIM>(x0[j], x[j]);
-        copy_state<S::DIM>(y0[j], y[j]);
-        mx[j] = my[j] = 0;
-    }
-#pragma unroll 2
-    for (int i = 0; i < n; ++i) {
-#pragma unroll
-        for (int j = 0; j < PPT; ++j) {
-            S::step(x[j], c[j]);
-            S::step(y[j], c[j]);
-            mx[j] = max(mx[j], abs_hi(x[j][0]));
-            my[j] = max(my[j], abs_hi(y[j][0]));
-        }
-    }
-#pragma unroll
-    for (int j = 0; j < PPT; ++j) {
-        if (mx[j] >= J.divHi) {
-            copy_state<S::DIM>(x[j], x0[j]);
-            for (int i = 0; i < n; ++i) {
-                S::step(x[j], c[j]);
-                if (diverged(x[j][0], J.divThresh)) break;
-            }
-        }
-        if (my[j] >= J.divHi) {
-            copy_state<S::DIM>(y[j], y0[j]);
-            for (int i = 0; i < n; ++i) {
-                S::step(y[j], c[j]);
-                if (diverged(y[j][0], J.divThresh)) break;
-            }
-        }
-    }
-}
 
 template <class S, bool IC, int PPT, int THREADS, int MINB>
 __global__ void __launch_bounds__(THREADS, MINB) lle_kernel(const DevJob J, double* __restrict__ out)

@@ -132,6 +132,35 @@ cbf_status cbf_autotune(const cbf_job* job, int32_t* chosenVariant, double* msPe
 cbf_status cbf_set_lle_variant(int32_t system, int32_t variant);
 int32_t cbf_get_lle_variant(int32_t system);
 
+/* ---- ragged batches: many jobs, one persistent launch ----------------- */
+/* A batch is any mix of LLE / KDE / DBSCAN / 1-D peak jobs (systems, grid sizes,
+ * record lengths, steps) executed by one persistent kernel whose warps pull
+ * 32-point tiles from a device work queue, longest jobs first.  Results equal
+ * those of the same jobs run one by one.  d_outs[i] / d_auxs[i] are the
+ * device buffers cbf_run would take for jobs[i] (d_auxs may be NULL when no job
+ * needs one).  No counterpart in the reference (it runs one map per call). */
+typedef struct cbf_batch cbf_batch;
+cbf_status cbf_batch_create(const cbf_job* jobs, int32_t nJobs, void* const* d_outs,
+                            void* const* d_auxs, cbf_batch** batch);
+void cbf_batch_destroy(cbf_batch* batch);
+int64_t cbf_batch_points(const cbf_batch* batch);
+int32_t cbf_batch_blocks_per_sm(const cbf_batch* batch);
+/* Enqueue one run on `stream` (reset the queue, launch the persistent kernel). */
+cbf_status cbf_batch_run(cbf_batch* batch, void* stream);
+/* Capture one run as a CUDA graph (on `stream`, or the library's stream when
+ * NULL); cbf_batch_launch replays it for repeated sweeps. */
+cbf_status cbf_batch_capture(cbf_batch* batch, void* stream);
+cbf_status cbf_batch_launch(cbf_batch* batch, void* stream);
+/* The same jobs launched one by one through the per-job kernels. */
+cbf_status cbf_batch_run_sequential(cbf_batch* batch, void* stream);
+/* After the stream has synchronised: CBF_ERR_INTERNAL if a device guard fired. */
+cbf_status cbf_batch_check(cbf_batch* batch);
+/* Choose the persistent grid (blocks per SM among 1,2,3,4,6,8,12,16) by timing a
+ * copy of the batch with transients and records cut 32x; overwrites outputs and
+ * drops a captured graph.  msPerCandidate (optional, 8 entries; -1 = skipped). */
+cbf_status cbf_batch_autotune(cbf_batch* batch, void* stream, int32_t* blocksPerSm,
+                              double* msPerCandidate);
+
 /* ---- host-buffer entry points (drop-in for hostLibrary.cuh) ---------- */
 /* bifurcation1D, hostLibrary.cuh:29-42 / hostLibrary.cu:7-158.
  * outPeaks[k*peakCapacity + j], outCounts[k]; peakCapacity >= record/2. */
