@@ -25,7 +25,7 @@ LIB_PATH = PKG_DIR / "libcbf.so"
 
 SYS_MEMRISTIVE5, SYS_ROSSLER, SYS_LORENZ, SYS_CHEN = 0, 1, 2, 3
 SYSTEMS = {"memristive5": 0, "rossler": 1, "lorenz": 2, "chen": 3}
-TASK_PEAKS, TASK_KDE, TASK_DBSCAN, TASK_LLE, TASK_TRAJECTORY = 0, 1, 2, 3, 4
+TASK_PEAKS, TASK_KDE, TASK_DBSCAN, TASK_LLE, TASK_TRAJECTORY, TASK_LLE_REGIME = 0, 1, 2, 3, 4, 5
 FLAG_EXACT_GRID, FLAG_KDE_FIXED = 1, 2
 STATUS = {0: "ok", 1: "invalid argument", 2: "unknown system", 3: "CUDA error",
           4: "out of device memory", 5: "no CUDA device", 6: "I/O error",
@@ -88,6 +88,8 @@ class Job(C.Structure):
         ("kdeSampling", C.c_int32),
         ("flags", C.c_uint32),
         ("peakCapacity", C.c_int32),
+        ("regimeTime", C.c_double),
+        ("pointIndex", C.c_void_p),
     ]
 
 
@@ -211,7 +213,8 @@ def _i(a):
 def make_job(*, task, system, nPts, ranges, idxMut, ic, values, h, tMax=0.0, transientTime=0.0,
              maxValue=0.0, writableVar=0, preScaller=1, sweepIC=False, maxAmountOfPeaks=0,
              kdeSampling=0, kdeI1=0.0, kdeI2=0.0, kdeH=0.0, dbscanEps=0.0, NT=0.0, lleEps=0.0,
-             seedChunk=0, firstPoint=0, nPoints=0, flags=0, peakCapacity=0) -> Job:
+             seedChunk=0, firstPoint=0, nPoints=0, flags=0, peakCapacity=0, regimeTime=0.0,
+             pointIndex=0) -> Job:
     j = Job()
     lib().cbf_job_init(C.byref(j))
     dims = len(idxMut)
@@ -232,6 +235,8 @@ def make_job(*, task, system, nPts, ranges, idxMut, ic, values, h, tMax=0.0, tra
     j.kdeI1, j.kdeI2, j.kdeH, j.dbscanEps = kdeI1, kdeI2, kdeH, dbscanEps
     j.NT, j.lleEps, j.seedChunk = NT, lleEps, seedChunk
     j.firstPoint, j.nPoints, j.flags, j.peakCapacity = firstPoint, nPoints, flags, peakCapacity
+    j.regimeTime = regimeTime
+    j.pointIndex = pointIndex or None
     return j
 
 
@@ -243,6 +248,9 @@ def run_host(job: Job):
     aux = None
     if job.task == TASK_LLE:
         out = np.zeros(n, np.float64)
+    elif job.task == TASK_LLE_REGIME:
+        out = np.zeros(n, np.float64)
+        aux = np.zeros(n, np.int32)
     elif job.task in (TASK_KDE, TASK_DBSCAN):
         out = np.zeros(n, np.int32)
     else:

@@ -44,7 +44,7 @@ __device__ __forceinline__ void bif_tile(const DevJob& J, void* out, int* aux, l
 {
     const long long p = p0 + lane;
     const bool valid = p < J.nPoints;
-    const long long g = J.firstPoint + p;
+    const long long g = grid_index(J, p);
     if (TASK == CBF_TASK_PEAKS) {
         if (valid) {
             double* pk = (double*)out + p * (long long)J.peakCap;
@@ -82,7 +82,7 @@ __device__ __forceinline__ void run_tile(const DevJob& J, void* out, int* aux, l
     case CBF_TASK_LLE: {
         const long long p = p0 + lane;
         if (p < J.nPoints) {
-            const long long g = J.firstPoint + p;
+            const long long g = grid_index(J, p);
             ((double*)out)[p] = J.sweepIC ? lle_point<S, true>(J, g) : lle_point<S, false>(J, g);
         }
         break;

@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(kBifThreads) bif_kernel(const DevJob J, void* 
     for (long long tile = warpId; tile < nTiles; tile += nWarps) {
         const long long p = tile * 32 + lane;
         const bool valid = p < J.nPoints;
-        const long long g = J.firstPoint + p;
+        const long long g = grid_index(J, p);
 
         if (TASK == CBF_TASK_PEAKS) {
             if (valid) {

@@ -158,7 +158,7 @@ cbf_status lower_job(const cbf_job* j, DevJob* d)
     memset(d, 0, sizeof(*d));
     const int dim = system_dim(j->system);
     if (dim < 0) return fail(CBF_ERR_UNKNOWN_SYSTEM, "unknown system id %d", j->system);
-    if (j->task < CBF_TASK_PEAKS || j->task > CBF_TASK_TRAJECTORY)
+    if (j->task < CBF_TASK_PEAKS || j->task > CBF_TASK_LLE_REGIME)
         return fail(CBF_ERR_INVALID_ARG, "unknown task %d", j->task);
     if (j->dims != 1 && j->dims != 2) return fail(CBF_ERR_INVALID_ARG, "dims must be 1 or 2 (got %d)", j->dims);
     if (j->nPts < 1) return fail(CBF_ERR_INVALID_ARG, "nPts must be >= 1 (got %d)", j->nPts);
@@ -174,6 +174,7 @@ cbf_status lower_job(const cbf_job* j, DevJob* d)
             return fail(CBF_ERR_INVALID_ARG, "indicesOfMutVars[%d]=%d out of range [0,%d)", i,
                         j->idxMut[i], limit);
     // The LLE kernels always check x[0] and ignore writableVar (cudaLibrary.cu:735-753).
+    const bool lleTask = (j->task == CBF_TASK_LLE || j->task == CBF_TASK_LLE_REGIME);
     if (j->task != CBF_TASK_LLE && (j->writableVar < 0 || j->writableVar >= dim))
         return fail(CBF_ERR_INVALID_ARG, "writableVar %d out of range [0,%d)", j->writableVar, dim);
     if (!(isfinite(j->h) && j->h != 0)) return fail(CBF_ERR_INVALID_ARG, "h must be finite and nonzero");
@@ -183,6 +184,8 @@ cbf_status lower_job(const cbf_job* j, DevJob* d)
     const long long nPoints = j->nPoints > 0 ? j->nPoints : total;
     if (j->firstPoint < 0 || j->nPoints < 0)
         return fail(CBF_ERR_INVALID_ARG, "negative point range");
+    if (j->pointIndex && j->nPoints <= 0)
+        return fail(CBF_ERR_INVALID_ARG, "a point list needs nPoints > 0");
     if (j->firstPoint + nPoints > 2147483647ll)
         return fail(CBF_ERR_INVALID_ARG, "grid index exceeds the int range of getValueByIdx");
 
@@ -199,6 +202,7 @@ cbf_status lower_job(const cbf_job* j, DevJob* d)
     d->exactGrid = (j->flags & CBF_FLAG_EXACT_GRID) ? 1 : 0;
     d->firstPoint = j->firstPoint;
     d->nPoints = nPoints;
+    d->pointIndex = (const long long*)j->pointIndex;
     for (int i = 0; i < 4; ++i) d->ranges[i] = j->ranges[i];
     for (int i = 0; i < CBF_MAX_DIM; ++i) d->ic[i] = i < j->nIC ? j->ic[i] : 0.0;
     for (int i = 0; i < CBF_MAX_VALUES; ++i) d->values[i] = i < j->nV ? j->values[i] : 0.0;
@@ -214,7 +218,7 @@ cbf_status lower_job(const cbf_job* j, DevJob* d)
         return fail(CBF_ERR_INVALID_ARG, "transientTime/h does not fit an int");
     if (d->nSkip < 0) d->nSkip = 0;
 
-    if (j->task == CBF_TASK_LLE) {
+    if (lleTask) {
         if (!(j->NT != 0 && isfinite(j->NT))) return fail(CBF_ERR_INVALID_ARG, "NT must be finite and nonzero");
         if (!to_int(j->tMax / j->NT, &d->nRecord))
             return fail(CBF_ERR_INVALID_ARG, "tMax/NT does not fit an int");
@@ -227,6 +231,19 @@ cbf_status lower_job(const cbf_job* j, DevJob* d)
         d->tMax = j->tMax;
         if (j->seedChunk < 0) return fail(CBF_ERR_INVALID_ARG, "seedChunk must be >= 0");
         d->seedChunk = j->seedChunk;
+        if (j->task == CBF_TASK_LLE_REGIME) {
+            if (!to_int(j->regimeTime / j->h, &d->regimeSteps) || d->regimeSteps < 0)
+                return fail(CBF_ERR_INVALID_ARG, "regimeTime/h must be in [0, 2^31)");
+            d->maxPeaks = j->maxAmountOfPeaks;
+            const int half = d->regimeSteps / 2 > 0 ? d->regimeSteps / 2 : 1;
+            const int cap = j->maxAmountOfPeaks < half ? j->maxAmountOfPeaks : half;
+            d->peakCap = cap > 0 ? cap : 1;
+            const double e = j->dbscanEps;
+            d->dbEps = e;
+            if (!(e > 0)) d->dbSkip = 0.0;
+            else if (!(4.0 * e >= 1.1754943508222875e-38) || isinf(e)) d->dbSkip = INFINITY;
+            else d->dbSkip = 4.0 * e;
+        }
     } else {
         if (j->preScaller < 1) return fail(CBF_ERR_INVALID_ARG, "preScaller must be >= 1");
         d->preScaller = j->preScaller;
@@ -272,7 +289,8 @@ cbf_status lower_job(const cbf_job* j, DevJob* d)
 size_t out_bytes(const DevJob& d)
 {
     switch (d.task) {
-    case CBF_TASK_LLE: return (size_t)d.nPoints * sizeof(double);
+    case CBF_TASK_LLE:
+    case CBF_TASK_LLE_REGIME: return (size_t)d.nPoints * sizeof(double);
     case CBF_TASK_KDE:
     case CBF_TASK_DBSCAN: return (size_t)d.nPoints * sizeof(int);
     default: return (size_t)d.nPoints * (size_t)d.peakCap * sizeof(double);
@@ -281,7 +299,9 @@ size_t out_bytes(const DevJob& d)
 
 size_t aux_bytes(const DevJob& d)
 {
-    return (d.task == CBF_TASK_PEAKS || d.task == CBF_TASK_TRAJECTORY) ? (size_t)d.nPoints * sizeof(int) : 0;
+    return (d.task == CBF_TASK_PEAKS || d.task == CBF_TASK_TRAJECTORY || d.task == CBF_TASK_LLE_REGIME)
+               ? (size_t)d.nPoints * sizeof(int)
+               : 0;
 }
 
 cbf_status run_lowered(const DevJob& d, void* d_out, void* d_aux, cudaStream_t s)
@@ -290,6 +310,8 @@ cbf_status run_lowered(const DevJob& d, void* d_out, void* d_aux, cudaStream_t s
     if (d.nPoints == 0) return CBF_OK;
     if (d.task == CBF_TASK_LLE)
         e = launch_lle(d, (double*)d_out, s);
+    else if (d.task == CBF_TASK_LLE_REGIME)
+        e = launch_lle_regime(d, (double*)d_out, (int*)d_aux, s);
     else
         e = launch_bif(d, d_out, (int*)d_aux, s);
     if (e == cudaErrorAssert) return fail(CBF_ERR_INTERNAL, "device-side iteration guard fired");
@@ -491,7 +513,7 @@ int32_t cbf_record_length(const cbf_job* j)
 {
     if (!j) return -1;
     int v = 0;
-    if (j->task == CBF_TASK_LLE) {
+    if (j->task == CBF_TASK_LLE || j->task == CBF_TASK_LLE_REGIME) {
         if (j->NT == 0 || !to_int(j->tMax / j->NT, &v)) return -1;
     } else {
         if (j->h == 0 || j->preScaller < 1 || !to_int(j->tMax / j->h / (double)j->preScaller, &v)) return -1;
@@ -727,7 +749,8 @@ cbf_status cbf_lle_seeds(const cbf_job* job, double* out_host)
     DevJob d;
     cbf_status st = lower_job(job, &d);
     if (st != CBF_OK) return st;
-    if (d.task != CBF_TASK_LLE) return fail(CBF_ERR_INVALID_ARG, "cbf_lle_seeds needs an LLE job");
+    if (d.task != CBF_TASK_LLE && d.task != CBF_TASK_LLE_REGIME)
+        return fail(CBF_ERR_INVALID_ARG, "cbf_lle_seeds needs an LLE job");
     if (!out_host) return fail(CBF_ERR_INVALID_ARG, "null output");
     if (d.nPoints == 0) return CBF_OK;
     cudaStream_t s;

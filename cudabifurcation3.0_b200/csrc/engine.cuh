@@ -28,6 +28,8 @@ struct DevJob {
     long long firstPoint;
     long long nPoints;
     long long seedChunk;
+    const long long* pointIndex;  // optional device list of grid indices (see cbf_job)
+    int regimeSteps;    // LLE_REGIME: recorded steps after the transient
     int nPts, dims, nIC, nV;
     int idxMut0, idxMut1;
     int writableVar, preScaller;
@@ -45,6 +47,12 @@ struct DevJob {
     int system;
     int sweepIC;
 };
+
+// Grid index of the job's k-th point: an explicit list, or a contiguous range.
+__device__ __forceinline__ long long grid_index(const DevJob& J, long long k)
+{
+    return J.pointIndex ? J.pointIndex[k] : J.firstPoint + k;
+}
 
 // getValueByIdx (cudaLibrary.cu:210-216): `(int)idx / powf(nPts, v)` is a float
 // division, so above 2^24 the index is rounded; exactGrid uses integer math.
@@ -145,6 +153,7 @@ int lle_variant_for(int system);
 cudaError_t launch_bif(const DevJob& J, void* d_out, int* d_aux, cudaStream_t s);
 cudaError_t launch_grid_coords(const DevJob& J, double* d_out, cudaStream_t s);
 cudaError_t launch_lle_seeds(const DevJob& J, double* d_out, cudaStream_t s);
+cudaError_t launch_lle_regime(const DevJob& J, double* d_lle, int* d_class, cudaStream_t s);
 // KDE/DBSCAN with caller-provided scratch (no allocation): `scratch` holds
 // `scratchBytes` of peak buffers, `err` one int that must be zero on entry.
 // Synchronises `s` to read `err`.

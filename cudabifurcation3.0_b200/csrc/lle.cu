@@ -38,7 +38,7 @@ __global__ void __launch_bounds__(THREADS, MINB) lle_kernel(const DevJob J, doub
             long long p = q * PPT + j;
             if (p >= J.nPoints) p = J.nPoints - 1;  // tail lane repeats a point, never stores it
             double v[CBF_MAX_VALUES];
-            setup_point<D>(J, J.firstPoint + p, x[j], v);
+            setup_point<D>(J, grid_index(J, p), x[j], v);
             c[j] = S::prep(v, J.h);
         }
 
@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(THREADS, MINB) lle_kernel(const DevJob J, doub
             long long p = q * PPT + j;
             if (p >= J.nPoints) p = J.nPoints - 1;
             double z[D];
-            lle_seed<D, IC>(J.firstPoint + p, J.seedChunk, z);
+            lle_seed<D, IC>(grid_index(J, p), J.seedChunk, z);
 #pragma unroll
             for (int i = 0; i < D; ++i) y[j][i] = z[i] * J.lleEps + x[j][i];
         }
@@ -85,7 +85,7 @@ __global__ void lle_seed_kernel(const DevJob J, double* __restrict__ out)
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= J.nPoints) return;
     double z[D];
-    lle_seed<D, IC>(J.firstPoint + p, J.seedChunk, z);
+    lle_seed<D, IC>(grid_index(J, p), J.seedChunk, z);
 #pragma unroll
     for (int i = 0; i < D; ++i) out[p * D + i] = z[i];
 }

@@ -1,0 +1,200 @@
+// LLE map with a peak-count regime class per point, in one pass.
+//
+// The LLE is computed exactly as by the LLE kernels (LLEKernelCUDA semantics,
+// cudaLibrary.cu:666-908).  During the first `regimeSteps` steps after the
+// transient, the base trajectory's x[writableVar] is sampled before every step
+// (the record semantics of loopCalculateDiscreteModel, cudaLibrary.cu:59-62) and
+// fed to the streaming peak finder; the class is the reference's DBSCAN cluster
+// count of those (peak, interval) pairs (dbscan, cudaLibrary.cu:457-529), with
+//   0  when the trajectory diverged inside the window or has no peaks,
+//   15 when it has more than maxAmountOfPeaks peaks (or 15 or more clusters).
+// The window costs one peak-state update per step on top of the LLE; the
+// transient is shared.  This is the plain FP64 method that labels the surrogate's
+// training data and recomputes the points it cannot be trusted with.
+#include "bif_device.cuh"
+#include "lle_device.cuh"
+
+namespace cbf {
+namespace {
+
+constexpr int kRegWarps = 4;
+constexpr int kRegThreads = kRegWarps * 32;
+constexpr int kNumClasses = 16;
+
+// One point: returns the LLE; *n = emitted peaks in the window, -1 if the
+// divergence test fired inside it.
+template <class S, bool IC>
+__device__ double lle_regime_point(const DevJob& J, long long g, double* pk, double* iv, int cap,
+                                   int* nOut)
+{
+    constexpr int D = S::DIM;
+    double x[1][D], y[1][D];
+    typename S::Coef c[1];
+    {
+        double v[CBF_MAX_VALUES];
+        setup_point<D>(J, g, x[0], v);
+        c[0] = S::prep(v, J.h);
+    }
+    run_checked<S, 1>(x, c, J.nSkip, J);
+    {
+        double z[D];
+        lle_seed<D, IC>(g, J.seedChunk, z);
+#pragma unroll
+        for (int i = 0; i < D; ++i) y[0][i] = z[i] * J.lleEps + x[0][i];
+    }
+    PeakStream ps;
+    ps.init();
+    bool regimeDiv = false;
+    int t = 0;  // step index since the transient
+    double result = 0;
+    for (int b = 0; b < J.nRecord; ++b) {
+        if (t < J.regimeSteps) {
+            // Intervals overlapping the window run the exact per-step path.
+            bool ax = true, ay = true;
+            for (int i = 0; i < J.nNT; ++i, ++t) {
+                if (ax) {
+                    if (t < J.regimeSteps) ps.push<true>(pick<D>(x[0], J.writableVar), t, pk, iv, cap);
+                    S::step(x[0], c[0]);
+                    if (J.checkDiv && diverged(x[0][0], J.divThresh)) {
+                        ax = false;
+                        if (t < J.regimeSteps) regimeDiv = true;
+                    }
+                }
+                if (ay) {
+                    S::step(y[0], c[0]);
+                    if (J.checkDiv && diverged(y[0][0], J.divThresh)) ay = false;
+                }
+            }
+        } else {
+            run_pair<S, 1>(x, y, c, J.nNT, J);
+            t += J.nNT;
+        }
+        double tt = 0;
+#pragma unroll
+        for (int l = 0; l < D; ++l) tt += (x[0][l] - y[0][l]) * (x[0][l] - y[0][l]);
+        tt = sqrt(tt) / J.lleEps;
+        result += log(tt);
+        if (tt != 0) tt = (1 / tt);
+#pragma unroll
+        for (int i = 0; i < D; ++i) y[0][i] = x[0][i] - ((x[0][i] - y[0][i]) * tt);
+    }
+    *nOut = regimeDiv ? -1 : ps.emitted();
+    return result / J.tMax;
+}
+
+template <class S, bool IC>
+__global__ void __launch_bounds__(kRegThreads) lle_regime_kernel(const DevJob J, double* __restrict__ lle,
+                                                                 int* __restrict__ cls, double* scrPk,
+                                                                 double* scrIv, int bitWords, int* err)
+{
+    extern __shared__ unsigned smem[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const long long warpId = (long long)blockIdx.x * kRegWarps + wib;
+    const long long nWarps = (long long)gridDim.x * kRegWarps;
+    const long long nTiles = (J.nPoints + 31) / 32;
+    const int cap = J.peakCap;
+    unsigned* L = smem + (size_t)wib * 2 * bitWords;
+    unsigned* Sb = L + bitWords;
+    const long long slot0 = warpId * 32;
+
+    for (long long tile = warpId; tile < nTiles; tile += nWarps) {
+        const long long p = tile * 32 + lane;
+        const bool valid = p < J.nPoints;
+        double* myPk = scrPk + (slot0 + lane) * (long long)cap;
+        double* myIv = scrIv + (slot0 + lane) * (long long)cap;
+        int n = 0;
+        double lv = 0;
+        if (valid) lv = lle_regime_point<S, IC>(J, grid_index(J, p), myPk, myIv, cap, &n);
+        __syncwarp();
+        int res = 0;
+        const int live = (int)min(32ll, J.nPoints - tile * 32);
+        for (int j = 0; j < live; ++j) {
+            const int nj = __shfl_sync(kFull, n, j);
+            int r;
+            if (nj <= 0) r = 0;
+            else if (nj > J.maxPeaks) r = kNumClasses - 1;
+            else {
+                const double* pk = scrPk + (slot0 + j) * (long long)cap;
+                const double* iv = scrIv + (slot0 + j) * (long long)cap;
+                r = min(dbscan_warp(J, pk, iv, nj, lane, L, Sb, err), kNumClasses - 1);
+            }
+            if (lane == j) res = r;
+        }
+        if (valid) {
+            lle[p] = lv;
+            cls[p] = res;
+        }
+        __syncwarp();
+    }
+}
+
+template <class S, bool IC>
+cudaError_t launch_t(const DevJob& J, double* d_lle, int* d_cls, cudaStream_t s)
+{
+    const long long nTiles = (J.nPoints + 31) / 32;
+    if (nTiles == 0) return cudaSuccess;
+    const int bitWords = (J.peakCap + 31) / 32;
+    const size_t smemBytes = (size_t)kRegWarps * 2 * bitWords * sizeof(unsigned);
+    auto kern = lle_regime_kernel<S, IC>;
+    cudaError_t e;
+    if (smemBytes > 48 * 1024) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBytes);
+        if (e != cudaSuccess) return e;
+    }
+    int dev = 0, sms = 0, perSm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, kRegThreads, smemBytes)) != cudaSuccess)
+        return e;
+    if (perSm < 1) return cudaErrorInvalidConfiguration;
+    long long blocks = (nTiles + kRegWarps - 1) / kRegWarps;
+    if (blocks > (long long)sms * perSm) blocks = (long long)sms * perSm;
+    const size_t perBlock = (size_t)kRegThreads * J.peakCap * sizeof(double) * 2;
+    size_t freeB = 0, totalB = 0;
+    if ((e = cudaMemGetInfo(&freeB, &totalB)) != cudaSuccess) return e;
+    size_t budget = freeB / 4;
+    if (budget > ((size_t)8 << 30)) budget = (size_t)8 << 30;
+    long long fit = (long long)(budget / perBlock);
+    if (fit < 1) fit = 1;
+    if (blocks > fit) blocks = fit;
+    const size_t bytes = (size_t)blocks * perBlock;
+    double* scr = nullptr;
+    if ((e = cudaMallocAsync((void**)&scr, bytes + 256, s)) != cudaSuccess) return e;
+    double* scrIv = scr + (size_t)blocks * kRegThreads * J.peakCap;
+    int* err = (int*)((char*)scr + bytes);
+    if ((e = cudaMemsetAsync(err, 0, sizeof(int), s)) == cudaSuccess) {
+        kern<<<(unsigned)blocks, kRegThreads, smemBytes, s>>>(J, d_lle, d_cls, scr, scrIv, bitWords, err);
+        note_launch();
+        e = cudaGetLastError();
+    }
+    int hostErr = 0;
+    cudaError_t e2 = cudaMemcpyAsync(&hostErr, err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaError_t e3 = cudaFreeAsync(scr, s);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = e3;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess && hostErr) return cudaErrorAssert;
+    return e;
+}
+
+template <class S>
+cudaError_t launch_s(const DevJob& J, double* d_lle, int* d_cls, cudaStream_t s)
+{
+    return J.sweepIC ? launch_t<S, true>(J, d_lle, d_cls, s) : launch_t<S, false>(J, d_lle, d_cls, s);
+}
+
+}  // namespace
+
+cudaError_t launch_lle_regime(const DevJob& J, double* d_lle, int* d_cls, cudaStream_t s)
+{
+    switch (J.system) {
+    case CBF_SYS_MEMRISTIVE5: return launch_s<Memristive5>(J, d_lle, d_cls, s);
+    case CBF_SYS_ROSSLER: return launch_s<Rossler>(J, d_lle, d_cls, s);
+    case CBF_SYS_LORENZ: return launch_s<Lorenz>(J, d_lle, d_cls, s);
+    case CBF_SYS_CHEN: return launch_s<Chen>(J, d_lle, d_cls, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace cbf

@@ -47,7 +47,7 @@ __global__ void grid_coords_kernel(const DevJob J, double* out)
 {
     const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= J.nPoints) return;
-    const long long g = J.firstPoint + k;
+    const long long g = grid_index(J, k);
     const bool exact = J.exactGrid != 0;
     out[k * 2 + 0] = grid_value(g, J.nPts, J.ranges[0], J.ranges[1], 0, exact);
     out[k * 2 + 1] = J.dims > 1 ? grid_value(g, J.nPts, J.ranges[2], J.ranges[3], 1, exact) : 0.0;

@@ -56,6 +56,7 @@ typedef int32_t cbf_status;
 #define CBF_TASK_DBSCAN 2       /* DBSCAN cluster count per point (int32) */
 #define CBF_TASK_LLE 3          /* largest Lyapunov exponent per point (double) */
 #define CBF_TASK_TRAJECTORY 4   /* recorded x[writableVar] samples per point (+diverged flags) */
+#define CBF_TASK_LLE_REGIME 5   /* LLE (double) + peak-count regime class 0..15 (int32, in d_aux) */
 
 /* Job flags. */
 #define CBF_FLAG_EXACT_GRID 1u  /* integer grid index instead of the FP32 quirk */
@@ -94,6 +95,11 @@ typedef struct cbf_job {
     int32_t kdeSampling;
     uint32_t flags;                 /* CBF_FLAG_* */
     int32_t peakCapacity;           /* PEAKS/TRAJECTORY: row stride of d_out (0: derived) */
+    double regimeTime;              /* LLE_REGIME: time units of the base trajectory, right
+                                       after the transient, whose peaks define the class */
+    const int64_t* pointIndex;      /* optional DEVICE array: point k of the job is grid
+                                       index pointIndex[k] (nPoints entries) instead of
+                                       firstPoint + k; outputs stay compact */
 } cbf_job;
 
 /* ---- library ---------------------------------------------------------- */

@@ -492,6 +492,81 @@ double orc_lle_point_seeded(const orc_job* job, int64_t g, const double* zIn)
     return result / job->tMax;
 }
 
+double orc_lle_regime_point(const orc_job* job, int64_t g, const double* zIn, int32_t* cls)
+{
+    double x[8], y[8], z[8], v[16];
+    setup_point(job, g, x, v);
+    const int nIC = job->nIC;
+    if (zIn) {
+        for (int i = 0; i < nIC; ++i)
+            z[i] = zIn[i];
+    } else {
+        orc_lle_seed(job, g, z);
+    }
+    const int sys = job->system;
+    const double h = job->h;
+    const int nNT = (int)(size_t)(job->NT / h);
+    const int sizeOfBlock = (int)(job->tMax / job->NT);
+    const double eps = job->lleEps;
+    const int win = (int)(job->regimeTime / h);
+    int64_t total = (int64_t)nNT * (sizeOfBlock > 0 ? sizeOfBlock : 0);
+    const int recorded = (int)(win < total ? win : total);
+    double* data = (double*)malloc(sizeof(double) * (size_t)(recorded > 0 ? recorded : 1));
+    int regimeDiv = 0;
+
+    orc_loop(sys, x, v, h, orc_skip_len(job), 1, 0, job->maxValue, NULL, 0, 1);
+    for (int i = 0; i < nIC; ++i)
+        y[i] = z[i] * eps + x[i];
+
+    double result = 0;
+    int t = 0;
+    for (int b = 0; b < sizeOfBlock; ++b) {
+        /* the base trajectory's interval, recording while inside the window; the
+         * divergence test stops the interval (cudaLibrary.cu:69-71) */
+        int inWin = recorded - t;
+        if (inWin > nNT) inWin = nNT;
+        if (inWin < 0) inWin = 0;
+        int ok = 1;
+        if (inWin > 0) {
+            ok = orc_loop(sys, x, v, h, inWin, 1, job->writableVar, job->maxValue, data, t, 1);
+            if (!ok) regimeDiv = 1;
+        }
+        if (ok && nNT - inWin > 0)
+            orc_loop(sys, x, v, h, nNT - inWin, 1, 0, job->maxValue, NULL, 0, 1);
+        orc_loop(sys, y, v, h, nNT, 1, 0, job->maxValue, NULL, 0, 1);
+        t += nNT;
+
+        double tempData = 0;
+        for (int l = 0; l < nIC; ++l)
+            tempData += (x[l] - y[l]) * (x[l] - y[l]);
+        tempData = sqrt(tempData) / eps;
+        result += log(tempData);
+        if (tempData != 0)
+            tempData = (1 / tempData);
+        for (int j = 0; j < nIC; ++j)
+            y[j] = (double)(x[j] - ((x[j] - y[j]) * tempData));
+    }
+
+    int c = 0;
+    if (!regimeDiv && recorded > 0) {
+        double* times = (double*)malloc(sizeof(double) * (size_t)recorded);
+        int n = orc_peak_finder(data, 0, recorded, data, times, 0.01);
+        if (n > job->maxAmountOfPeaks) {
+            c = 15;
+        } else if (n > 0) {
+            double* helpful = (double*)malloc(sizeof(double) * (size_t)(2 * n + 2));
+            c = orc_dbscan(data, times, helpful, 0, n, 2 * n + 2, job->maxAmountOfPeaks,
+                           job->dbscanEps);
+            free(helpful);
+            if (c > 15) c = 15;
+        }
+        free(times);
+    }
+    free(data);
+    *cls = c;
+    return result / job->tMax;
+}
+
 /* ------------------------------------------------------------------------- */
 /* Map drivers                                                                */
 
@@ -622,6 +697,17 @@ int orc_map_lle_seeded(const orc_job* job, int64_t first, int64_t count, const d
 #pragma omp parallel for schedule(dynamic, 1) num_threads(threads_or_default(nThreads))
     for (int64_t k = 0; k < count; ++k)
         out[k] = orc_lle_point_seeded(job, first + k, z + k * job->nIC);
+    return 0;
+}
+
+int orc_map_lle_regime_list(const orc_job* job, const int64_t* idx, int64_t count,
+                            const double* z, double* outLle, int32_t* outCls, int nThreads)
+{
+    if ((int)(job->tMax / job->NT) <= 0 || job->nIC <= 0)
+        return -1;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads_or_default(nThreads))
+    for (int64_t k = 0; k < count; ++k)
+        outLle[k] = orc_lle_regime_point(job, idx[k], z ? z + k * job->nIC : NULL, &outCls[k]);
     return 0;
 }
 

@@ -61,6 +61,7 @@ typedef struct orc_job {
     int32_t preScaller;
     int32_t maxAmountOfPeaks;
     int32_t kdeSampling;
+    double regimeTime;  /* LLE + regime: window after the transient (time units) */
 } orc_job;
 
 /* cudaLibrary.cu:210-216 */
@@ -121,6 +122,15 @@ int orc_map_lle_seeded(const orc_job* job, int64_t first, int64_t count, const d
                        double* out, int nThreads);
 /* Same, over an explicit list of global indices (strided samples for the CPU baseline). */
 int orc_map_lle_list(const orc_job* job, const int64_t* idx, int64_t count, double* out, int nThreads);
+
+/* LLE plus peak-count regime class (the library's plain labelling method): the
+ * LLE of orc_lle_point_seeded; x[writableVar] recorded before every step of the
+ * base trajectory for the first (int)(regimeTime/h) steps after the transient;
+ * class = 0 if the divergence test fired inside that window or no peak,
+ * 15 if more than maxAmountOfPeaks peaks, else min(dbscan, 15). */
+double orc_lle_regime_point(const orc_job* job, int64_t g, const double* z, int32_t* cls);
+int orc_map_lle_regime_list(const orc_job* job, const int64_t* idx, int64_t count,
+                            const double* z, double* outLle, int32_t* outCls, int nThreads);
 
 /* Divergence test of loopCalculateDiscreteModel (cudaLibrary.cu:69-71), exposed for tests. */
 int orc_diverged(double v, double maxValue);

@@ -48,13 +48,14 @@ class OrcJob(C.Structure):
         ("preScaller", C.c_int32),
         ("maxAmountOfPeaks", C.c_int32),
         ("kdeSampling", C.c_int32),
+        ("regimeTime", C.c_double),
     ]
 
 
 def make_job(*, system, nPts, ranges, idxMut, ic, values, h, tMax=0.0, transientTime=0.0,
              maxValue=0.0, writableVar=0, preScaller=1, sweepIC=False, maxAmountOfPeaks=0,
              kdeSampling=0, kdeI1=0.0, kdeI2=0.0, kdeH=0.0, dbscanEps=0.0, NT=0.0,
-             lleEps=0.0, seedChunk=0) -> OrcJob:
+             lleEps=0.0, seedChunk=0, regimeTime=0.0) -> OrcJob:
     j = OrcJob()
     dims = len(idxMut)
     j.system = SYSTEMS[system] if isinstance(system, str) else int(system)
@@ -77,6 +78,7 @@ def make_job(*, system, nPts, ranges, idxMut, ic, values, h, tMax=0.0, transient
     j.kdeI1, j.kdeI2, j.kdeH = kdeI1, kdeI2, kdeH
     j.dbscanEps = dbscanEps
     j.NT, j.lleEps, j.seedChunk = NT, lleEps, seedChunk
+    j.regimeTime = regimeTime
     return j
 
 
@@ -149,6 +151,9 @@ def lib():
         L.orc_lle_seed.argtypes = [C.POINTER(OrcJob), C.c_int64, _dp]
         L.orc_map_lle_seeded.restype = C.c_int
         L.orc_map_lle_seeded.argtypes = [C.POINTER(OrcJob), C.c_int64, C.c_int64, _dp, _dp, C.c_int]
+        L.orc_map_lle_regime_list.restype = C.c_int
+        L.orc_map_lle_regime_list.argtypes = [C.POINTER(OrcJob), _lp, C.c_int64, C.c_void_p, _dp,
+                                              _ip, C.c_int]
         L.orc_map_lle_list.restype = C.c_int
         L.orc_map_lle_list.argtypes = [C.POINTER(OrcJob), _lp, C.c_int64, _dp, C.c_int]
         _lib = L
@@ -292,6 +297,21 @@ def lle_seeds(job: OrcJob, first: int, count: int):
         lib().orc_lle_seed(C.byref(job), first + k, row)
         out[k] = row
     return out
+
+
+def map_lle_regime(job: OrcJob, idx, z=None, threads: int = 0):
+    """LLE and regime class at grid indices idx (optionally from given seeds z)."""
+    idx = np.ascontiguousarray(idx, dtype=np.int64)
+    lle = np.zeros(len(idx), np.float64)
+    cls = np.zeros(len(idx), np.int32)
+    zp = None
+    if z is not None:
+        z = np.ascontiguousarray(z, dtype=np.float64)
+        zp = z.ctypes.data_as(C.c_void_p)
+    rc = lib().orc_map_lle_regime_list(C.byref(job), idx, len(idx), zp, lle, cls, threads)
+    if rc != 0:
+        raise RuntimeError(f"orc_map_lle_regime_list failed: {rc}")
+    return lle, cls
 
 
 def map_lle_list(job: OrcJob, idx, threads: int = 0):

@@ -42,7 +42,7 @@ def assert_lle_close(got, want, tol=LLE_TOL):
 def both(cbf, orc, **kw):
     """The same job for the product (cbf.Job) and the oracle (orc.OrcJob)."""
     okw = {k: v for k, v in kw.items() if k not in ("task", "firstPoint", "nPoints", "flags",
-                                                    "peakCapacity")}
+                                                    "peakCapacity", "pointIndex")}
     return cbf.make_job(**kw), orc.make_job(**okw)
 
 
@@ -257,6 +257,55 @@ def test_lle_long_run_seed_sensitivity_is_small(cbf, orc, gpu_ok):
     got, _ = cbf.run_host(j)
     want = orc.map_lle(o, 0, 16)
     assert_lle_close(got, want, 1e-5)
+
+
+REGIME = dict(CHEN_LLE, nPts=10, tMax=40.0, transientTime=20.0, maxAmountOfPeaks=512,
+              dbscanEps=0.05, regimeTime=20.0)
+
+
+@pytest.mark.parametrize("extra", [dict(), dict(maxValue=20.0), dict(maxAmountOfPeaks=20),
+                                   dict(regimeTime=60.0), dict(writableVar=2)])
+def test_lle_regime_matches_oracle(cbf, orc, gpu_ok, extra):
+    kw = dict(REGIME, **extra)
+    j, o = both(cbf, orc, task=cbf.TASK_LLE_REGIME, **kw)
+    lle, cls = cbf.run_host(j)
+    n = kw["nPts"] ** 2
+    want_lle, want_cls = orc.map_lle_regime(o, np.arange(n), cbf.lle_seeds(j))
+    assert np.array_equal(cls, want_cls), np.nonzero(cls != want_cls)
+    assert_lle_close(lle, want_lle)
+    assert 0 <= cls.min() and cls.max() <= 15
+    # the LLE of the fused kernel is the LLE kernel's, bit for bit
+    plain = {k: v for k, v in kw.items() if k not in ("maxAmountOfPeaks", "dbscanEps", "regimeTime")}
+    lle2, _ = cbf.run_host(cbf.make_job(task=cbf.TASK_LLE, **plain))
+    assert np.array_equal(lle, lle2, equal_nan=True)
+
+
+@pytest.mark.parametrize("task", ["lle", "regime", "dbscan"])
+def test_point_lists_equal_full_map_entries(cbf, gpu_ok, task):
+    torch = pytest.importorskip("torch")
+    if task == "dbscan":
+        kw = dict(LORENZ_MAP, maxAmountOfPeaks=10000, dbscanEps=0.05)
+        t = cbf.TASK_DBSCAN
+    else:
+        kw = dict(REGIME)
+        t = cbf.TASK_LLE if task == "lle" else cbf.TASK_LLE_REGIME
+        if task == "lle":
+            kw = {k: v for k, v in kw.items() if k not in ("maxAmountOfPeaks", "dbscanEps",
+                                                           "regimeTime")}
+    full, full_aux = cbf.run_host(cbf.make_job(task=t, **kw))
+    n = kw["nPts"] ** 2
+    idx = torch.tensor(np.random.default_rng(3).permutation(n)[: n // 3], dtype=torch.int64,
+                       device="cuda")
+    m = idx.numel()
+    out = torch.empty(m, dtype=torch.int32 if t == cbf.TASK_DBSCAN else torch.float64, device="cuda")
+    aux = torch.empty(m, dtype=torch.int32, device="cuda")
+    j = cbf.make_job(task=t, nPoints=m, pointIndex=idx.data_ptr(), **kw)
+    cbf.run_device(j, out.data_ptr(), aux.data_ptr() if t == cbf.TASK_LLE_REGIME else 0)
+    torch.cuda.synchronize()
+    sel = idx.cpu().numpy()
+    assert np.array_equal(out.cpu().numpy(), full[sel], equal_nan=True)
+    if t == cbf.TASK_LLE_REGIME:
+        assert np.array_equal(aux.cpu().numpy(), full_aux[sel])
 
 
 def test_device_api_with_torch_stream(cbf, gpu_ok):
