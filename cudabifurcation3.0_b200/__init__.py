@@ -45,6 +45,9 @@ EXPORTS = [
     "cbf_batch_blocks_per_sm", "cbf_batch_run", "cbf_batch_capture", "cbf_batch_launch",
     "cbf_batch_run_sequential", "cbf_batch_check", "cbf_batch_autotune", "cbf_bifurcation2d_dbscan_noalloc",
     "cbf_csv_write_map", "cbf_csv_write_peaks", "cbf_csv_write_pairs",
+    "cbf_mlp_num_params", "cbf_mlp_create", "cbf_mlp_destroy", "cbf_mlp_get_params",
+    "cbf_mlp_set_params", "cbf_mlp_forward_backward", "cbf_mlp_train", "cbf_mlp_predict",
+    "cbf_surrogate_config_init", "cbf_lle_map_surrogate",
 ]
 
 
@@ -90,7 +93,59 @@ class Job(C.Structure):
         ("peakCapacity", C.c_int32),
         ("regimeTime", C.c_double),
         ("pointIndex", C.c_void_p),
+        ("regimeMinAmp", C.c_double),
+        ("regimeChaosLle", C.c_double),
     ]
+
+
+class SurrogateConfig(C.Structure):
+    """Mirror of ``cbf_surrogate_config`` (include/cbf.h)."""
+    _fields_ = [
+        ("coarseSide", C.c_int32),
+        ("randomPoints", C.c_int32),
+        ("batch", C.c_int32),
+        ("trainSteps", C.c_int32),
+        ("lr", C.c_float),
+        ("wLle", C.c_float),
+        ("confThreshold", C.c_float),
+        ("auditFraction", C.c_float),
+        ("boundaryRadius", C.c_int32),
+        ("refine", C.c_int32),
+        ("seed", C.c_uint64),
+        ("expandRadius", C.c_int32),
+        ("maxWaves", C.c_int32),
+    ]
+
+
+class SurrogateReport(C.Structure):
+    """Mirror of ``cbf_surrogate_report`` (include/cbf.h)."""
+    _fields_ = [
+        ("points", C.c_int64),
+        ("labelled", C.c_int64),
+        ("refined", C.c_int64),
+        ("boundary", C.c_int64),
+        ("lowConfidence", C.c_int64),
+        ("audit", C.c_int64),
+        ("auditOnly", C.c_int64),
+        ("auditOnlyAgree", C.c_int64),
+        ("refinedChanged", C.c_int64),
+        ("auditOnlyLleMeanAbsErr", C.c_double),
+        ("auditOnlyLleMaxAbsErr", C.c_double),
+        ("lleMean", C.c_double),
+        ("lleStd", C.c_double),
+        ("finalLoss", C.c_float),
+        ("msLabel", C.c_double),
+        ("msTrain", C.c_double),
+        ("msPredict", C.c_double),
+        ("msMask", C.c_double),
+        ("msRefine", C.c_double),
+        ("msTotal", C.c_double),
+        ("expanded", C.c_int64),
+        ("waves", C.c_int32),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 _lib = None
@@ -185,6 +240,30 @@ def lib():
         L.cbf_csv_write_pairs.restype = C.c_int32
         L.cbf_csv_write_pairs.argtypes = [C.c_char_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64,
                                           C.c_int32]
+        _fp = C.POINTER(C.c_float)
+        L.cbf_mlp_num_params.restype = C.c_int64
+        L.cbf_mlp_create.argtypes = [C.c_int32, C.c_uint64, C.POINTER(C.c_void_p)]
+        L.cbf_mlp_create.restype = C.c_int32
+        L.cbf_mlp_destroy.argtypes = [C.c_void_p]
+        L.cbf_mlp_destroy.restype = None
+        for f in ("cbf_mlp_get_params", "cbf_mlp_set_params"):
+            getattr(L, f).argtypes = [C.c_void_p, _fp, C.c_int64]
+            getattr(L, f).restype = C.c_int32
+        L.cbf_mlp_forward_backward.argtypes = [C.c_void_p, _fp, _fp, _ip, C.c_int32, C.c_float, _fp,
+                                               _fp, _fp]
+        L.cbf_mlp_forward_backward.restype = C.c_int32
+        L.cbf_mlp_train.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                    C.c_int32, C.c_float, C.c_int32, C.c_float, _fp, C.c_void_p]
+        L.cbf_mlp_train.restype = C.c_int32
+        L.cbf_mlp_predict.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_float, C.c_float,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.cbf_mlp_predict.restype = C.c_int32
+        L.cbf_surrogate_config_init.argtypes = [C.POINTER(SurrogateConfig)]
+        L.cbf_surrogate_config_init.restype = None
+        L.cbf_lle_map_surrogate.argtypes = [C.POINTER(Job), C.POINTER(SurrogateConfig), C.c_void_p,
+                                            C.c_void_p, C.c_void_p, C.POINTER(SurrogateReport),
+                                            C.c_void_p]
+        L.cbf_lle_map_surrogate.restype = C.c_int32
         L.cbf_facade_set_system.argtypes = [C.c_int32]
         L.cbf_facade_set_output_path.argtypes = [C.c_char_p]
         _lib = L
@@ -214,7 +293,7 @@ def make_job(*, task, system, nPts, ranges, idxMut, ic, values, h, tMax=0.0, tra
              maxValue=0.0, writableVar=0, preScaller=1, sweepIC=False, maxAmountOfPeaks=0,
              kdeSampling=0, kdeI1=0.0, kdeI2=0.0, kdeH=0.0, dbscanEps=0.0, NT=0.0, lleEps=0.0,
              seedChunk=0, firstPoint=0, nPoints=0, flags=0, peakCapacity=0, regimeTime=0.0,
-             pointIndex=0) -> Job:
+             pointIndex=0, regimeMinAmp=0.0, regimeChaosLle=0.0) -> Job:
     j = Job()
     lib().cbf_job_init(C.byref(j))
     dims = len(idxMut)
@@ -237,6 +316,8 @@ def make_job(*, task, system, nPts, ranges, idxMut, ic, values, h, tMax=0.0, tra
     j.firstPoint, j.nPoints, j.flags, j.peakCapacity = firstPoint, nPoints, flags, peakCapacity
     j.regimeTime = regimeTime
     j.pointIndex = pointIndex or None
+    j.regimeMinAmp = regimeMinAmp
+    j.regimeChaosLle = regimeChaosLle
     return j
 
 
@@ -346,6 +427,92 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+class Mlp:
+    """The surrogate network (cbf_mlp_*): 4 -> 256 x3 (SiLU) -> 17, BF16 tensor-core
+    kernels with FP32 accumulation.  Device arrays are raw pointers."""
+
+    def __init__(self, batch: int, seed: int = 0):
+        h = C.c_void_p()
+        check(lib().cbf_mlp_create(batch, seed, C.byref(h)))
+        self.handle = h
+        self.batch = batch
+
+    @staticmethod
+    def num_params() -> int:
+        return int(lib().cbf_mlp_num_params())
+
+    def get_params(self) -> np.ndarray:
+        p = np.zeros(self.num_params(), np.float32)
+        check(lib().cbf_mlp_get_params(self.handle, p.ctypes.data_as(C.POINTER(C.c_float)), p.size))
+        return p
+
+    def set_params(self, p) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        check(lib().cbf_mlp_set_params(self.handle, p.ctypes.data_as(C.POINTER(C.c_float)), p.size))
+
+    def forward_backward(self, x, y_lle, y_cls, w_lle: float = 1.0):
+        """One pass on host rows; returns (loss, grads, out[n, 17])."""
+        fp = C.POINTER(C.c_float)
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, 4)
+        yl = np.ascontiguousarray(y_lle, np.float32)
+        yc = np.ascontiguousarray(y_cls, np.int32)
+        n = x.shape[0]
+        loss = C.c_float(0.0)
+        g = np.zeros(self.num_params(), np.float32)
+        out = np.zeros((n, 17), np.float32)
+        check(lib().cbf_mlp_forward_backward(self.handle, x.ctypes.data_as(fp), yl.ctypes.data_as(fp),
+                                             yc.ctypes.data_as(_ip), n, w_lle, C.byref(loss),
+                                             g.ctypes.data_as(fp), out.ctypes.data_as(fp)))
+        return float(loss.value), g, out
+
+    def train(self, d_x: int, d_yl: int, d_yc: int, n: int, steps: int, lr: float,
+              horizon: int = 0, w_lle: float = 1.0, stream: int = 0, losses: bool = False):
+        buf = np.zeros(max(steps, 1), np.float32) if losses else None
+        check(lib().cbf_mlp_train(self.handle, C.c_void_p(d_x), C.c_void_p(d_yl), C.c_void_p(d_yc), n,
+                                  steps, lr, horizon, w_lle,
+                                  None if buf is None else buf.ctypes.data_as(C.POINTER(C.c_float)),
+                                  C.c_void_p(stream or None)))
+        return buf[:steps] if buf is not None else None
+
+    def predict(self, d_x: int, n: int, lle_mean: float, lle_std: float, d_lle: int = 0, d_cls: int = 0,
+                d_conf: int = 0, stream: int = 0) -> None:
+        check(lib().cbf_mlp_predict(self.handle, C.c_void_p(d_x), n, lle_mean, lle_std,
+                                    C.c_void_p(d_lle or None), C.c_void_p(d_cls or None),
+                                    C.c_void_p(d_conf or None), C.c_void_p(stream or None)))
+
+    def close(self):
+        if self.handle:
+            lib().cbf_mlp_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def surrogate_config(**kw) -> SurrogateConfig:
+    """Defaults of cbf_surrogate_config_init, overridden by keyword."""
+    c = SurrogateConfig()
+    lib().cbf_surrogate_config_init(C.byref(c))
+    for k, v in kw.items():
+        if not hasattr(c, k):
+            raise AttributeError(k)
+        setattr(c, k, v)
+    return c
+
+
+def lle_map_surrogate(job: Job, cfg: SurrogateConfig, d_lle: int, d_cls: int, d_src: int = 0,
+                      stream: int = 0) -> SurrogateReport:
+    """Surrogate-refined LLE + regime map into device buffers; returns the report."""
+    rep = SurrogateReport()
+    check(lib().cbf_lle_map_surrogate(C.byref(job), C.byref(cfg), C.c_void_p(d_lle), C.c_void_p(d_cls),
+                                      C.c_void_p(d_src or None), C.byref(rep),
+                                      C.c_void_p(stream or None)))
+    return rep
 
 
 def set_lle_variant(system, variant: int) -> None:

@@ -235,6 +235,9 @@ cbf_status lower_job(const cbf_job* j, DevJob* d)
             if (!to_int(j->regimeTime / j->h, &d->regimeSteps) || d->regimeSteps < 0)
                 return fail(CBF_ERR_INVALID_ARG, "regimeTime/h must be in [0, 2^31)");
             d->maxPeaks = j->maxAmountOfPeaks;
+            if (!(j->regimeMinAmp >= 0)) return fail(CBF_ERR_INVALID_ARG, "regimeMinAmp must be >= 0");
+            d->regimeMinAmp = j->regimeMinAmp;
+            d->regimeChaosLle = j->regimeChaosLle;
             const int half = d->regimeSteps / 2 > 0 ? d->regimeSteps / 2 : 1;
             const int cap = j->maxAmountOfPeaks < half ? j->maxAmountOfPeaks : half;
             d->peakCap = cap > 0 ? cap : 1;

@@ -30,6 +30,8 @@ struct DevJob {
     long long seedChunk;
     const long long* pointIndex;  // optional device list of grid indices (see cbf_job)
     int regimeSteps;    // LLE_REGIME: recorded steps after the transient
+    double regimeMinAmp;  // LLE_REGIME: window range below this -> class 0
+    double regimeChaosLle;  // LLE_REGIME: > 0 and LLE above it -> class 15
     int nPts, dims, nIC, nV;
     int idxMut0, idxMut1;
     int writableVar, preScaller;
@@ -154,6 +156,8 @@ cudaError_t launch_bif(const DevJob& J, void* d_out, int* d_aux, cudaStream_t s)
 cudaError_t launch_grid_coords(const DevJob& J, double* d_out, cudaStream_t s);
 cudaError_t launch_lle_seeds(const DevJob& J, double* d_out, cudaStream_t s);
 cudaError_t launch_lle_regime(const DevJob& J, double* d_lle, int* d_class, cudaStream_t s);
+// Points the LLE_REGIME kernel keeps in flight at once on the current device.
+long long lle_regime_resident_points(const DevJob& J);
 // KDE/DBSCAN with caller-provided scratch (no allocation): `scratch` holds
 // `scratchBytes` of peak buffers, `err` one int that must be zero on entry.
 // Synchronises `s` to read `err`.

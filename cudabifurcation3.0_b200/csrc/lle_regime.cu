@@ -7,8 +7,11 @@
 // fed to the streaming peak finder; the class is the reference's DBSCAN cluster
 // count of those (peak, interval) pairs (dbscan, cudaLibrary.cu:457-529), with
 //   0  when the trajectory diverged inside the window or has no peaks,
-//   15 when it has more than maxAmountOfPeaks peaks (or 15 or more clusters).
-// The window costs one peak-state update per step on top of the LLE; the
+//   15 when its LLE exceeds regimeChaosLle (if > 0; no clustering needed), when
+//      it has more than maxAmountOfPeaks peaks, or 15 or more clusters.
+// A window whose samples span less than regimeMinAmp is class 0 as well: an
+// equilibrium reached to FP64 precision can still wobble by an ulp and show
+// spurious peaks.  The window costs one peak-state update per step on top of the LLE; the
 // transient is shared.  This is the plain FP64 method that labels the surrogate's
 // training data and recomputes the points it cannot be trusted with.
 #include "bif_device.cuh"
@@ -22,10 +25,10 @@ constexpr int kRegThreads = kRegWarps * 32;
 constexpr int kNumClasses = 16;
 
 // One point: returns the LLE; *n = emitted peaks in the window, -1 if the
-// divergence test fired inside it.
+// divergence test fired inside it; *amp = max - min of the window's samples.
 template <class S, bool IC>
 __device__ double lle_regime_point(const DevJob& J, long long g, double* pk, double* iv, int cap,
-                                   int* nOut)
+                                   int* nOut, double* amp)
 {
     constexpr int D = S::DIM;
     double x[1][D], y[1][D];
@@ -44,6 +47,7 @@ __device__ double lle_regime_point(const DevJob& J, long long g, double* pk, dou
     }
     PeakStream ps;
     ps.init();
+    double lo = INFINITY, hi = -INFINITY;
     bool regimeDiv = false;
     int t = 0;  // step index since the transient
     double result = 0;
@@ -53,7 +57,12 @@ __device__ double lle_regime_point(const DevJob& J, long long g, double* pk, dou
             bool ax = true, ay = true;
             for (int i = 0; i < J.nNT; ++i, ++t) {
                 if (ax) {
-                    if (t < J.regimeSteps) ps.push<true>(pick<D>(x[0], J.writableVar), t, pk, iv, cap);
+                    if (t < J.regimeSteps) {
+                        const double v = pick<D>(x[0], J.writableVar);
+                        lo = fmin(lo, v);
+                        hi = fmax(hi, v);
+                        ps.push<true>(v, t, pk, iv, cap);
+                    }
                     S::step(x[0], c[0]);
                     if (J.checkDiv && diverged(x[0][0], J.divThresh)) {
                         ax = false;
@@ -79,6 +88,7 @@ __device__ double lle_regime_point(const DevJob& J, long long g, double* pk, dou
         for (int i = 0; i < D; ++i) y[0][i] = x[0][i] - ((x[0][i] - y[0][i]) * tt);
     }
     *nOut = regimeDiv ? -1 : ps.emitted();
+    *amp = hi - lo;
     return result / J.tMax;
 }
 
@@ -104,15 +114,18 @@ __global__ void __launch_bounds__(kRegThreads) lle_regime_kernel(const DevJob J,
         double* myPk = scrPk + (slot0 + lane) * (long long)cap;
         double* myIv = scrIv + (slot0 + lane) * (long long)cap;
         int n = 0;
-        double lv = 0;
-        if (valid) lv = lle_regime_point<S, IC>(J, grid_index(J, p), myPk, myIv, cap, &n);
+        double lv = 0, amp = 0;
+        if (valid) lv = lle_regime_point<S, IC>(J, grid_index(J, p), myPk, myIv, cap, &n, &amp);
+        if (amp < J.regimeMinAmp) n = 0;  // no oscillation
         __syncwarp();
         int res = 0;
         const int live = (int)min(32ll, J.nPoints - tile * 32);
         for (int j = 0; j < live; ++j) {
             const int nj = __shfl_sync(kFull, n, j);
+            const double lj = __shfl_sync(kFull, lv, j);
             int r;
             if (nj <= 0) r = 0;
+            else if (J.regimeChaosLle > 0 && lj > J.regimeChaosLle) r = kNumClasses - 1;
             else if (nj > J.maxPeaks) r = kNumClasses - 1;
             else {
                 const double* pk = scrPk + (slot0 + j) * (long long)cap;
@@ -184,7 +197,34 @@ cudaError_t launch_s(const DevJob& J, double* d_lle, int* d_cls, cudaStream_t s)
     return J.sweepIC ? launch_t<S, true>(J, d_lle, d_cls, s) : launch_t<S, false>(J, d_lle, d_cls, s);
 }
 
+template <class S>
+long long resident_s(const DevJob& J)
+{
+    const int bitWords = (J.peakCap + 31) / 32;
+    const size_t smemBytes = (size_t)kRegWarps * 2 * bitWords * sizeof(unsigned);
+    auto kern = J.sweepIC ? lle_regime_kernel<S, true> : lle_regime_kernel<S, false>;
+    if (smemBytes > 48 * 1024)
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBytes);
+    int dev = 0, sms = 0, perSm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, kRegThreads, smemBytes) != cudaSuccess)
+        return 0;
+    return (long long)sms * perSm * kRegThreads;
+}
+
 }  // namespace
+
+long long lle_regime_resident_points(const DevJob& J)
+{
+    switch (J.system) {
+    case CBF_SYS_MEMRISTIVE5: return resident_s<Memristive5>(J);
+    case CBF_SYS_ROSSLER: return resident_s<Rossler>(J);
+    case CBF_SYS_LORENZ: return resident_s<Lorenz>(J);
+    case CBF_SYS_CHEN: return resident_s<Chen>(J);
+    default: return 0;
+    }
+}
 
 cudaError_t launch_lle_regime(const DevJob& J, double* d_lle, int* d_cls, cudaStream_t s)
 {

@@ -1,0 +1,598 @@
+// Surrogate-refined LLE + regime map of a 2-D parameter sweep.
+//
+// The plain FP64 method (the LLE_REGIME kernels: LLEKernelCUDA semantics plus the
+// peak-count regime class) labels a coarse sub-grid of the map -- every
+// (nPts/coarseSide)-th row and column -- and a seeded random sample of points.
+// The network of mlp.cu is trained on those labels on the GPU, predicts LLE,
+// class and confidence for every grid point, and the plain method then
+// recomputes every point
+//   * on a predicted regime boundary (a neighbour within boundaryRadius has
+//     another predicted class),
+//   * whose softmax confidence is below confThreshold,
+//   * in a seeded random audit sample (auditFraction of the grid).
+// Wherever the plain class of a label or a recomputed point differs from the
+// network's, its neighbours (expandRadius) are recomputed in a further wave, until
+// a wave finds no new disagreement: thin structures the network cannot resolve
+// (periodic windows inside chaos) are traced from any point that hits them.
+// Labelled and recomputed points carry plain values; the rest carry the
+// network's prediction.  The audit points that no other rule selected measure
+// the error of the kept predictions.  Everything runs on one stream; the host
+// only sizes the recompute list and normalises the LLE targets.
+#include <math.h>
+#include <string.h>
+
+#include <vector>
+
+#include "mlp.cuh"
+
+namespace cbf {
+namespace {
+
+constexpr int kChunk = 4096;          // points per compaction block
+constexpr int kChunkThreads = 256;
+// flag bits: reasons to recompute, then the point's state
+constexpr unsigned char kBoundary = 1, kLowConf = 2, kAudit = 4, kExpand = 8;
+constexpr unsigned char kReasons = kBoundary | kLowConf | kAudit | kExpand;
+constexpr unsigned char kDone = 0x40, kLabel = 0x80;
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z)
+{
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Training points: the coarse sub-grid (cs x cs, stride `stride`) then nRand
+// seeded random grid points.  Grid index g = row * nPts + column (axis 0 fastest).
+__global__ void label_index_kernel(long long* __restrict__ idx, int cs, int stride, int nPts, long long nRand,
+                                   long long nPoints, unsigned long long seed)
+{
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nCoarse = (long long)cs * cs;
+    if (k >= nCoarse + nRand) return;
+    if (k < nCoarse) {
+        const long long r = k / cs, c = k % cs;
+        idx[k] = r * stride * (long long)nPts + c * stride;
+    } else {
+        idx[k] = (long long)(mix64(seed ^ mix64((unsigned long long)k)) % (unsigned long long)nPoints);
+    }
+}
+
+// Labels into the map.  surprise[k]: the network's class at the label's point
+// differed from the plain class (of duplicated points at least the first
+// reader sees the prediction, so the set of surprised points is deterministic).
+__global__ void label_scatter_kernel(const long long* __restrict__ idx, long long n, const double* __restrict__ lle,
+                                     const int* __restrict__ cls, double* __restrict__ mapLle,
+                                     int* __restrict__ mapCls, unsigned char* __restrict__ flag,
+                                     unsigned char* __restrict__ src, unsigned char* __restrict__ surprise)
+{
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const long long g = idx[k];
+    surprise[k] = mapCls[g] != cls[k];
+    mapLle[g] = lle[k];
+    mapCls[g] = cls[k];
+    flag[g] = kLabel;
+    src[g] = 1;
+}
+
+// Refinement reasons of every grid point from the predicted classes/confidences.
+__global__ void mask_kernel(const int* __restrict__ cls, const float* __restrict__ conf, int nPts, long long nPoints,
+                            int radius, float confThr, unsigned long long auditCut, unsigned long long seed,
+                            unsigned char* __restrict__ flag, unsigned char* __restrict__ src)
+{
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= nPoints) return;
+    const int row = (int)(g / nPts), col = (int)(g % nPts);
+    const int c = cls[g];
+    unsigned char f = 0;
+    for (int dr = -radius; dr <= radius && !(f & kBoundary); ++dr) {
+        const int r = row + dr;
+        if (r < 0 || r >= nPts) continue;
+        for (int dc = -radius; dc <= radius; ++dc) {
+            const int q = col + dc;
+            if (q < 0 || q >= nPts) continue;
+            if (cls[(long long)r * nPts + q] != c) {
+                f |= kBoundary;
+                break;
+            }
+        }
+    }
+    if (!(conf[g] >= confThr)) f |= kLowConf;
+    if (mix64(seed ^ mix64((unsigned long long)g + 0x5851F42D4C957F2Dull)) < auditCut) f |= kAudit;
+    flag[g] = f;
+    src[g] = 0;
+}
+
+// Points with one of the `want` reasons that are neither labels nor computed.
+__device__ __forceinline__ bool selected(unsigned char f, unsigned char want)
+{
+    return (f & want) && !(f & (kLabel | kDone));
+}
+
+__global__ void __launch_bounds__(kChunkThreads) count_kernel(const unsigned char* __restrict__ flag, long long n,
+                                                              unsigned char want, int* __restrict__ blockCount)
+{
+    const long long base = (long long)blockIdx.x * kChunk;
+    int total = 0;
+    for (int r = 0; r < kChunk; r += kChunkThreads) {
+        const long long g = base + r + threadIdx.x;
+        total += __syncthreads_count(g < n && selected(flag[g], want));
+    }
+    if (threadIdx.x == 0) blockCount[blockIdx.x] = total;
+}
+
+// Exclusive prefix over nb block counts (one block of 1024 threads);
+// offsets[nb] = total.
+__global__ void __launch_bounds__(1024) scan_kernel(const int* __restrict__ blockCount, int nb,
+                                                    long long* __restrict__ offsets)
+{
+    __shared__ long long part[1024];
+    const int per = (nb + 1023) / 1024;
+    const int b0 = threadIdx.x * per;
+    long long s = 0;
+    for (int i = 0; i < per && b0 + i < nb; ++i) s += blockCount[b0 + i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int d = 1; d < 1024; d <<= 1) {
+        const long long v = threadIdx.x >= d ? part[threadIdx.x - d] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    long long run = part[threadIdx.x] - s;  // exclusive
+    for (int i = 0; i < per && b0 + i < nb; ++i) {
+        offsets[b0 + i] = run;
+        run += blockCount[b0 + i];
+    }
+    if (threadIdx.x == 1023) offsets[nb] = part[1023];
+}
+
+// Selected grid indices in ascending order.
+__global__ void __launch_bounds__(kChunkThreads) compact_kernel(const unsigned char* __restrict__ flag, long long n,
+                                                                unsigned char want,
+                                                                const long long* __restrict__ offsets,
+                                                                long long* __restrict__ list)
+{
+    __shared__ int warpTot[kChunkThreads / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    long long out = offsets[blockIdx.x];
+    const long long base = (long long)blockIdx.x * kChunk;
+    for (int r = 0; r < kChunk; r += kChunkThreads) {
+        const long long g = base + r + threadIdx.x;
+        const bool sel = g < n && selected(flag[g], want);
+        const unsigned ball = __ballot_sync(0xffffffffu, sel);
+        if (lane == 0) warpTot[w] = __popc(ball);
+        __syncthreads();
+        int before = 0, all = 0;
+        for (int i = 0; i < kChunkThreads / 32; ++i) {
+            if (i < w) before += warpTot[i];
+            all += warpTot[i];
+        }
+        if (sel) list[out + before + __popc(ball & ((1u << lane) - 1u))] = g;
+        out += all;
+        __syncthreads();
+    }
+}
+
+struct Stats {
+    unsigned long long boundary, lowConf, audit, auditOnly, auditOnlyAgree, changed, expanded;
+    double errSum;
+    unsigned long long errMaxBits;
+};
+
+// Plain results into the map; statistics of the predictions they replace;
+// surprise[k] = the plain class differs from the predicted one.
+__global__ void merge_kernel(const long long* __restrict__ list, long long n, const double* __restrict__ rl,
+                             const int* __restrict__ rc, unsigned char* __restrict__ flag,
+                             double* __restrict__ mapLle, int* __restrict__ mapCls,
+                             unsigned char* __restrict__ src, unsigned char* __restrict__ surprise, Stats* st)
+{
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long b = 0, lc = 0, au = 0, ao = 0, aa = 0, ch = 0, ex = 0;
+    double es = 0, em = 0;
+    if (k < n) {
+        const long long g = list[k];
+        const unsigned char f = flag[g];
+        const int pc = mapCls[g];
+        const double pl = mapLle[g];
+        b = (f & kBoundary) != 0;
+        lc = (f & kLowConf) != 0;
+        au = (f & kAudit) != 0;
+        ex = (f & kReasons) == kExpand;
+        ch = pc != rc[k];
+        surprise[k] = (unsigned char)ch;
+        if (f == kAudit) {
+            ao = 1;
+            aa = pc == rc[k];
+            const double err = fabs(pl - rl[k]);
+            if (isfinite(err)) {
+                es = err;
+                em = err;
+            }
+        }
+        mapLle[g] = rl[k];
+        mapCls[g] = rc[k];
+        src[g] = 2;
+        flag[g] = f | kDone;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        b += __shfl_down_sync(0xffffffffu, b, o);
+        lc += __shfl_down_sync(0xffffffffu, lc, o);
+        au += __shfl_down_sync(0xffffffffu, au, o);
+        ao += __shfl_down_sync(0xffffffffu, ao, o);
+        aa += __shfl_down_sync(0xffffffffu, aa, o);
+        ch += __shfl_down_sync(0xffffffffu, ch, o);
+        ex += __shfl_down_sync(0xffffffffu, ex, o);
+        es += __shfl_down_sync(0xffffffffu, es, o);
+        em = fmax(em, __shfl_down_sync(0xffffffffu, em, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (b) atomicAdd(&st->boundary, b);
+        if (lc) atomicAdd(&st->lowConf, lc);
+        if (au) atomicAdd(&st->audit, au);
+        if (ao) atomicAdd(&st->auditOnly, ao);
+        if (aa) atomicAdd(&st->auditOnlyAgree, aa);
+        if (ch) atomicAdd(&st->changed, ch);
+        if (ex) atomicAdd(&st->expanded, ex);
+        if (es != 0) atomicAdd(&st->errSum, es);
+        if (em > 0) atomicMax(&st->errMaxBits, (unsigned long long)__double_as_longlong(em));
+    }
+}
+
+// Neighbours (Chebyshev radius) of every surprised point that no rule selected
+// and the plain method has not computed are marked for the next wave (rule-
+// selected points are computed in their own chunk and expand from there).
+__global__ void expand_kernel(const long long* __restrict__ list, const unsigned char* __restrict__ surprise,
+                              long long n, int nPts, int radius, unsigned char* __restrict__ flag)
+{
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n || !surprise[k]) return;
+    const long long g = list[k];
+    const int row = (int)(g / nPts), col = (int)(g % nPts);
+    for (int dr = -radius; dr <= radius; ++dr) {
+        const int r = row + dr;
+        if (r < 0 || r >= nPts) continue;
+        for (int dc = -radius; dc <= radius; ++dc) {
+            const int q = col + dc;
+            if (q < 0 || q >= nPts) continue;
+            const long long nb = (long long)r * nPts + q;
+            if (flag[nb] == 0) flag[nb] = kExpand;
+        }
+    }
+}
+
+template <class F>
+cudaError_t launch1d(long long n, cudaStream_t s, F f)
+{
+    if (n <= 0) return cudaSuccess;
+    f((unsigned)((n + 255) / 256), 256);
+    note_launch();
+    return cudaGetLastError();
+}
+
+struct DeviceBuffers {
+    std::vector<void*> ptrs;
+    template <class T>
+    cudaError_t get(T** p, long long n)
+    {
+        void* q = nullptr;
+        cudaError_t e = cudaMalloc(&q, (size_t)(n > 0 ? n : 1) * sizeof(T));
+        if (e == cudaSuccess) ptrs.push_back(q);
+        *p = (T*)q;
+        return e;
+    }
+    ~DeviceBuffers()
+    {
+        for (void* p : ptrs) cudaFree(p);
+    }
+};
+
+}  // namespace
+}  // namespace cbf
+
+using namespace cbf;
+
+extern "C" {
+
+void cbf_surrogate_config_init(cbf_surrogate_config* c)
+{
+    if (!c) return;
+    memset(c, 0, sizeof(*c));
+    c->coarseSide = 512;
+    c->randomPoints = 65536;
+    c->batch = 4096;
+    c->trainSteps = 4000;
+    c->lr = 2e-3f;
+    c->wLle = 1.0f;
+    c->confThreshold = 0.95f;
+    c->auditFraction = 0.01f;
+    c->boundaryRadius = 1;
+    c->refine = 1;
+    c->seed = 20240101ull;
+    c->expandRadius = -1;
+    c->maxWaves = 256;
+}
+
+cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config* cfg, double* dLle,
+                                 int32_t* dCls, uint8_t* dSource, cbf_surrogate_report* rep, void* stream)
+{
+    if (!job || !cfg || !dLle || !dCls) return report_error(CBF_ERR_INVALID_ARG, "null argument");
+    if (job->task != CBF_TASK_LLE_REGIME || job->dims != 2 || job->sweepIC)
+        return report_error(CBF_ERR_INVALID_ARG, "the surrogate map needs a 2-D LLE_REGIME parameter sweep");
+    if (job->system != CBF_SYS_ROSSLER && job->system != CBF_SYS_LORENZ && job->system != CBF_SYS_CHEN)
+        return report_error(CBF_ERR_INVALID_ARG, "the surrogate supports the Rossler, Lorenz and Chen systems");
+    if (job->pointIndex || job->firstPoint != 0 ||
+        (job->nPoints != 0 && job->nPoints != (int64_t)job->nPts * job->nPts))
+        return report_error(CBF_ERR_INVALID_ARG, "the surrogate map covers the whole grid");
+    if (job->nPts < 3 || cfg->coarseSide < 2 || cfg->randomPoints < 0 || cfg->batch < 1 ||
+        cfg->trainSteps < 0 || !(cfg->lr > 0) || cfg->boundaryRadius < 0 || cfg->boundaryRadius > 8 ||
+        cfg->expandRadius < -1 || cfg->expandRadius > 16 || cfg->maxWaves < 0 ||
+        !(cfg->auditFraction >= 0 && cfg->auditFraction <= 1))
+        return report_error(CBF_ERR_INVALID_ARG, "bad surrogate configuration");
+    DevJob dj;
+    cbf_status st = lower_job_for(job, &dj);
+    if (st != CBF_OK) return st;
+
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaStream_t own = nullptr;
+    if (!s) {
+        cudaDeviceSynchronize();
+        if (cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking) != cudaSuccess)
+            return report_cuda_error(cudaGetLastError(), "stream");
+        s = own;
+    }
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard()
+        {
+            if (s) cudaStreamDestroy(s);
+        }
+    } guard{own};
+
+    const int nPts = job->nPts;
+    const long long n = (long long)nPts * nPts;
+    const int cs = cfg->coarseSide < nPts ? cfg->coarseSide : nPts;
+    const int stride = nPts / cs;
+    const long long nLab = (long long)cs * cs + cfg->randomPoints;
+
+    cudaEvent_t ev[6];
+    for (auto& e : ev) cudaEventCreate(&e);
+    struct EventGuard {
+        cudaEvent_t* e;
+        ~EventGuard()
+        {
+            for (int i = 0; i < 6; ++i) cudaEventDestroy(e[i]);
+        }
+    } evGuard{ev};
+
+    DeviceBuffers buf;
+    long long* dIdx = nullptr;
+    double* labLle = nullptr;
+    int* labCls = nullptr;
+    float *X = nullptr, *yl = nullptr, *conf = nullptr;
+    unsigned char *flag = nullptr, *src = dSource;
+    int* blockCount = nullptr;
+    long long* offsets = nullptr;
+    Stats* stats = nullptr;
+    const int nb = (int)((n + kChunk - 1) / kChunk);
+    cudaError_t e = buf.get(&dIdx, nLab);
+    if (e == cudaSuccess) e = buf.get(&labLle, nLab);
+    if (e == cudaSuccess) e = buf.get(&labCls, nLab);
+    if (e == cudaSuccess) e = buf.get(&X, nLab * 4);
+    if (e == cudaSuccess) e = buf.get(&yl, nLab);
+    if (e == cudaSuccess) e = buf.get(&conf, n);
+    if (e == cudaSuccess) e = buf.get(&flag, n);
+    if (e == cudaSuccess && !src) e = buf.get(&src, n);
+    if (e == cudaSuccess) e = buf.get(&blockCount, nb);
+    if (e == cudaSuccess) e = buf.get(&offsets, (long long)nb + 1);
+    if (e == cudaSuccess) e = buf.get(&stats, 1);
+    if (e != cudaSuccess) return report_cuda_error(e, "surrogate map buffers");
+
+    // 1. plain labels
+    cudaEventRecord(ev[0], s);
+    e = launch1d(nLab, s, [&](unsigned b, int t) {
+        label_index_kernel<<<b, t, 0, s>>>(dIdx, cs, stride, nPts, cfg->randomPoints, n, cfg->seed);
+    });
+    if (e != cudaSuccess) return report_cuda_error(e, "label points");
+    cbf_job lj = *job;
+    lj.pointIndex = (const int64_t*)dIdx;
+    lj.nPoints = nLab;
+    lj.firstPoint = 0;
+    if ((st = cbf_run(&lj, labLle, labCls, s)) != CBF_OK) return st;
+
+    // LLE normalisation on the host (finite labels), targets clipped to +-8 sd.
+    std::vector<double> hl(nLab);
+    e = cudaMemcpyAsync(hl.data(), labLle, nLab * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return report_cuda_error(e, "label readback");
+    double sum = 0, sum2 = 0;
+    long long cnt = 0;
+    for (double v : hl)
+        if (isfinite(v)) {
+            sum += v;
+            sum2 += v * v;
+            ++cnt;
+        }
+    const double mean = cnt ? sum / cnt : 0.0;
+    double sd = cnt ? sqrt(fmax(sum2 / cnt - mean * mean, 0.0)) : 1.0;
+    if (!(sd > 1e-12)) sd = 1.0;
+    std::vector<float> hy(nLab);
+    for (long long i = 0; i < nLab; ++i) {
+        const double v = hl[i];
+        const double z = isfinite(v) ? (v - mean) / sd : 0.0;
+        hy[i] = (float)fmin(8.0, fmax(-8.0, z));
+    }
+    e = cudaMemcpyAsync(yl, hy.data(), nLab * sizeof(float), cudaMemcpyHostToDevice, s);
+    const FeatureSpec fs = feature_spec(dj);
+    if (e == cudaSuccess) e = mlp_features(fs, dIdx, nLab, X, s);
+    if (e != cudaSuccess) return report_cuda_error(e, "training set");
+    cudaEventRecord(ev[1], s);
+
+    // 2. training
+    cbf_mlp* net = nullptr;
+    if ((st = cbf_mlp_create(cfg->batch, cfg->seed, &net)) != CBF_OK) return st;
+    struct NetGuard {
+        cbf_mlp* m;
+        ~NetGuard() { cbf_mlp_destroy(m); }
+    } netGuard{net};
+    const int tail = cfg->trainSteps < 100 ? cfg->trainSteps : 100;
+    std::vector<float> losses(tail > 0 ? tail : 1, 0.f);
+    st = cbf_mlp_train(net, X, yl, labCls, nLab, cfg->trainSteps - tail, cfg->lr, cfg->trainSteps, cfg->wLle,
+                       nullptr, s);
+    if (st == CBF_OK && tail > 0)
+        st = cbf_mlp_train(net, X, yl, labCls, nLab, tail, cfg->lr, cfg->trainSteps, cfg->wLle, losses.data(), s);
+    if (st != CBF_OK) return st;
+    cudaEventRecord(ev[2], s);
+
+    // 3. prediction on every grid point
+    e = mlp_predict_grid(net, fs, n, (float)mean, (float)sd, dLle, dCls, conf, s);
+    if (e != cudaSuccess) return report_cuda_error(e, "prediction");
+    cudaEventRecord(ev[3], s);
+
+    // 4. refinement mask, labels into the map (surprised labels seed the expansion)
+    const double frac = cfg->refine ? cfg->auditFraction : 0.0;
+    const unsigned long long auditCut =
+        frac >= 1.0 ? ~0ull : (unsigned long long)(frac * 18446744073709551616.0);
+    const float thr = cfg->refine ? cfg->confThreshold : -1.0f;
+    const int radius = cfg->refine ? cfg->boundaryRadius : 0;  // radius 0 marks no boundary
+    // expansion radius: automatic = one grid step per 2048 points of side, so
+    // the number of waves needed to trace a structure does not grow with nPts
+    const int autoR = (nPts + 2047) / 2048;
+    const int er = cfg->refine ? (cfg->expandRadius < 0 ? autoR : cfg->expandRadius) : 0;
+    unsigned char* lsur = nullptr;
+    if ((e = buf.get(&lsur, nLab)) != cudaSuccess) return report_cuda_error(e, "label buffers");
+    e = launch1d(n, s, [&](unsigned b, int t) {
+        mask_kernel<<<b, t, 0, s>>>(dCls, conf, nPts, n, radius, thr, auditCut,
+                                    cfg->seed ^ 0xA0761D6478BD642Full, flag, src);
+    });
+    if (e == cudaSuccess)
+        e = launch1d(nLab, s, [&](unsigned b, int t) {
+            label_scatter_kernel<<<b, t, 0, s>>>(dIdx, nLab, labLle, labCls, dLle, dCls, flag, src, lsur);
+        });
+    if (e == cudaSuccess && er > 0)
+        e = launch1d(nLab, s, [&](unsigned b, int t) {
+            expand_kernel<<<b, t, 0, s>>>(dIdx, lsur, nLab, nPts, er, flag);
+        });
+    if (e == cudaSuccess) e = cudaMemsetAsync(stats, 0, sizeof(Stats), s);
+    if (e != cudaSuccess) return report_cuda_error(e, "refinement mask");
+    cudaEventRecord(ev[4], s);
+
+    // 5. plain recompute in rounds.  The rule-selected points (ascending grid
+    // index) are fed in chunks; every round also takes all points the expansion
+    // marked in the previous rounds, so the chain of expansion waves overlaps
+    // the bulk of the recompute.  A round is sized to about two waves of
+    // resident threads of the LLE_REGIME kernel.
+    auto select = [&](unsigned char want, long long* out, long long* count) -> cudaError_t {
+        count_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, want, blockCount);
+        scan_kernel<<<1, 1024, 0, s>>>(blockCount, nb, offsets);
+        note_launch(2);
+        cudaError_t ce = cudaGetLastError();
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(count, offsets + nb, sizeof(long long), cudaMemcpyDeviceToHost, s);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+        if (ce == cudaSuccess && out && *count > 0) {
+            compact_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, want, offsets, out);
+            note_launch();
+            ce = cudaGetLastError();
+        }
+        return ce;
+    };
+    long long n0 = 0;
+    if ((e = select(kBoundary | kLowConf | kAudit, nullptr, &n0)) != cudaSuccess)
+        return report_cuda_error(e, "recompute list");
+    long long* rule = nullptr;
+    if ((e = buf.get(&rule, n0)) != cudaSuccess) return report_cuda_error(e, "recompute list");
+    if (n0 > 0 && (e = select(kBoundary | kLowConf | kAudit, rule, &n0)) != cudaSuccess)
+        return report_cuda_error(e, "recompute list");
+    long long resident = lle_regime_resident_points(dj);
+    if (resident < 4096) resident = 4096;
+    const long long target = 2 * resident;
+    long long* list = nullptr;
+    double* rl = nullptr;
+    int* rc = nullptr;
+    unsigned char* sur = nullptr;
+    long long cap = 0, refined = 0, pos = 0;
+    int waves = 0;
+    for (int w = 0;; ++w) {
+        // the expansion marks of the previous rounds (counted first: sizes the chunk)
+        long long nA = 0;
+        if ((e = select(kExpand, nullptr, &nA)) != cudaSuccess) return report_cuda_error(e, "expansion list");
+        long long nB = target - nA > target / 4 ? target - nA : target / 4;
+        if (nB > n0 - pos) nB = n0 - pos;
+        const long long nSel = nA + nB;
+        if (nSel == 0) break;
+        if (nSel > cap) {
+            cap = nSel > 2 * cap ? nSel : 2 * cap;
+            e = buf.get(&list, cap);
+            if (e == cudaSuccess) e = buf.get(&rl, cap);
+            if (e == cudaSuccess) e = buf.get(&rc, cap);
+            if (e == cudaSuccess) e = buf.get(&sur, cap);
+            if (e != cudaSuccess) return report_cuda_error(e, "recompute buffers");
+        }
+        if (nA > 0 && (e = select(kExpand, list, &nA)) != cudaSuccess) return report_cuda_error(e, "expansion list");
+        if (nB > 0 && (e = cudaMemcpyAsync(list + nA, rule + pos, nB * sizeof(long long), cudaMemcpyDeviceToDevice,
+                                           s)) != cudaSuccess)
+            return report_cuda_error(e, "recompute list");
+        cbf_job rj = *job;
+        rj.pointIndex = (const int64_t*)list;
+        rj.nPoints = nSel;
+        rj.firstPoint = 0;
+        if ((st = cbf_run(&rj, rl, rc, s)) != CBF_OK) return st;
+        e = launch1d(nSel, s, [&](unsigned b, int t) {
+            merge_kernel<<<b, t, 0, s>>>(list, nSel, rl, rc, flag, dLle, dCls, src, sur, stats);
+        });
+        if (e == cudaSuccess && er > 0 && w < cfg->maxWaves)
+            e = launch1d(nSel, s, [&](unsigned b, int t) {
+                expand_kernel<<<b, t, 0, s>>>(list, sur, nSel, nPts, er, flag);
+            });
+        if (e != cudaSuccess) return report_cuda_error(e, "merge");
+        pos += nB;
+        refined += nSel;
+        waves = w + 1;
+    }
+    Stats hs;
+    memset(&hs, 0, sizeof(hs));
+    e = cudaMemcpyAsync(&hs, stats, sizeof(Stats), cudaMemcpyDeviceToHost, s);
+    cudaEventRecord(ev[5], s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return report_cuda_error(e, "recompute");
+
+    if (rep) {
+        memset(rep, 0, sizeof(*rep));
+        rep->points = n;
+        rep->labelled = nLab;
+        rep->refined = refined;
+        rep->expanded = (int64_t)hs.expanded;
+        rep->waves = waves;
+        rep->boundary = (int64_t)hs.boundary;
+        rep->lowConfidence = (int64_t)hs.lowConf;
+        rep->audit = (int64_t)hs.audit;
+        rep->auditOnly = (int64_t)hs.auditOnly;
+        rep->auditOnlyAgree = (int64_t)hs.auditOnlyAgree;
+        rep->refinedChanged = (int64_t)hs.changed;
+        rep->auditOnlyLleMeanAbsErr = hs.auditOnly ? hs.errSum / (double)hs.auditOnly : 0.0;
+        double mx;
+        memcpy(&mx, &hs.errMaxBits, sizeof(mx));
+        rep->auditOnlyLleMaxAbsErr = mx;
+        rep->lleMean = mean;
+        rep->lleStd = sd;
+        double ls = 0;
+        for (int i = 0; i < tail; ++i) ls += losses[i];
+        rep->finalLoss = tail ? (float)(ls / tail) : 0.f;
+        float ms[5];
+        for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]);
+        rep->msLabel = ms[0];
+        rep->msTrain = ms[1];
+        rep->msPredict = ms[2];
+        rep->msMask = ms[3];
+        rep->msRefine = ms[4];
+        float tot = 0;
+        cudaEventElapsedTime(&tot, ev[0], ev[5]);
+        rep->msTotal = tot;
+    }
+    return CBF_OK;
+}
+
+}  // extern "C"

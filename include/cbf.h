@@ -56,7 +56,11 @@ typedef int32_t cbf_status;
 #define CBF_TASK_DBSCAN 2       /* DBSCAN cluster count per point (int32) */
 #define CBF_TASK_LLE 3          /* largest Lyapunov exponent per point (double) */
 #define CBF_TASK_TRAJECTORY 4   /* recorded x[writableVar] samples per point (+diverged flags) */
-#define CBF_TASK_LLE_REGIME 5   /* LLE (double) + peak-count regime class 0..15 (int32, in d_aux) */
+#define CBF_TASK_LLE_REGIME 5   /* LLE (double) + peak-count regime class 0..15 (int32, in d_aux):
+                                   0 no oscillation in the window (no peak, range below
+                                   regimeMinAmp, or diverged), 15 chaotic (LLE above
+                                   regimeChaosLle), more than maxAmountOfPeaks peaks or >= 15
+                                   clusters, else the DBSCAN cluster count */
 
 /* Job flags. */
 #define CBF_FLAG_EXACT_GRID 1u  /* integer grid index instead of the FP32 quirk */
@@ -100,6 +104,13 @@ typedef struct cbf_job {
     const int64_t* pointIndex;      /* optional DEVICE array: point k of the job is grid
                                        index pointIndex[k] (nPoints entries) instead of
                                        firstPoint + k; outputs stay compact */
+    double regimeMinAmp;            /* LLE_REGIME: a window whose peak-to-trough range of
+                                       x[writableVar] is below this is class 0 (no
+                                       oscillation: an equilibrium whose FP64 state still
+                                       wobbles by ulps shows spurious peaks); 0 disables */
+    double regimeChaosLle;          /* LLE_REGIME: if > 0, points (with an oscillation)
+                                       whose LLE exceeds it are class 15 (chaotic) without
+                                       clustering their peaks */
 } cbf_job;
 
 /* ---- library ---------------------------------------------------------- */
@@ -166,6 +177,90 @@ cbf_status cbf_batch_check(cbf_batch* batch);
  * drops a captured graph.  msPerCandidate (optional, 8 entries; -1 = skipped). */
 cbf_status cbf_batch_autotune(cbf_batch* batch, void* stream, int32_t* blocksPerSm,
                               double* msPerCandidate);
+
+/* ---- the surrogate network ------------------------------------------- */
+/* MLP 4 -> 256 -> 256 -> 256 -> 17 (SiLU): output 0 = normalised LLE, outputs
+ * 1..16 = logits of the 16-way peak-count regime class.  BF16 tensor-core GEMMs
+ * with FP32 accumulation for forward and backward, FP32 master weights, Adam.
+ * No counterpart in the reference.  Parameters are one flat FP32 vector: W1[256x4]
+ * b1 W2[256x256] b2 W3[256x256] b3 W4[17x256] b4 (W row-major [out][in]). */
+typedef struct cbf_mlp cbf_mlp;
+int64_t cbf_mlp_num_params(void);
+cbf_status cbf_mlp_create(int32_t batch, uint64_t seed, cbf_mlp** mlp);
+void cbf_mlp_destroy(cbf_mlp* mlp);
+cbf_status cbf_mlp_get_params(cbf_mlp* mlp, float* host, int64_t n);
+cbf_status cbf_mlp_set_params(cbf_mlp* mlp, const float* host, int64_t n);
+/* One forward and backward pass on n <= batch host rows (features x[n*4], LLE
+ * targets, classes) with loss = wLle*MSE(out0) + CE(out1..16), both batch means;
+ * returns loss, the flat gradient and the raw outputs (each optional). */
+cbf_status cbf_mlp_forward_backward(cbf_mlp* mlp, const float* x, const float* yLle,
+                                    const int32_t* yCls, int32_t n, float wLle, float* loss,
+                                    float* grads, float* out);
+/* `steps` Adam steps on minibatches drawn from the device training set (captured
+ * as a CUDA graph and replayed); the learning rate decays from lr to lr/20 on a
+ * cosine over `horizon` optimiser steps (0: constant); losses (optional, host)
+ * receives each step's loss.  cbf_mlp_set_params resets the optimiser state. */
+cbf_status cbf_mlp_train(cbf_mlp* mlp, const float* dX, const float* dYLle, const int32_t* dYCls,
+                         int64_t n, int32_t steps, float lr, int32_t horizon, float wLle,
+                         float* losses, void* stream);
+/* Predictions for n device feature rows: LLE = out0*lleStd + lleMean, class
+ * (argmax), confidence (softmax maximum); each output optional. */
+cbf_status cbf_mlp_predict(cbf_mlp* mlp, const float* dX, int64_t n, float lleMean, float lleStd,
+                           float* dLle, int32_t* dCls, float* dConf, void* stream);
+
+/* ---- surrogate-refined LLE + regime map -------------------------------- */
+/* No counterpart in the reference.  The plain method (CBF_TASK_LLE_REGIME)
+ * labels a coarse sub-grid (every (nPts/coarseSide)-th row and column) and
+ * randomPoints seeded random points; the network above is trained on them,
+ * predicts every grid point, and the plain method recomputes every point on a
+ * predicted regime boundary, below confThreshold softmax confidence, or in the
+ * random audit sample; then, in waves, the neighbours of every label or
+ * recomputed point whose plain class differs from the prediction.  Labelled and
+ * recomputed points carry plain values. */
+typedef struct cbf_surrogate_config {
+    int32_t coarseSide;      /* training sub-grid side (512) */
+    int32_t randomPoints;    /* extra random training points (65536) */
+    int32_t batch;           /* training minibatch rows (4096) */
+    int32_t trainSteps;      /* Adam steps, cosine learning-rate decay over them (4000) */
+    float lr;                /* peak learning rate (2e-3) */
+    float wLle;              /* weight of the LLE squared error in the loss (1) */
+    float confThreshold;     /* recompute points whose softmax maximum is below it (0.95) */
+    float auditFraction;     /* random audit sample of the grid, recomputed (0.01) */
+    int32_t boundaryRadius;  /* a neighbour within this Chebyshev radius with another
+                                predicted class marks a boundary point (1) */
+    int32_t refine;          /* 0: keep every prediction (ablation: network alone) */
+    uint64_t seed;           /* training points, minibatches, weights and audit sample */
+    int32_t expandRadius;    /* neighbours within this radius of a point whose plain class
+                                differs from the prediction are recomputed next; -1 (default):
+                                ceil(nPts / 2048); 0: no expansion */
+    int32_t maxWaves;        /* recompute rounds that may mark expansions (256) */
+} cbf_surrogate_config;
+void cbf_surrogate_config_init(cbf_surrogate_config* cfg);
+
+typedef struct cbf_surrogate_report {
+    int64_t points;            /* grid points */
+    int64_t labelled;          /* plain training points (kept in the map) */
+    int64_t refined;           /* points recomputed by the plain method */
+    int64_t boundary;          /* ... of which on a predicted boundary */
+    int64_t lowConfidence;     /* ... of which below the confidence threshold */
+    int64_t audit;             /* ... of which in the audit sample */
+    int64_t auditOnly;         /* audit points no other rule selected */
+    int64_t auditOnlyAgree;    /* ... whose predicted class equals the plain class */
+    int64_t refinedChanged;    /* recomputed points whose class the plain method changed */
+    double auditOnlyLleMeanAbsErr, auditOnlyLleMaxAbsErr;  /* predicted vs plain LLE */
+    double lleMean, lleStd;    /* normalisation of the LLE target */
+    float finalLoss;           /* mean training loss over the last 100 steps */
+    double msLabel, msTrain, msPredict, msMask, msRefine, msTotal;  /* stream time */
+    int64_t expanded;          /* recomputed points selected only by the expansion */
+    int32_t waves;             /* recompute rounds run */
+} cbf_surrogate_report;
+
+/* job: a whole-grid 2-D CBF_TASK_LLE_REGIME sweep of the Rossler, Lorenz or
+ * Chen system.  dLle double[nPts^2], dCls int32[nPts^2] (device); dSource
+ * (optional, device uint8[nPts^2]): 0 predicted, 1 training label, 2 recomputed. */
+cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config* cfg, double* dLle,
+                                 int32_t* dCls, uint8_t* dSource, cbf_surrogate_report* report,
+                                 void* stream);
 
 /* ---- host-buffer entry points (drop-in for hostLibrary.cuh) ---------- */
 /* bifurcation1D, hostLibrary.cuh:29-42 / hostLibrary.cu:7-158.

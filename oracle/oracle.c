@@ -548,10 +548,17 @@ double orc_lle_regime_point(const orc_job* job, int64_t g, const double* zIn, in
     }
 
     int c = 0;
-    if (!regimeDiv && recorded > 0) {
+    double lo = INFINITY, hi = -INFINITY;
+    for (int i = 0; i < recorded && !regimeDiv; ++i) {
+        lo = fmin(lo, data[i]);
+        hi = fmax(hi, data[i]);
+    }
+    if (!regimeDiv && recorded > 0 && !(hi - lo < job->regimeMinAmp)) {
         double* times = (double*)malloc(sizeof(double) * (size_t)recorded);
         int n = orc_peak_finder(data, 0, recorded, data, times, 0.01);
-        if (n > job->maxAmountOfPeaks) {
+        if (n > 0 && job->regimeChaosLle > 0 && result / job->tMax > job->regimeChaosLle) {
+            c = 15;
+        } else if (n > job->maxAmountOfPeaks) {
             c = 15;
         } else if (n > 0) {
             double* helpful = (double*)malloc(sizeof(double) * (size_t)(2 * n + 2));

@@ -62,6 +62,8 @@ typedef struct orc_job {
     int32_t maxAmountOfPeaks;
     int32_t kdeSampling;
     double regimeTime;  /* LLE + regime: window after the transient (time units) */
+    double regimeMinAmp; /* LLE + regime: window range below this -> class 0 */
+    double regimeChaosLle; /* LLE + regime: > 0 and LLE above it -> class 15 */
 } orc_job;
 
 /* cudaLibrary.cu:210-216 */
@@ -126,7 +128,9 @@ int orc_map_lle_list(const orc_job* job, const int64_t* idx, int64_t count, doub
 /* LLE plus peak-count regime class (the library's plain labelling method): the
  * LLE of orc_lle_point_seeded; x[writableVar] recorded before every step of the
  * base trajectory for the first (int)(regimeTime/h) steps after the transient;
- * class = 0 if the divergence test fired inside that window or no peak,
+ * class = 0 if the divergence test fired inside that window, no peak, or the
+ * window's samples span less than regimeMinAmp (max - min, fmin/fmax); 15 if
+ * regimeChaosLle > 0 and the LLE exceeds it,
  * 15 if more than maxAmountOfPeaks peaks, else min(dbscan, 15). */
 double orc_lle_regime_point(const orc_job* job, int64_t g, const double* z, int32_t* cls);
 int orc_map_lle_regime_list(const orc_job* job, const int64_t* idx, int64_t count,

@@ -49,13 +49,16 @@ class OrcJob(C.Structure):
         ("maxAmountOfPeaks", C.c_int32),
         ("kdeSampling", C.c_int32),
         ("regimeTime", C.c_double),
+        ("regimeMinAmp", C.c_double),
+        ("regimeChaosLle", C.c_double),
     ]
 
 
 def make_job(*, system, nPts, ranges, idxMut, ic, values, h, tMax=0.0, transientTime=0.0,
              maxValue=0.0, writableVar=0, preScaller=1, sweepIC=False, maxAmountOfPeaks=0,
              kdeSampling=0, kdeI1=0.0, kdeI2=0.0, kdeH=0.0, dbscanEps=0.0, NT=0.0,
-             lleEps=0.0, seedChunk=0, regimeTime=0.0) -> OrcJob:
+             lleEps=0.0, seedChunk=0, regimeTime=0.0, regimeMinAmp=0.0,
+             regimeChaosLle=0.0) -> OrcJob:
     j = OrcJob()
     dims = len(idxMut)
     j.system = SYSTEMS[system] if isinstance(system, str) else int(system)
@@ -79,6 +82,8 @@ def make_job(*, system, nPts, ranges, idxMut, ic, values, h, tMax=0.0, transient
     j.dbscanEps = dbscanEps
     j.NT, j.lleEps, j.seedChunk = NT, lleEps, seedChunk
     j.regimeTime = regimeTime
+    j.regimeMinAmp = regimeMinAmp
+    j.regimeChaosLle = regimeChaosLle
     return j
 
 

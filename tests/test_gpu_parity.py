@@ -264,7 +264,9 @@ REGIME = dict(CHEN_LLE, nPts=10, tMax=40.0, transientTime=20.0, maxAmountOfPeaks
 
 
 @pytest.mark.parametrize("extra", [dict(), dict(maxValue=20.0), dict(maxAmountOfPeaks=20),
-                                   dict(regimeTime=60.0), dict(writableVar=2)])
+                                   dict(regimeTime=60.0), dict(writableVar=2),
+                                   dict(regimeMinAmp=1e-6), dict(regimeMinAmp=15.0),
+                                   dict(regimeMinAmp=1e-6, regimeChaosLle=0.05, dbscanEps=0.02)])
 def test_lle_regime_matches_oracle(cbf, orc, gpu_ok, extra):
     kw = dict(REGIME, **extra)
     j, o = both(cbf, orc, task=cbf.TASK_LLE_REGIME, **kw)
@@ -275,7 +277,8 @@ def test_lle_regime_matches_oracle(cbf, orc, gpu_ok, extra):
     assert_lle_close(lle, want_lle)
     assert 0 <= cls.min() and cls.max() <= 15
     # the LLE of the fused kernel is the LLE kernel's, bit for bit
-    plain = {k: v for k, v in kw.items() if k not in ("maxAmountOfPeaks", "dbscanEps", "regimeTime")}
+    plain = {k: v for k, v in kw.items() if k not in ("maxAmountOfPeaks", "dbscanEps", "regimeTime",
+                                                      "regimeMinAmp", "regimeChaosLle")}
     lle2, _ = cbf.run_host(cbf.make_job(task=cbf.TASK_LLE, **plain))
     assert np.array_equal(lle, lle2, equal_nan=True)
 

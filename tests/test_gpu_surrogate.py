@@ -1,0 +1,167 @@
+"""GPU tests of the surrogate network (csrc/mlp.cu) and the surrogate-refined
+LLE + regime map (csrc/surrogate.cu).
+
+* gradients of the BF16 tensor-core forward/backward kernels against the CPU
+  oracle (oracle/mlp_oracle.py) with the same BF16 rounding points;
+* predictions and training behaviour;
+* the refined map against the plain map on the same grid: every point the plain
+  method computed (labels, recomputed points) is bit-identical to the plain map,
+  the report's counts match the map, and the refined map agrees with the plain
+  one at >= 99.5 % of points while computing only a fraction of them -- the
+  gain over the method without the network.
+"""
+import numpy as np
+import pytest
+
+import mlp_oracle as M
+
+pytestmark = pytest.mark.gpu
+
+CHEN_REGIME = dict(system="chen", ranges=[30.0, 45.0, 20.0, 30.0], idxMut=[1, 3], ic=[0.1, 0.1, 0.1],
+                   values=[0.5, 35.0, 3.0, 28.0], h=0.002, NT=0.5, lleEps=1e-8, maxValue=1e4,
+                   seedChunk=200000, maxAmountOfPeaks=512, dbscanEps=0.02, regimeMinAmp=1e-6,
+                   regimeChaosLle=0.05, flags=1)
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def _batch(rng, n):
+    return (rng.uniform(-1, 1, (n, 4)).astype(np.float32), rng.normal(size=n).astype(np.float32),
+            rng.integers(0, 16, n).astype(np.int32))
+
+
+def test_mlp_init_matches_oracle(cbf, gpu_ok):
+    net = cbf.Mlp(64, seed=11)
+    assert net.num_params() == M.NUM_PARAMS
+    assert np.array_equal(net.get_params().astype(np.float64), M.init_params(11))
+
+
+@pytest.mark.parametrize("n", [37, 1000])
+def test_mlp_gradients_match_oracle(cbf, gpu_ok, n):
+    """n=37: ragged tiles; n=1000: two split-K slices in the weight gradients."""
+    rng = np.random.default_rng(n)
+    net = cbf.Mlp(1024, seed=5)
+    p = M.init_params(5)
+    off = M.offsets()
+    for b in ("b1", "b2", "b3", "b4"):
+        o, shape = off[b]
+        p[o:o + shape[0]] = rng.normal(scale=0.2, size=shape[0])
+    p = p.astype(np.float32)
+    net.set_params(p)
+    x, yl, yc = _batch(rng, n)
+    loss, g, out = net.forward_backward(x, yl, yc, 0.5)
+    wl, wg, wout = M.forward_backward(p.astype(np.float64), x, yl, yc, 0.5, bf16_round=True)
+    assert abs(loss - wl) <= 1e-4 * abs(wl)
+    assert _rel(out, wout) < 1e-3
+    for name, (o, shape) in off.items():
+        k = int(np.prod(shape))
+        err = _rel(g[o:o + k], wg[o:o + k])
+        assert err < 1e-2, (name, err)
+    # and the BF16 gradients stay near the exact float64 ones
+    _, eg, _ = M.forward_backward(p.astype(np.float64), x, yl, yc, 0.5, bf16_round=False)
+    assert _rel(g, eg) < 0.05
+
+
+def test_mlp_predict_matches_forward(cbf, gpu_ok):
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(9)
+    net = cbf.Mlp(512, seed=2)
+    x, yl, yc = _batch(rng, 300)
+    _, _, out = net.forward_backward(x, yl, yc, 1.0)
+    dx = torch.from_numpy(x).cuda()
+    lle = torch.empty(300, dtype=torch.float32, device="cuda")
+    cls = torch.empty(300, dtype=torch.int32, device="cuda")
+    conf = torch.empty(300, dtype=torch.float32, device="cuda")
+    net.predict(dx.data_ptr(), 300, 0.25, 2.0, lle.data_ptr(), cls.data_ptr(), conf.data_ptr())
+    torch.cuda.synchronize()
+    logits = out[:, 1:].astype(np.float64)
+    assert np.array_equal(cls.cpu().numpy(), logits.argmax(axis=1))
+    assert np.allclose(lle.cpu().numpy(), out[:, 0] * 2.0 + 0.25, rtol=1e-6, atol=1e-6)
+    pm = np.exp(logits - logits.max(axis=1, keepdims=True))
+    assert np.allclose(conf.cpu().numpy(), 1.0 / pm.sum(axis=1), rtol=1e-5)
+
+
+def test_mlp_training_reduces_loss(cbf, gpu_ok):
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(4)
+    n = 20000
+    x = rng.uniform(-1, 1, (n, 4)).astype(np.float32)
+    yl = np.sin(3 * x[:, 1]) * np.cos(2 * x[:, 2])
+    yc = ((x[:, 1] > 0).astype(np.int32) * 2 + (x[:, 2] > 0.3)).astype(np.int32)
+    d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (x, yl.astype(np.float32), yc)]
+    s = torch.cuda.Stream()
+    net = cbf.Mlp(1024, seed=1)
+    losses = net.train(d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), n, 600, 2e-3, horizon=600,
+                       stream=s.cuda_stream, losses=True)
+    assert np.all(np.isfinite(losses))
+    assert losses[-50:].mean() < 0.1 * losses[:5].mean(), (losses[:5], losses[-50:].mean())
+    # replaying the captured step continues from the same optimiser state
+    more = net.train(d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), n, 20, 2e-3, horizon=600,
+                     stream=s.cuda_stream, losses=True)
+    assert more.mean() < 2 * losses[-50:].mean()
+
+
+def _plain_and_surrogate(cbf, torch, side, cfg_kw, **job_kw):
+    kw = dict(CHEN_REGIME, nPts=side, **job_kw)
+    job = cbf.make_job(task=cbf.TASK_LLE_REGIME, **kw)
+    plain_lle, plain_cls = cbf.run_host(job)
+    n = side * side
+    d_lle = torch.empty(n, dtype=torch.float64, device="cuda")
+    d_cls = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_src = torch.empty(n, dtype=torch.uint8, device="cuda")
+    cfg = cbf.surrogate_config(**cfg_kw)
+    rep = cbf.lle_map_surrogate(job, cfg, d_lle.data_ptr(), d_cls.data_ptr(), d_src.data_ptr())
+    torch.cuda.synchronize()
+    return (plain_lle, plain_cls, d_lle.cpu().numpy(), d_cls.cpu().numpy(), d_src.cpu().numpy(), rep)
+
+
+SMALL = dict(tMax=60.0, transientTime=30.0, regimeTime=30.0)
+SMALL_CFG = dict(coarseSide=64, randomPoints=4096, batch=2048, trainSteps=1500, seed=7)
+
+
+def test_surrogate_map_refines_to_plain(cbf, gpu_ok):
+    torch = pytest.importorskip("torch")
+    pl, pc, sl, sc, src, rep = _plain_and_surrogate(cbf, torch, 384, SMALL_CFG, **SMALL)
+    n = 384 * 384
+    assert rep.points == n and rep.labelled == 64 * 64 + 4096
+    assert set(np.unique(src)) <= {0, 1, 2}
+    computed = src > 0
+    # every point the plain method computed is the plain map's value, bit for bit
+    assert np.array_equal(sl[computed], pl[computed], equal_nan=True)
+    assert np.array_equal(sc[computed], pc[computed])
+    assert int((src == 2).sum()) == rep.refined
+    assert rep.boundary + rep.lowConfidence + rep.audit + rep.expanded >= rep.refined
+    assert rep.waves >= 1
+    assert 0 < rep.auditOnly <= rep.audit
+    assert 0 <= sc.min() and sc.max() <= 15
+    agree = float(np.mean(sc == pc))
+    frac = float(np.mean(computed))
+    print(f"agreement {agree:.5f} computed {frac:.4f} report {rep.as_dict()}")
+    assert agree >= 0.995
+    assert frac < 0.7  # the network spared the plain method at least 30 % of the map
+
+
+def test_surrogate_is_deterministic_and_ablation_is_worse(cbf, gpu_ok):
+    torch = pytest.importorskip("torch")
+    side = 256
+    a = _plain_and_surrogate(cbf, torch, side, SMALL_CFG, **SMALL)
+    b = _plain_and_surrogate(cbf, torch, side, SMALL_CFG, **SMALL)
+    assert np.array_equal(a[2], b[2], equal_nan=True) and np.array_equal(a[3], b[3])
+    assert np.array_equal(a[4], b[4])
+    # network alone (no recompute): only labels are plain, agreement drops
+    pl, pc, sl, sc, src, rep = _plain_and_surrogate(cbf, torch, side, dict(SMALL_CFG, refine=0), **SMALL)
+    assert rep.refined == 0 and rep.waves == 0 and set(np.unique(src)) <= {0, 1}
+    assert np.mean(sc == pc) <= np.mean(a[3] == a[1])
+
+
+def test_surrogate_rejects_bad_jobs(cbf, gpu_ok):
+    job = cbf.make_job(task=cbf.TASK_LLE, nPts=16, tMax=1.0, transientTime=1.0, **CHEN_REGIME)
+    cfg = cbf.surrogate_config()
+    with pytest.raises(cbf.CbfError):
+        cbf.lle_map_surrogate(job, cfg, 1, 1)
+    job = cbf.make_job(task=cbf.TASK_LLE_REGIME, nPts=16, tMax=1.0, transientTime=1.0,
+                       regimeTime=1.0, **dict(CHEN_REGIME, system="memristive5"))
+    with pytest.raises(cbf.CbfError):
+        cbf.lle_map_surrogate(job, cfg, 1, 1)

@@ -130,3 +130,35 @@ def test_live_random_against_reference(orc):
             L.orc_dbscan(p.copy(), t.copy(), hb, 0, n, len(hb), 60, 0.05)
         assert R.ref_kde(p.copy(), 0, n, 60, 4, -3.0, 3.0, 0.1) == \
             L.orc_kde(p.copy(), 0, n, 60, 4, -3.0, 3.0, 0.1)
+
+
+def test_regime_amplitude_rule_on_oracle(orc):
+    """The regime class of the plain labelling method: equilibria (negative LLE,
+    no oscillation left after the transient) are class 0 once the window range
+    rule is on, whatever ulp-level wobble the FP64 state shows; limit cycles keep
+    their cluster count."""
+    side = 2048
+    kw = dict(system="chen", nPts=side, ranges=[30.0, 45.0, 20.0, 30.0], idxMut=[1, 3],
+              ic=[0.1, 0.1, 0.1], values=[0.5, 35.0, 3.0, 28.0], h=0.002, NT=0.5, tMax=100.0,
+              transientTime=500.0, lleEps=1e-8, maxValue=1e4, seedChunk=200000,
+              maxAmountOfPeaks=512, dbscanEps=0.05, regimeTime=50.0)
+
+    def idx(a, c):  # exact-grid index of the point nearest (a, c)
+        i0 = int(round((a - 30.0) / 15.0 * (side - 1)))
+        i1 = int(round((c - 20.0) / 10.0 * (side - 1)))
+        return i1 * side + i0
+
+    stable = [idx(a, c) for a in (38.5, 39.0, 39.7, 40.3) for c in (20.2, 20.5)]
+    cycle = [idx(a, c) for a in (30.6, 31.2) for c in (27.2, 27.8)]
+    on = orc.make_job(regimeMinAmp=1e-6, **kw)
+    lle, cls = orc.map_lle_regime(on, stable)
+    assert np.all(lle < -0.05), lle
+    assert np.all(cls == 0), cls
+    lle, cls = orc.map_lle_regime(on, cycle)
+    assert np.all(np.abs(lle) < 0.05), lle
+    assert np.all(cls >= 1), cls
+    # the rule only ever lowers a class to 0
+    off = orc.make_job(**kw)
+    _, raw = orc.map_lle_regime(off, stable + cycle)
+    _, ruled = orc.map_lle_regime(on, stable + cycle)
+    assert np.all((ruled == raw) | (ruled == 0))
