@@ -1,14 +1,24 @@
-"""Benchmark: 2-D largest-Lyapunov-exponent map, grid points per second.
+"""Benchmark: 2-D largest-Lyapunov-exponent maps, grid points per second.
 
-Workload (one step = one full map): Chen system x'=a(y-x), y'=(c-a)x-xz+cy,
-z'=xy-bz on a 2048x2048 (a, c) grid over a in [30,45], c in [20,30], b=3,
-h=0.002, Benettin two-trajectory LLE with initial offset 1e-8 renormalised every
-NT=0.5 over tMax=1000 after a 500-unit transient (LLE2D semantics of the
-reference, seed chunk 200000).  FP64 throughout.  Inputs are synthetic by
-nature: the grid itself.
+Default workload (chen-surrogate-8192; one step = one full map): the LLE and
+peak-count regime class of the Chen system x'=a(y-x), y'=(c-a)x-xz+cy, z'=xy-bz
+on an 8192x8192 (a, c) grid over a in [30,45], c in [20,30], b=3, h=0.002,
+Benettin two-trajectory LLE (offset 1e-8, renormalised every NT=0.5 over
+tMax=1000 after a 500-unit transient; seed chunk 200000), regime class from the
+first 50 time units after the transient (DBSCAN eps 0.02 on (peak, interval),
+range below 1e-6 -> 0, LLE above 0.05 -> 15), produced surrogate-refined
+(cbf_lle_map_surrogate: plain labels on a 512x512 sub-grid + 65536 random
+points, BF16 tensor-core MLP trained on the GPU, plain FP64 recompute of
+boundary, low-confidence, 1 % audit and expansion points).  The plain FP64 map
+of the same grid is computed once per run: its throughput is reported beside the
+surrogate's, and the regime agreement and LLE error of the refined map are
+measured against it point by point.
+
+chen-lle2d-2048: the plain LLE map alone on 2048x2048 (the FP64 roofline case).
+Inputs are synthetic by nature: the grid itself.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-    python bench.py --workload lorenz-dbscan-1024|lorenz-kde256-1024|lorenz-kde-1024|rossler-bif1d-1000|batch64
+    python bench.py --workload chen-lle2d-2048|lorenz-dbscan-1024|lorenz-kde256-1024|lorenz-kde-1024|rossler-bif1d-1000|batch64
 
 Multi-GPU (torchrun, one rank per GPU): every rank computes its own 2048x2048 map
 of one c-stripe (weak scaling, no data-path collective); time = max over ranks.
@@ -46,6 +56,9 @@ WORKLOAD = dict(system="chen", nPts=2048, ranges=[30.0, 45.0, 20.0, 30.0], idxMu
                 ic=[0.1, 0.1, 0.1], values=[0.5, 35.0, 3.0, 28.0], h=0.002, NT=0.5, tMax=1000.0,
                 transientTime=500.0, lleEps=1e-8, maxValue=1e4, seedChunk=200000)
 METRIC = "grid points/s, 2D LLE map (plain FP64)"
+SUR_METRIC = "grid points/s, 2D LLE map: plain FP64 vs surrogate-refined at \u226599.5% agreement"
+SUR_WORKLOAD = dict(WORKLOAD, nPts=8192, seedChunk=200000, maxAmountOfPeaks=512, dbscanEps=0.02,
+                    regimeTime=50.0, regimeMinAmp=1e-6, regimeChaosLle=0.05, flags=1)
 # FP64 work of one CD step of each system (csrc/systems.cuh; FMA = 2 flops)
 FLOPS_PER_STEP = {"chen": 19, "lorenz": 19, "rossler": 17, "memristive5": 66}
 FP64_INSTR_PER_STEP = {"chen": 14, "lorenz": 14, "rossler": 10, "memristive5": 52}
@@ -319,24 +332,36 @@ def traffic_from_profiles():
         return None
 
 
+def _orc_kw(w):
+    return {k: v for k, v in w.items() if k not in ("flags",)}
+
+
 def run_reference(args) -> int:
-    """The reference's per-point code (oracle port) on the host cores."""
+    """The reference's per-point code (oracle port) on the host cores: the plain
+    LLE (+ regime class for the default workload) of strided grid points."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    w = WORKLOAD
+    sur = args.workload == "chen-surrogate-8192"
+    w = SUR_WORKLOAD if sur else WORKLOAD
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
     if not O.LIB_PATH.exists():
         O.build(with_ref=False)
     threads = O.host_threads()
-    job = O.make_job(**w)
+    job = O.make_job(**_orc_kw(w))
     n_total = w["nPts"] ** 2
+    if sur:
+        def compute(idx):
+            O.map_lle_regime(job, idx, threads=threads)
+    else:
+        def compute(idx):
+            O.map_lle_list(job, idx, threads)
     # Calibrate on one point per thread, then size every step to ~target seconds.
     target = float(os.environ.get("CBF_REF_STEP_SECONDS", "5"))
     cal = (np.arange(threads, dtype=np.int64) * 7919) % n_total
     t0 = time.perf_counter()
-    O.map_lle_list(job, cal, threads)
+    compute(cal)
     t_cal = max(time.perf_counter() - t0, 1e-3)
     per_step = threads * max(1, int(target / t_cal))
     stride = max(1, n_total // (per_step * (args.steps + args.warmup)))
@@ -344,19 +369,21 @@ def run_reference(args) -> int:
     for s in range(args.warmup + args.steps):
         idx = ((np.arange(per_step, dtype=np.int64) + s * per_step) * stride) % n_total
         t0 = time.perf_counter()
-        O.map_lle_list(job, idx, threads)
+        compute(idx)
         dt = time.perf_counter() - t0
         if s >= args.warmup:
             times.append(dt)
     tot = sum(times)
     value = per_step * args.steps / tot
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "points/s",
+        "impl": "reference", "metric": SUR_METRIC if sur else METRIC, "value": value, "unit": "points/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "chen-lle2d-2048", "grid": "2048x2048", "tMax": 1000, "NT": 0.5,
-                   "h": 0.002, "transient": 500, "steps_per_point": steps_per_point(w),
+        "config": {"workload": args.workload, "grid": f"{w['nPts']}x{w['nPts']}", "tMax": 1000,
+                   "NT": 0.5, "h": 0.002, "transient": 500, "steps_per_point": steps_per_point(w),
+                   "method": "plain LLE + regime class per point (the reference has no surrogate)"
+                   if sur else "plain LLE per point",
                    "cache": "inputs are scalars; CPU arm"},
         "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads, "kind": "port",
                          "sample": f"{per_step} strided points per step of {n_total}"},
@@ -446,6 +473,215 @@ def run_secondary(args, name: str) -> int:
     return 0
 
 
+def cpu_baseline_regime(w: dict, target_s: float = 15.0) -> dict:
+    """Oracle port of the plain LLE + regime per-point code on a strided sample."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    threads = O.host_threads()
+    job = O.make_job(**_orc_kw(w))
+    n_total = w["nPts"] ** 2
+    probe = np.arange(threads, dtype=np.int64) * (n_total // max(threads, 1))
+    t0 = time.perf_counter()
+    O.map_lle_regime(job, probe, threads=threads)
+    per_round = max(time.perf_counter() - t0, 1e-3)
+    count = max(1, int(target_s / per_round)) * threads
+    stride = max(1, n_total // count)
+    idx = (np.arange(count, dtype=np.int64) * stride) % n_total
+    t0 = time.perf_counter()
+    O.map_lle_regime(job, idx, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": count / dt, "unit": "points/s", "cores": threads, "kind": "port",
+            "sample": f"{count} of {n_total} points (every {stride}th), plain LLE + regime, "
+                      f"{steps_per_point(w)} steps each"}
+
+
+def run_surrogate(args) -> int:
+    """Surrogate-refined 8192^2 LLE + regime map against the plain map."""
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900),
+                                device_id=torch.device("cuda", local))
+    cbf = load_cbf()
+    cbf.check(cbf.lib().cbf_set_device(local))
+    w = dict(SUR_WORKLOAD)
+    if world > 1:  # weak scaling: each rank maps its own c-stripe at full resolution
+        lo, hi = w["ranges"][2], w["ranges"][3]
+        step = (hi - lo) / world
+        w["ranges"] = [w["ranges"][0], w["ranges"][1], lo + rank * step, lo + (rank + 1) * step]
+    if args.nPts:
+        w["nPts"] = args.nPts
+    n = w["nPts"] ** 2
+    job = cbf.make_job(task=cbf.TASK_LLE_REGIME, **w)
+    spp = steps_per_point(w)
+    cfg = cbf.surrogate_config()
+    probe = cbf.probe_fp64_peak(300.0)
+    stream = torch.cuda.Stream()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    # plain FP64 map of the same grid, once: throughput and the agreement reference
+    p_lle = torch.empty(n, dtype=torch.float64, device="cuda")
+    p_cls = torch.empty(n, dtype=torch.int32, device="cuda")
+    with torch.cuda.stream(stream):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+    cbf.run_device(job, p_lle.data_ptr(), p_cls.data_ptr(), stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        e1.record(stream)
+    stream.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+
+    s_lle = torch.empty(n, dtype=torch.float64, device="cuda")
+    s_cls = torch.empty(n, dtype=torch.int32, device="cuda")
+    s_src = torch.empty(n, dtype=torch.uint8, device="cuda")
+
+    def one_map():
+        with torch.cuda.stream(stream):
+            return cbf.lle_map_surrogate(job, cfg, s_lle.data_ptr(), s_cls.data_ptr(), s_src.data_ptr(),
+                                         stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        one_map()
+    stream.synchronize()
+
+    sampler = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    launches0 = cbf.kernel_launches()
+    evs, reps = [], []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        reps.append(one_map())
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = cbf.kernel_launches() - launches0
+    clocks = sampler.stop()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    t = torch.tensor([sum(step_ms), plain_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms, plain_max = float(t[0].item()), float(t[1].item())
+    value = world * n * args.steps / (total_ms / 1e3)
+    plain_value = world * n / (plain_max / 1e3)
+
+    # agreement and LLE error against the plain map, point by point
+    same_cls = (s_cls == p_cls)
+    agree = float(same_cls.double().mean().item())
+    kept = s_src == 0
+    err = (s_lle - p_lle).abs()
+    fin = torch.isfinite(err) & kept
+    kept_err = err[fin]
+    computed = s_src > 0
+    exact = bool(torch.equal(s_cls[computed], p_cls[computed]) and
+                 torch.equal(torch.nan_to_num(s_lle[computed], nan=7.0, posinf=8.0, neginf=9.0),
+                             torch.nan_to_num(p_lle[computed], nan=7.0, posinf=8.0, neginf=9.0)))
+    stats = torch.tensor([agree], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(stats, op=dist.ReduceOp.MIN)
+    agree_min = float(stats.item())
+
+    # end to end through the public API: the map into pinned host buffers
+    h_lle = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    h_cls = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    e2e_times = []
+    for _ in range(max(1, args.e2e_steps)):
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        one_map()
+        with torch.cuda.stream(stream):
+            h_lle.copy_(s_lle, non_blocking=True)
+            h_cls.copy_(s_cls, non_blocking=True)
+        stream.synchronize()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_total = torch.tensor([sum(e2e_times)], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(e2e_total, op=dist.ReduceOp.MAX)
+    e2e_value = world * n * len(e2e_times) / float(e2e_total.item())
+
+    r = reps[-1].as_dict()
+    plain_points = r["labelled"] + r["refined"]
+    plain_phase_ms = r["msLabel"] + r["msRefine"]
+    props = torch.cuda.get_device_properties(local)
+    max_mhz = clocks.get("sm_max_mhz") or 1965.0
+    nominal = props.multi_processor_count * FP64_LANES_PER_SM * 2 * max_mhz * 1e6 / 1e12
+    peak = max(nominal, probe)
+    flops = float(plain_points) * spp * FLOPS_PER_STEP["chen"]
+    achieved = flops / (plain_phase_ms / 1e3) / 1e12
+    plain_achieved = float(n) * spp * FLOPS_PER_STEP["chen"] / (plain_ms / 1e3) / 1e12
+    roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak,
+            "kernel": "lle_regime_kernel (plain FP64 labels + recompute rounds of the refined map)",
+            "peak_source": "max(nominal SMs x 64 FP64 lanes x 2 flops x max SM clock, FP64 FMA "
+                           "probe measured in this run); MEASURED_PEAKS.json has no FP64 figure",
+            "peak_nominal": nominal, "peak_probe": probe,
+            "flops_per_step": FLOPS_PER_STEP["chen"], "steps_per_point": spp,
+            "plain_points_in_step": plain_points, "plain_phase_ms": plain_phase_ms,
+            "plain_map_achieved": plain_achieved, "plain_map_frac": plain_achieved / peak,
+            "traffic": None}
+
+    ok = agree_min >= 0.995 and exact
+    if rank == 0:
+        base = None
+        if world == 1 and not args.no_cpu_baseline:
+            base = cpu_baseline_regime(w)
+        line = {
+            "metric": SUR_METRIC, "value": value, "unit": "points/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (the parameter grid is the input)",
+            "config": {"workload": "chen-surrogate-8192", "grid": f"{w['nPts']}x{w['nPts']}",
+                       "system": "chen", "tMax": w["tMax"], "NT": w["NT"], "h": w["h"],
+                       "transient": w["transientTime"], "eps": w["lleEps"], "regimeTime": 50.0,
+                       "steps_per_point": spp, "points_per_rank": n,
+                       "surrogate": {k: getattr(cfg, k) for k, _ in cfg._fields_},
+                       "cache": "L2 flushed (256 MB write) before every timed map; the outputs "
+                                "(805 MB) exceed L2",
+                       "parallelism": f"{world} independent c-stripes, one per GPU"},
+            "plain": {"value": plain_value, "unit": "points/s", "ms": plain_max,
+                      "note": "plain FP64 LLE + regime map of the same grid, CUDA events, once"},
+            "speedup_vs_plain": plain_max / (total_ms / args.steps),
+            "agreement": {"regime_agreement": agree, "min_over_ranks": agree_min,
+                          "computed_fraction": float(computed.double().mean().item()),
+                          "plain_points_bit_exact": exact,
+                          "kept_lle_mean_abs_err": float(kept_err.mean().item()) if kept_err.numel() else None,
+                          "kept_lle_p99_abs_err": float(torch.quantile(kept_err[:1 << 24].float(), 0.99).item())
+                          if kept_err.numel() else None},
+            "report": r,
+            "e2e": {"value": e2e_value, "unit": "points/s", "h2d_bytes_per_step": C.sizeof(cbf.Job),
+                    "d2h_bytes_per_step": n * 12},
+            "roofline": roof,
+            "cpu_baseline": base,
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "step_ms": step_ms,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0 if ok else 1
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__,
                                  formatter_class=argparse.RawDescriptionHelpFormatter)
@@ -456,14 +692,16 @@ def main(argv=None) -> int:
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--nPts", type=int, default=None, help="override the grid side (testing)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="chen-lle2d-2048",
-                    choices=["chen-lle2d-2048", "batch64", *SECONDARY])
+    ap.add_argument("--workload", default="chen-surrogate-8192",
+                    choices=["chen-surrogate-8192", "chen-lle2d-2048", "batch64", *SECONDARY])
     args = ap.parse_args(argv)
 
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch64":
         return run_batch(args)
+    if args.workload == "chen-surrogate-8192":
+        return run_surrogate(args)
     if args.workload != "chen-lle2d-2048":
         return run_secondary(args, args.workload)
 

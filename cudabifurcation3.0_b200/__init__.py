@@ -261,8 +261,8 @@ def lib():
         L.cbf_surrogate_config_init.argtypes = [C.POINTER(SurrogateConfig)]
         L.cbf_surrogate_config_init.restype = None
         L.cbf_lle_map_surrogate.argtypes = [C.POINTER(Job), C.POINTER(SurrogateConfig), C.c_void_p,
-                                            C.c_void_p, C.c_void_p, C.POINTER(SurrogateReport),
-                                            C.c_void_p]
+                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                            C.POINTER(SurrogateReport), C.c_void_p]
         L.cbf_lle_map_surrogate.restype = C.c_int32
         L.cbf_facade_set_system.argtypes = [C.c_int32]
         L.cbf_facade_set_output_path.argtypes = [C.c_char_p]
@@ -506,11 +506,12 @@ def surrogate_config(**kw) -> SurrogateConfig:
 
 
 def lle_map_surrogate(job: Job, cfg: SurrogateConfig, d_lle: int, d_cls: int, d_src: int = 0,
-                      stream: int = 0) -> SurrogateReport:
+                      stream: int = 0, d_conf: int = 0, d_pred: int = 0) -> SurrogateReport:
     """Surrogate-refined LLE + regime map into device buffers; returns the report."""
     rep = SurrogateReport()
     check(lib().cbf_lle_map_surrogate(C.byref(job), C.byref(cfg), C.c_void_p(d_lle), C.c_void_p(d_cls),
-                                      C.c_void_p(d_src or None), C.byref(rep),
+                                      C.c_void_p(d_src or None), C.c_void_p(d_conf or None),
+                                      C.c_void_p(d_pred or None), C.byref(rep),
                                       C.c_void_p(stream or None)))
     return rep
 

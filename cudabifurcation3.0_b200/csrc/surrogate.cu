@@ -304,20 +304,21 @@ void cbf_surrogate_config_init(cbf_surrogate_config* c)
     c->coarseSide = 512;
     c->randomPoints = 65536;
     c->batch = 4096;
-    c->trainSteps = 4000;
+    c->trainSteps = 2500;
     c->lr = 2e-3f;
     c->wLle = 1.0f;
-    c->confThreshold = 0.95f;
+    c->confThreshold = 0.7f;
     c->auditFraction = 0.01f;
     c->boundaryRadius = 1;
     c->refine = 1;
     c->seed = 20240101ull;
     c->expandRadius = -1;
-    c->maxWaves = 256;
+    c->maxWaves = 30;
 }
 
 cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config* cfg, double* dLle,
-                                 int32_t* dCls, uint8_t* dSource, cbf_surrogate_report* rep, void* stream)
+                                 int32_t* dCls, uint8_t* dSource, float* dConf, int32_t* dPred,
+                                 cbf_surrogate_report* rep, void* stream)
 {
     if (!job || !cfg || !dLle || !dCls) return report_error(CBF_ERR_INVALID_ARG, "null argument");
     if (job->task != CBF_TASK_LLE_REGIME || job->dims != 2 || job->sweepIC)
@@ -372,7 +373,7 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
     long long* dIdx = nullptr;
     double* labLle = nullptr;
     int* labCls = nullptr;
-    float *X = nullptr, *yl = nullptr, *conf = nullptr;
+    float *X = nullptr, *yl = nullptr, *conf = dConf;
     unsigned char *flag = nullptr, *src = dSource;
     int* blockCount = nullptr;
     long long* offsets = nullptr;
@@ -383,7 +384,7 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
     if (e == cudaSuccess) e = buf.get(&labCls, nLab);
     if (e == cudaSuccess) e = buf.get(&X, nLab * 4);
     if (e == cudaSuccess) e = buf.get(&yl, nLab);
-    if (e == cudaSuccess) e = buf.get(&conf, n);
+    if (e == cudaSuccess && !conf) e = buf.get(&conf, n);
     if (e == cudaSuccess) e = buf.get(&flag, n);
     if (e == cudaSuccess && !src) e = buf.get(&src, n);
     if (e == cudaSuccess) e = buf.get(&blockCount, nb);
@@ -449,6 +450,7 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
 
     // 3. prediction on every grid point
     e = mlp_predict_grid(net, fs, n, (float)mean, (float)sd, dLle, dCls, conf, s);
+    if (e == cudaSuccess && dPred) e = cudaMemcpyAsync(dPred, dCls, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
     if (e != cudaSuccess) return report_cuda_error(e, "prediction");
     cudaEventRecord(ev[3], s);
 
@@ -458,9 +460,9 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
         frac >= 1.0 ? ~0ull : (unsigned long long)(frac * 18446744073709551616.0);
     const float thr = cfg->refine ? cfg->confThreshold : -1.0f;
     const int radius = cfg->refine ? cfg->boundaryRadius : 0;  // radius 0 marks no boundary
-    // expansion radius: automatic = one grid step per 2048 points of side, so
-    // the number of waves needed to trace a structure does not grow with nPts
-    const int autoR = (nPts + 2047) / 2048;
+    // expansion radius: automatic = one grid step per 4096 points of side, so
+    // that the rounds needed to trace a structure grow slower than nPts
+    const int autoR = (nPts + 4095) / 4096;
     const int er = cfg->refine ? (cfg->expandRadius < 0 ? autoR : cfg->expandRadius) : 0;
     unsigned char* lsur = nullptr;
     if ((e = buf.get(&lsur, nLab)) != cudaSuccess) return report_cuda_error(e, "label buffers");

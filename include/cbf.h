@@ -221,10 +221,10 @@ typedef struct cbf_surrogate_config {
     int32_t coarseSide;      /* training sub-grid side (512) */
     int32_t randomPoints;    /* extra random training points (65536) */
     int32_t batch;           /* training minibatch rows (4096) */
-    int32_t trainSteps;      /* Adam steps, cosine learning-rate decay over them (4000) */
+    int32_t trainSteps;      /* Adam steps, cosine learning-rate decay over them (2500) */
     float lr;                /* peak learning rate (2e-3) */
     float wLle;              /* weight of the LLE squared error in the loss (1) */
-    float confThreshold;     /* recompute points whose softmax maximum is below it (0.95) */
+    float confThreshold;     /* recompute points whose softmax maximum is below it (0.7) */
     float auditFraction;     /* random audit sample of the grid, recomputed (0.01) */
     int32_t boundaryRadius;  /* a neighbour within this Chebyshev radius with another
                                 predicted class marks a boundary point (1) */
@@ -232,8 +232,8 @@ typedef struct cbf_surrogate_config {
     uint64_t seed;           /* training points, minibatches, weights and audit sample */
     int32_t expandRadius;    /* neighbours within this radius of a point whose plain class
                                 differs from the prediction are recomputed next; -1 (default):
-                                ceil(nPts / 2048); 0: no expansion */
-    int32_t maxWaves;        /* recompute rounds that may mark expansions (256) */
+                                ceil(nPts / 4096); 0: no expansion */
+    int32_t maxWaves;        /* recompute rounds that may mark expansions (30) */
 } cbf_surrogate_config;
 void cbf_surrogate_config_init(cbf_surrogate_config* cfg);
 
@@ -256,11 +256,13 @@ typedef struct cbf_surrogate_report {
 } cbf_surrogate_report;
 
 /* job: a whole-grid 2-D CBF_TASK_LLE_REGIME sweep of the Rossler, Lorenz or
- * Chen system.  dLle double[nPts^2], dCls int32[nPts^2] (device); dSource
- * (optional, device uint8[nPts^2]): 0 predicted, 1 training label, 2 recomputed. */
+ * Chen system.  dLle double[nPts^2], dCls int32[nPts^2] (device).  Optional
+ * device outputs: dSource uint8[nPts^2] (0 predicted, 1 training label, 2
+ * recomputed), dConf float[nPts^2] (the network's softmax confidence), dPred
+ * int32[nPts^2] (the network's class before any plain value replaced it). */
 cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config* cfg, double* dLle,
-                                 int32_t* dCls, uint8_t* dSource, cbf_surrogate_report* report,
-                                 void* stream);
+                                 int32_t* dCls, uint8_t* dSource, float* dConf, int32_t* dPred,
+                                 cbf_surrogate_report* report, void* stream);
 
 /* ---- host-buffer entry points (drop-in for hostLibrary.cuh) ---------- */
 /* bifurcation1D, hostLibrary.cuh:29-42 / hostLibrary.cu:7-158.

@@ -118,7 +118,8 @@ def _plain_and_surrogate(cbf, torch, side, cfg_kw, **job_kw):
 
 
 SMALL = dict(tMax=60.0, transientTime=30.0, regimeTime=30.0)
-SMALL_CFG = dict(coarseSide=64, randomPoints=4096, batch=2048, trainSteps=1500, seed=7)
+SMALL_CFG = dict(coarseSide=64, randomPoints=4096, batch=2048, trainSteps=1500, seed=7, confThreshold=0.95,
+                 expandRadius=2, maxWaves=256)
 
 
 def test_surrogate_map_refines_to_plain(cbf, gpu_ok):
