@@ -336,6 +336,16 @@ def _orc_kw(w):
     return {k: v for k, v in w.items() if k not in ("flags",)}
 
 
+def regime_traffic(points):
+    """DRAM bytes of the plain regime kernel for `points` points, scaled from the
+    committed ncu capture (traffic grows with the points computed)."""
+    p = ROOT / "profiles" / "lle_regime_chen_512_traffic.json"
+    try:
+        return float(json.loads(p.read_text())["dram_bytes_per_point"]) * points
+    except (OSError, ValueError, KeyError):
+        return None
+
+
 def run_reference(args) -> int:
     """The reference's per-point code (oracle port) on the host cores: the plain
     LLE (+ regime class for the default workload) of strided grid points."""
@@ -538,6 +548,15 @@ def run_surrogate(args) -> int:
         e1.record(stream)
     stream.synchronize()
     plain_ms = e0.elapsed_time(e1)
+    if args.plain_only:
+        if rank == 0:
+            print(json.dumps({"workload": "chen-surrogate-8192 (plain map only)",
+                              "grid": f"{w['nPts']}x{w['nPts']}", "plain_ms": plain_ms,
+                              "plain_points_per_s": n / (plain_ms / 1e3)}), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
 
     s_lle = torch.empty(n, dtype=torch.float64, device="cuda")
     s_cls = torch.empty(n, dtype=torch.int32, device="cuda")
@@ -637,7 +656,7 @@ def run_surrogate(args) -> int:
             "flops_per_step": FLOPS_PER_STEP["chen"], "steps_per_point": spp,
             "plain_points_in_step": plain_points, "plain_phase_ms": plain_phase_ms,
             "plain_map_achieved": plain_achieved, "plain_map_frac": plain_achieved / peak,
-            "traffic": None}
+            "traffic": regime_traffic(plain_points)}
 
     ok = agree_min >= 0.995 and exact
     if rank == 0:
@@ -692,6 +711,8 @@ def main(argv=None) -> int:
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--nPts", type=int, default=None, help="override the grid side (testing)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-only", action="store_true",
+                    help="chen-surrogate-8192: compute and time only the plain map (profiling)")
     ap.add_argument("--workload", default="chen-surrogate-8192",
                     choices=["chen-surrogate-8192", "chen-lle2d-2048", "batch64", *SECONDARY])
     args = ap.parse_args(argv)
