@@ -25,7 +25,7 @@ LIB_PATH = PKG_DIR / "libcbf.so"
 
 SYS_MEMRISTIVE5, SYS_ROSSLER, SYS_LORENZ, SYS_CHEN = 0, 1, 2, 3
 SYSTEMS = {"memristive5": 0, "rossler": 1, "lorenz": 2, "chen": 3}
-TASK_PEAKS, TASK_KDE, TASK_DBSCAN, TASK_LLE, TASK_TRAJECTORY, TASK_LLE_REGIME = 0, 1, 2, 3, 4, 5
+TASK_PEAKS, TASK_KDE, TASK_DBSCAN, TASK_LLE, TASK_TRAJECTORY, TASK_LLE_REGIME, TASK_LS = 0, 1, 2, 3, 4, 5, 6
 FLAG_EXACT_GRID, FLAG_KDE_FIXED = 1, 2
 STATUS = {0: "ok", 1: "invalid argument", 2: "unknown system", 3: "CUDA error",
           4: "out of device memory", 5: "no CUDA device", 6: "I/O error",
@@ -47,7 +47,8 @@ EXPORTS = [
     "cbf_csv_write_map", "cbf_csv_write_peaks", "cbf_csv_write_pairs",
     "cbf_mlp_num_params", "cbf_mlp_create", "cbf_mlp_destroy", "cbf_mlp_get_params",
     "cbf_mlp_set_params", "cbf_mlp_forward_backward", "cbf_mlp_train", "cbf_mlp_predict",
-    "cbf_surrogate_config_init", "cbf_lle_map_surrogate",
+    "cbf_surrogate_config_init", "cbf_lle_map_surrogate", "cbf_ls1d", "cbf_ls2d",
+    "cbf_csv_write_rows",
 ]
 
 
@@ -222,14 +223,14 @@ def lib():
         L.cbf_bifurcation2d_dbscan_noalloc.restype = C.c_int32
         lle = [C.c_int32, C.c_double, C.c_double, C.c_int32, C.c_double, C.c_double, _dp, C.c_int32,
                _dp, _ip, C.c_int32, C.c_double, C.c_double, _dp, C.c_int32, C.c_int64, _dp]
-        for f in ("cbf_lle1d", "cbf_lle1d_ic", "cbf_lle2d", "cbf_lle2d_ic"):
+        for f in ("cbf_lle1d", "cbf_lle1d_ic", "cbf_lle2d", "cbf_lle2d_ic", "cbf_ls1d", "cbf_ls2d"):
             getattr(L, f).argtypes = lle
         for f in ("cbf_device_count", "cbf_set_device", "cbf_validate", "cbf_run", "cbf_run_host",
                   "cbf_grid_coordinates", "cbf_probe_fp64_peak", "cbf_probe_expf_zero",
                   "cbf_divergence_threshold", "cbf_bifurcation1d", "cbf_bifurcation1d_ic",
                   "cbf_bifurcation2d_kde", "cbf_bifurcation2d_kde_ic", "cbf_bifurcation2d_dbscan",
                   "cbf_bifurcation2d_dbscan_ic", "cbf_lle1d", "cbf_lle1d_ic", "cbf_lle2d",
-                  "cbf_lle2d_ic"):
+                  "cbf_lle2d_ic", "cbf_ls1d", "cbf_ls2d"):
             getattr(L, f).restype = C.c_int32
         L.cbf_csv_write_map.restype = C.c_int32
         L.cbf_csv_write_map.argtypes = [C.c_char_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int32,
@@ -237,6 +238,9 @@ def lib():
         L.cbf_csv_write_peaks.restype = C.c_int32
         L.cbf_csv_write_peaks.argtypes = [C.c_char_p, C.c_int32, C.c_void_p, C.c_int64, C.c_int64,
                                           C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]
+        L.cbf_csv_write_rows.restype = C.c_int32
+        L.cbf_csv_write_rows.argtypes = [C.c_char_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64,
+                                         C.c_int32, C.c_int32]
         L.cbf_csv_write_pairs.restype = C.c_int32
         L.cbf_csv_write_pairs.argtypes = [C.c_char_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64,
                                           C.c_int32]
@@ -332,6 +336,8 @@ def run_host(job: Job):
     elif job.task == TASK_LLE_REGIME:
         out = np.zeros(n, np.float64)
         aux = np.zeros(n, np.int32)
+    elif job.task == TASK_LS:
+        out = np.zeros((n, job.nIC), np.float64)
     elif job.task in (TASK_KDE, TASK_DBSCAN):
         out = np.zeros(n, np.int32)
     else:
@@ -521,9 +527,11 @@ def set_lle_variant(system, variant: int) -> None:
 
 
 def lle_seeds(job: Job) -> np.ndarray:
-    """Device-computed LLE perturbation vectors, shape (points, nIC)."""
+    """Device-computed perturbation vectors: LLE jobs (points, nIC); LS jobs the
+    seed rows (points, nIC, nIC)."""
     n = lib().cbf_job_points(C.byref(job))
-    out = np.zeros((n, job.nIC), np.float64)
+    shape = (n, job.nIC, job.nIC) if job.task == TASK_LS else (n, job.nIC)
+    out = np.zeros(shape, np.float64)
     check(lib().cbf_lle_seeds(C.byref(job), out.ctypes.data_as(_dp)))
     return out
 
@@ -668,6 +676,38 @@ def _lle(fn, dims, system, tMax, NT, nPts, h, eps, icv, nIC, ranges, idx, wv, ma
     check(fn(_sys(system), tMax, NT, nPts, h, eps, icp, nIC, rp, ixp, wv, maxValue, transient, vp,
              nV, seedChunk, out.ctypes.data_as(_dp)))
     return out.reshape((nPts, nPts) if dims == 2 else (nPts,))
+
+
+def _ls(fn, dims, system, tMax, NT, nPts, h, eps, icv, nIC, ranges, idx, wv, maxValue, transient,
+        values, nV, seedChunk):
+    ic, icp = _d(icv)
+    r, rp = _d(ranges)
+    ix, ixp = _i(idx)
+    v, vp = _d(values)
+    n = nPts ** dims
+    out = np.zeros((n, nIC), np.float64)
+    check(fn(_sys(system), tMax, NT, nPts, h, eps, icp, nIC, rp, ixp, wv, maxValue, transient, vp,
+             nV, seedChunk, out.ctypes.data_as(_dp)))
+    return out.reshape((nPts, nPts, nIC) if dims == 2 else (nPts, nIC))
+
+
+def LS1D(tMax, NT, nPts, h, eps, initialConditions, amountOfInitialConditions, ranges,
+         indicesOfMutVars, writableVar, maxValue, transientTime, values, amountOfValues, *,
+         system="memristive5", seedChunk=0):
+    """hostLibrary.cuh:482-496: the Lyapunov spectrum per point, shape (nPts, nIC)."""
+    return _ls(lib().cbf_ls1d, 1, system, tMax, NT, nPts, h, eps, initialConditions,
+               amountOfInitialConditions, ranges, indicesOfMutVars, writableVar, maxValue,
+               transientTime, values, amountOfValues, seedChunk)
+
+
+def LS2D(tMax, NT, nPts, h, eps, initialConditions, amountOfInitialConditions, ranges,
+         indicesOfMutVars, writableVar, maxValue, transientTime, values, amountOfValues, *,
+         system="memristive5", seedChunk=0):
+    """hostLibrary.cuh:520-534: the spectrum per grid point, shape (nPts, nPts, nIC)
+    (row = axis 1)."""
+    return _ls(lib().cbf_ls2d, 2, system, tMax, NT, nPts, h, eps, initialConditions,
+               amountOfInitialConditions, ranges, indicesOfMutVars, writableVar, maxValue,
+               transientTime, values, amountOfValues, seedChunk)
 
 
 def LLE1D(tMax, NT, nPts, h, eps, initialConditions, amountOfInitialConditions, ranges,

@@ -158,7 +158,7 @@ cbf_status lower_job(const cbf_job* j, DevJob* d)
     memset(d, 0, sizeof(*d));
     const int dim = system_dim(j->system);
     if (dim < 0) return fail(CBF_ERR_UNKNOWN_SYSTEM, "unknown system id %d", j->system);
-    if (j->task < CBF_TASK_PEAKS || j->task > CBF_TASK_LLE_REGIME)
+    if (j->task < CBF_TASK_PEAKS || j->task > CBF_TASK_LS)
         return fail(CBF_ERR_INVALID_ARG, "unknown task %d", j->task);
     if (j->dims != 1 && j->dims != 2) return fail(CBF_ERR_INVALID_ARG, "dims must be 1 or 2 (got %d)", j->dims);
     if (j->nPts < 1) return fail(CBF_ERR_INVALID_ARG, "nPts must be >= 1 (got %d)", j->nPts);
@@ -173,9 +173,10 @@ cbf_status lower_job(const cbf_job* j, DevJob* d)
         if (j->idxMut[i] < 0 || j->idxMut[i] >= limit)
             return fail(CBF_ERR_INVALID_ARG, "indicesOfMutVars[%d]=%d out of range [0,%d)", i,
                         j->idxMut[i], limit);
-    // The LLE kernels always check x[0] and ignore writableVar (cudaLibrary.cu:735-753).
-    const bool lleTask = (j->task == CBF_TASK_LLE || j->task == CBF_TASK_LLE_REGIME);
-    if (j->task != CBF_TASK_LLE && (j->writableVar < 0 || j->writableVar >= dim))
+    // The LLE and LS kernels always check x[0] and ignore writableVar
+    // (cudaLibrary.cu:735-753, 1049-1060).
+    const bool lleTask = (j->task == CBF_TASK_LLE || j->task == CBF_TASK_LLE_REGIME || j->task == CBF_TASK_LS);
+    if (j->task != CBF_TASK_LLE && j->task != CBF_TASK_LS && (j->writableVar < 0 || j->writableVar >= dim))
         return fail(CBF_ERR_INVALID_ARG, "writableVar %d out of range [0,%d)", j->writableVar, dim);
     if (!(isfinite(j->h) && j->h != 0)) return fail(CBF_ERR_INVALID_ARG, "h must be finite and nonzero");
 
@@ -294,6 +295,7 @@ size_t out_bytes(const DevJob& d)
     switch (d.task) {
     case CBF_TASK_LLE:
     case CBF_TASK_LLE_REGIME: return (size_t)d.nPoints * sizeof(double);
+    case CBF_TASK_LS: return (size_t)d.nPoints * (size_t)d.nIC * sizeof(double);
     case CBF_TASK_KDE:
     case CBF_TASK_DBSCAN: return (size_t)d.nPoints * sizeof(int);
     default: return (size_t)d.nPoints * (size_t)d.peakCap * sizeof(double);
@@ -315,6 +317,8 @@ cbf_status run_lowered(const DevJob& d, void* d_out, void* d_aux, cudaStream_t s
         e = launch_lle(d, (double*)d_out, s);
     else if (d.task == CBF_TASK_LLE_REGIME)
         e = launch_lle_regime(d, (double*)d_out, (int*)d_aux, s);
+    else if (d.task == CBF_TASK_LS)
+        e = launch_ls(d, (double*)d_out, s);
     else
         e = launch_bif(d, d_out, (int*)d_aux, s);
     if (e == cudaErrorAssert) return fail(CBF_ERR_INTERNAL, "device-side iteration guard fired");
@@ -444,6 +448,23 @@ cbf_status lle(bool ic_sweep, int dims, int32_t system, double tMax, double NT, 
     return run_host_impl(&j, out, nullptr);
 }
 
+cbf_status ls(int dims, int32_t system, double tMax, double NT, int32_t nPts, double h, double eps,
+              const double* ic, int32_t nIC, const double* ranges, const int32_t* idxMut, int32_t wv,
+              double maxValue, double transientTime, const double* values, int32_t nV,
+              int64_t seedChunk, double* out)
+{
+    cbf_status st = check_ptrs(nIC, ic, ranges, idxMut, values, nV);
+    if (st != CBF_OK) return st;
+    cbf_job j;
+    fill_common(&j, system, dims, nPts, h, nIC, ic, ranges, idxMut, wv, maxValue, transientTime, values, nV);
+    j.task = CBF_TASK_LS;
+    j.tMax = tMax;
+    j.NT = NT;
+    j.lleEps = eps;
+    j.seedChunk = seedChunk;
+    return run_host_impl(&j, out, nullptr);
+}
+
 }  // namespace
 
 cbf_status lower_job_for(const cbf_job* job, DevJob* d) { return lower_job(job, d); }
@@ -516,7 +537,7 @@ int32_t cbf_record_length(const cbf_job* j)
 {
     if (!j) return -1;
     int v = 0;
-    if (j->task == CBF_TASK_LLE || j->task == CBF_TASK_LLE_REGIME) {
+    if (j->task == CBF_TASK_LLE || j->task == CBF_TASK_LLE_REGIME || j->task == CBF_TASK_LS) {
         if (j->NT == 0 || !to_int(j->tMax / j->NT, &v)) return -1;
     } else {
         if (j->h == 0 || j->preScaller < 1 || !to_int(j->tMax / j->h / (double)j->preScaller, &v)) return -1;
@@ -657,6 +678,24 @@ cbf_status cbf_lle2d_ic(int32_t system, double tMax, double NT, int32_t nPts, do
                transientTime, values, nV, seedChunk, out);
 }
 
+cbf_status cbf_ls1d(int32_t system, double tMax, double NT, int32_t nPts, double h, double eps,
+                    const double* ic, int32_t nIC, const double* ranges, const int32_t* idxMut,
+                    int32_t wv, double maxValue, double transientTime, const double* values,
+                    int32_t nV, int64_t seedChunk, double* out)
+{
+    return ls(1, system, tMax, NT, nPts, h, eps, ic, nIC, ranges, idxMut, wv, maxValue, transientTime,
+              values, nV, seedChunk, out);
+}
+
+cbf_status cbf_ls2d(int32_t system, double tMax, double NT, int32_t nPts, double h, double eps,
+                    const double* ic, int32_t nIC, const double* ranges, const int32_t* idxMut,
+                    int32_t wv, double maxValue, double transientTime, const double* values,
+                    int32_t nV, int64_t seedChunk, double* out)
+{
+    return ls(2, system, tMax, NT, nPts, h, eps, ic, nIC, ranges, idxMut, wv, maxValue, transientTime,
+              values, nV, seedChunk, out);
+}
+
 cbf_status cbf_grid_coordinates(const cbf_job* job, double* out_host)
 {
     DevJob d;
@@ -752,16 +791,17 @@ cbf_status cbf_lle_seeds(const cbf_job* job, double* out_host)
     DevJob d;
     cbf_status st = lower_job(job, &d);
     if (st != CBF_OK) return st;
-    if (d.task != CBF_TASK_LLE && d.task != CBF_TASK_LLE_REGIME)
-        return fail(CBF_ERR_INVALID_ARG, "cbf_lle_seeds needs an LLE job");
+    if (d.task != CBF_TASK_LLE && d.task != CBF_TASK_LLE_REGIME && d.task != CBF_TASK_LS)
+        return fail(CBF_ERR_INVALID_ARG, "cbf_lle_seeds needs an LLE or LS job");
     if (!out_host) return fail(CBF_ERR_INVALID_ARG, "null output");
     if (d.nPoints == 0) return CBF_OK;
     cudaStream_t s;
     if ((st = library_stream(&s)) != CBF_OK) return st;
     double* dd = nullptr;
-    const size_t bytes = (size_t)d.nPoints * d.nIC * sizeof(double);
+    const size_t per = d.task == CBF_TASK_LS ? (size_t)d.nIC * d.nIC : (size_t)d.nIC;
+    const size_t bytes = (size_t)d.nPoints * per * sizeof(double);
     CBF_CUDA(cudaMallocAsync((void**)&dd, bytes, s));
-    cudaError_t e = launch_lle_seeds(d, dd, s);
+    cudaError_t e = d.task == CBF_TASK_LS ? launch_ls_seeds(d, dd, s) : launch_lle_seeds(d, dd, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(out_host, dd, bytes, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     cudaFreeAsync(dd, s);

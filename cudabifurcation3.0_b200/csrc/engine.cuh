@@ -139,6 +139,29 @@ __device__ __forceinline__ void lle_seed(long long g, long long seedChunk, doubl
     for (int i = 0; i < D; ++i) z[i] /= zPower;
 }
 
+// Initial perturbation rows of the Lyapunov-spectrum kernel (LSKernelCUDA,
+// cudaLibrary.cu:1001-1013): row j, entry i = 0.5 sinf(0.2171828 (i+1)(j+1) + idx
+// + (0.2171828 + i j idx)) in the reference's operation order (double sum, FP32
+// sinf), idx the chunk-local index; each row normalised to length 1.
+template <int D>
+__device__ __forceinline__ void ls_seed(long long g, long long seedChunk, double (&z)[D][D])
+{
+    const int idx = (int)(seedChunk > 0 ? (g % seedChunk) : g);
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+        double zPower = 0;
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+            const double arg = 0.2171828 * (i + 1) * (j + 1) + idx + (0.2171828 + i * j * idx);
+            z[j][i] = (double)sinf((float)arg) * 0.5;
+            zPower += z[j][i] * z[j][i];
+        }
+        zPower = sqrt(zPower);
+#pragma unroll
+        for (int i = 0; i < D; ++i) z[j][i] /= zPower;
+    }
+}
+
 // Kernel launch bookkeeping (defined in capi.cu).
 void note_launch(unsigned n = 1);
 
@@ -155,6 +178,10 @@ int lle_variant_for(int system);
 cudaError_t launch_bif(const DevJob& J, void* d_out, int* d_aux, cudaStream_t s);
 cudaError_t launch_grid_coords(const DevJob& J, double* d_out, cudaStream_t s);
 cudaError_t launch_lle_seeds(const DevJob& J, double* d_out, cudaStream_t s);
+// Lyapunov spectrum: nIC exponents per point (d_out[p*nIC + i]); seed rows
+// (nIC x nIC per point) for parity checks.
+cudaError_t launch_ls(const DevJob& J, double* d_out, cudaStream_t s);
+cudaError_t launch_ls_seeds(const DevJob& J, double* d_out, cudaStream_t s);
 cudaError_t launch_lle_regime(const DevJob& J, double* d_lle, int* d_class, cudaStream_t s);
 // Points the LLE_REGIME kernel keeps in flight at once on the current device.
 long long lle_regime_resident_points(const DevJob& J);

@@ -300,6 +300,45 @@ void lle_common(int variant, double tMax, double NT, int nPts, double h, double 
                                    variant == 2 ? ranges : nullptr, 6));
 }
 
+// Chunk of the reference's LS launches, to which its seed index is local:
+// min(points, (free/4) / (8 * blocks * nIC)) (hostLibrary.cu:1820-1826, :1945-1951).
+long long ls_seed_chunk(int dims, double tMax, double NT, int nPts, int nIC)
+{
+    const long long total = dims == 2 ? (long long)nPts * nPts : nPts;
+    size_t freeB = 0, totalB = 0;
+    if (cudaMemGetInfo(&freeB, &totalB) != cudaSuccess) return 0;
+    const int blocks = (int)(tMax / NT);
+    if (blocks <= 0 || nIC <= 0) return 0;
+    long long lim = (long long)((freeB / 4) / (sizeof(double) * (size_t)blocks * (size_t)nIC));
+    if (lim > total) lim = total;
+    return lim > 0 ? lim : 1;
+}
+
+void ls_common(int dims, double tMax, double NT, int nPts, double h, double eps, const double* icv,
+               int nIC, const double* ranges, const int* idx, int wv, double maxValue,
+               double transientTime, const double* values, int nV)
+{
+    const long long total = dims == 2 ? (long long)nPts * nPts : nPts;
+    const int cols = nIC > 0 ? nIC : 0;
+    std::vector<double> res((size_t)(total > 0 ? total : 0) * (size_t)cols);
+    const long long seedChunk = ls_seed_chunk(dims, tMax, NT, nPts, nIC);
+    const cbf_status st = (dims == 1 ? cbf_ls1d : cbf_ls2d)(current_system(), tMax, NT, nPts, h, eps, icv,
+                                                           nIC, ranges, idx, wv, maxValue, transientTime,
+                                                           values, nV, seedChunk, res.data());
+    CBF_CHECK(st);
+    const std::string path = current_path();
+    if (dims == 1) {
+        io_check(cbf_csv_write_rows(path.c_str(), nPts, ranges, res.data(), total, cols, 6));
+        return;
+    }
+    std::vector<double> col((size_t)(total > 0 ? total : 0));
+    for (int k = 0; k < cols; ++k) {
+        for (long long m = 0; m < total; ++m) col[(size_t)m] = res[(size_t)m * cols + k];
+        const std::string p = path + std::to_string(k + 1) + ".csv";
+        io_check(cbf_csv_write_map(p.c_str(), col.data(), 1, total, nPts, ranges, 6));
+    }
+}
+
 }  // namespace
 
 // hostLibrary.cu:7-158
@@ -431,6 +470,28 @@ void LLE2DIC(const double tMax, const double NT, const int nPts, const double h,
                indicesOfMutVars, writableVar, maxValue, transientTime, values, amountOfValues);
 }
 
+// hostLibrary.cu:1802-1924
+void LS1D(const double tMax, const double NT, const int nPts, const double h, const double eps,
+          const double* initialConditions, const int amountOfInitialConditions,
+          const double* ranges, const int* indicesOfMutVars, const int writableVar,
+          const double maxValue, const double transientTime, const double* values,
+          const int amountOfValues)
+{
+    ls_common(1, tMax, NT, nPts, h, eps, initialConditions, amountOfInitialConditions, ranges,
+              indicesOfMutVars, writableVar, maxValue, transientTime, values, amountOfValues);
+}
+
+// hostLibrary.cu:1928-2082
+void LS2D(const double tMax, const double NT, const int nPts, const double h, const double eps,
+          const double* initialConditions, const int amountOfInitialConditions,
+          const double* ranges, const int* indicesOfMutVars, const int writableVar,
+          const double maxValue, const double transientTime, const double* values,
+          const int amountOfValues)
+{
+    ls_common(2, tMax, NT, nPts, h, eps, initialConditions, amountOfInitialConditions, ranges,
+              indicesOfMutVars, writableVar, maxValue, transientTime, values, amountOfValues);
+}
+
 void cbfSetSystem(int system) { g_system.store(system); }
 int cbfGetSystem() { return current_system(); }
 
@@ -516,6 +577,26 @@ extern "C" cbf_status cbf_csv_write_pairs(const char* path, int32_t nPts, const 
         out.dbl(host_value_by_idx((int)k, nPts, ranges[0], ranges[1], 0));
         out.str(", ");
         out.dbl(values[k]);
+        out.str("\n");
+    }
+    return CBF_OK;
+}
+
+extern "C" cbf_status cbf_csv_write_rows(const char* path, int32_t nPts, const double* ranges,
+                                         const double* values, int64_t n, int32_t nCols,
+                                         int32_t precision)
+{
+    if (!path || !ranges || nCols < 0 || (n > 0 && nCols > 0 && !values)) return CBF_ERR_INVALID_ARG;
+    CsvOut out(path);
+    out.precision(precision);
+    if (open_or_fail(out, n) != CBF_OK) return CBF_ERR_IO;
+    // "param, v1, ..., vN\n" (hostLibrary.cu:1900-1910)
+    for (long long k = 0; k < n; ++k) {
+        out.dbl(host_value_by_idx((int)k, nPts, ranges[0], ranges[1], 0));
+        for (int c = 0; c < nCols; ++c) {
+            out.str(", ");
+            out.dbl(values[(size_t)k * nCols + c]);
+        }
         out.str("\n");
     }
     return CBF_OK;

@@ -62,6 +62,9 @@ typedef int32_t cbf_status;
                                    regimeChaosLle), more than maxAmountOfPeaks peaks or >= 15
                                    clusters, else the DBSCAN cluster count */
 
+#define CBF_TASK_LS 6           /* Lyapunov spectrum: nIC exponents per point (double[n*nIC],
+                                   point-major), LSKernelCUDA semantics */
+
 /* Job flags. */
 #define CBF_FLAG_EXACT_GRID 1u  /* integer grid index instead of the FP32 quirk */
 #define CBF_FLAG_KDE_FIXED 2u   /* KDE with kdeSampling samples in total, not per peak */
@@ -132,7 +135,7 @@ cbf_status cbf_validate(const cbf_job* job);
 /* ---- device-resident interface --------------------------------------- */
 /* Run one job on `stream` (a cudaStream_t, NULL = legacy default stream).
  * d_out: LLE double[n]; KDE/DBSCAN int32[n]; PEAKS double[n*cap];
- *        TRAJECTORY double[n*record].
+ *        TRAJECTORY double[n*record]; LS double[n*nIC].
  * d_aux: PEAKS int32[n] peak counts; TRAJECTORY int32[n] diverged flags; else unused.
  * Scratch for KDE/DBSCAN is taken from the stream-ordered allocator. */
 cbf_status cbf_run(const cbf_job* job, void* d_out, void* d_aux, void* stream);
@@ -343,6 +346,25 @@ cbf_status cbf_lle2d_ic(int32_t system, double tMax, double NT, int32_t nPts, do
                         const int32_t* indicesOfMutVars, int32_t writableVar, double maxValue,
                         double transientTime, const double* values, int32_t amountOfValues,
                         int64_t seedChunk, double* out);
+
+/* Lyapunov spectra (hostLibrary.cu:1802-1924 LS1D, :1928-2082 LS2D): out
+ * double[points * amountOfInitialConditions], the exponents of point k at
+ * out[k*nIC .. k*nIC+nIC).  seedChunk: the chunk the reference's seed index is
+ * local to (its nPtsLimiter; 0 = the global index). */
+cbf_status cbf_ls1d(int32_t system, double tMax, double NT, int32_t nPts, double h, double eps,
+                    const double* initialConditions, int32_t amountOfInitialConditions,
+                    const double* ranges, const int32_t* indicesOfMutVars, int32_t writableVar,
+                    double maxValue, double transientTime, const double* values,
+                    int32_t amountOfValues, int64_t seedChunk, double* out);
+cbf_status cbf_ls2d(int32_t system, double tMax, double NT, int32_t nPts, double h, double eps,
+                    const double* initialConditions, int32_t amountOfInitialConditions,
+                    const double* ranges, const int32_t* indicesOfMutVars, int32_t writableVar,
+                    double maxValue, double transientTime, const double* values,
+                    int32_t amountOfValues, int64_t seedChunk, double* out);
+/* CSV rows "param, v1, v2, ...\n" (LS1D layout, hostLibrary.cu:1900-1910) for n
+ * points with nCols values each (row-major). */
+cbf_status cbf_csv_write_rows(const char* path, int32_t nPts, const double* ranges,
+                              const double* values, int64_t n, int32_t nCols, int32_t precision);
 
 /* DBSCAN cluster-count map that allocates no device memory.  No counterpart in
  * the reference.  For callers that cannot call cudaMalloc: programs whose device

@@ -97,6 +97,20 @@ void LLE2DIC(const double tMax, const double NT, const int nPts, const double h,
              const double maxValue, const double transientTime, const double* values,
              const int amountOfValues);
 
+// Lyapunov spectra.  LS1D writes "param, l1, ..., lN" rows to the output path;
+// LS2D writes one map per exponent to <output path><k>.csv, k = 1..N, with the
+// 2-D map layout (hostLibrary.cu:1802-2082).
+void LS1D(const double tMax, const double NT, const int nPts, const double h, const double eps,
+          const double* initialConditions, const int amountOfInitialConditions,
+          const double* ranges, const int* indicesOfMutVars, const int writableVar,
+          const double maxValue, const double transientTime, const double* values,
+          const int amountOfValues);
+void LS2D(const double tMax, const double NT, const int nPts, const double h, const double eps,
+          const double* initialConditions, const int amountOfInitialConditions,
+          const double* ranges, const int* indicesOfMutVars, const int writableVar,
+          const double maxValue, const double transientTime, const double* values,
+          const int amountOfValues);
+
 // Run-time configuration of what the reference fixes at compile time.
 void cbfSetSystem(int system);            // CBF_SYS_* from cbf.h
 int cbfGetSystem();

@@ -718,6 +718,124 @@ int orc_map_lle_regime_list(const orc_job* job, const int64_t* idx, int64_t coun
     return 0;
 }
 
+/* ------------------------------------------------------------------------- */
+/* Lyapunov spectrum (LSKernelCUDA, cudaLibrary.cu:960-1100).                 */
+
+/* projectionOperator (cudaLibrary.cu:913-927): minuend -= (a.b / b.b) b, with
+ * the fraction 0 when b.b == 0; sums accumulated in index order. */
+void orc_projection(const double* a, const double* b, double* minuend, int n)
+{
+    double numerator = 0, denominator = 0;
+    for (int i = 0; i < n; ++i) {
+        numerator += a[i] * b[i];
+        denominator += b[i] * b[i];
+    }
+    const double fraction = denominator == 0 ? 0 : numerator / denominator;
+    for (int i = 0; i < n; ++i)
+        minuend[i] -= fraction * b[i];
+}
+
+/* gramSchmidtProcess (cudaLibrary.cu:931-956): classical Gram-Schmidt of the n
+ * rows of a into b (each row projected against the not yet normalised earlier
+ * rows of b), then every row of b normalised; den[i] (optional) = the norm. */
+void orc_gram_schmidt(const double* a, double* b, int n, double* den)
+{
+    for (int i = 0; i < n; ++i) {
+        for (int j = 0; j < n; ++j)
+            b[j + i * n] = a[j + i * n];
+        for (int j = 0; j < i; ++j)
+            orc_projection(a + i * n, b + j * n, b + i * n, n);
+    }
+    for (int i = 0; i < n; ++i) {
+        double d = 0;
+        for (int j = 0; j < n; ++j)
+            d += b[i * n + j] * b[i * n + j];
+        d = sqrt(d);
+        for (int j = 0; j < n; ++j)
+            b[i * n + j] = d == 0 ? 0 : b[i * n + j] / d;
+        if (den)
+            den[i] = d;
+    }
+}
+
+/* Initial perturbation rows (cudaLibrary.cu:1001-1013): row j, entry i =
+ * 0.5 sinf(0.2171828 (i+1)(j+1) + idx + (0.2171828 + i j idx)) with idx the
+ * chunk-local point index, each row normalised to length 1. */
+void orc_ls_seed(const orc_job* job, int64_t g, double* z)
+{
+    const int n = job->nIC;
+    const int idx = (int)(job->seedChunk > 0 ? g % job->seedChunk : g);
+    for (int j = 0; j < n; ++j) {
+        double zPower = 0;
+        for (int i = 0; i < n; ++i) {
+            const double arg = 0.2171828 * (i + 1) * (j + 1) + idx + (0.2171828 + i * j * idx);
+            z[j * n + i] = (double)sinf((float)arg) * 0.5;
+            zPower += z[j * n + i] * z[j * n + i];
+        }
+        zPower = sqrt(zPower);
+        for (int i = 0; i < n; ++i)
+            z[j * n + i] /= zPower;
+    }
+}
+
+/* One point of LSKernelCUDA: the nIC exponents into out[0..nIC).  zIn (n*n,
+ * optional) replaces the seed rows. */
+void orc_ls_point(const orc_job* job, int64_t g, const double* zIn, double* out)
+{
+    double x[8], y[64], z[64], v[16], den[8], result[8];
+    const int n = job->nIC;
+    setup_point(job, g, x, v);
+    if (zIn) {
+        for (int i = 0; i < n * n; ++i)
+            z[i] = zIn[i];
+    } else {
+        orc_ls_seed(job, g, z);
+    }
+    const int sys = job->system;
+    const double h = job->h;
+    const int nNT = (int)(size_t)(job->NT / h);
+    const int sizeOfBlock = (int)(job->tMax / job->NT);
+    const double eps = job->lleEps;
+    for (int i = 0; i < n; ++i)
+        result[i] = 0;
+
+    orc_loop(sys, x, v, h, orc_skip_len(job), 1, 0, job->maxValue, NULL, 0, 1);
+    orc_gram_schmidt(z, y, n, NULL);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i)
+            y[j * n + i] = y[j * n + i] * eps + x[i];
+
+    for (int b = 0; b < sizeOfBlock; ++b) {
+        /* every trajectory stops at its own first violation (cudaLibrary.cu:1049-1060) */
+        orc_loop(sys, x, v, h, nNT, 1, 0, job->maxValue, NULL, 0, 1);
+        for (int j = 0; j < n; ++j)
+            orc_loop(sys, y + j * n, v, h, nNT, 1, 0, job->maxValue, NULL, 0, 1);
+        for (int k = 0; k < n; ++k)
+            for (int l = 0; l < n; ++l)
+                y[k * n + l] = y[k * n + l] - x[l];
+        orc_gram_schmidt(y, z, n, den);
+        for (int k = 0; k < n; ++k) {
+            result[k] += log(den[k] / eps);
+            for (int j = 0; j < n; ++j)
+                y[k * n + j] = (double)(x[j] + z[k * n + j] * eps);
+        }
+    }
+    for (int i = 0; i < n; ++i)
+        out[i] = result[i] / job->tMax;
+}
+
+int orc_map_ls_list(const orc_job* job, const int64_t* idx, int64_t count, const double* z,
+                    double* out, int nThreads)
+{
+    if (job->nIC <= 0 || job->nIC > 8)
+        return -1;
+    const int n = job->nIC;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads_or_default(nThreads))
+    for (int64_t k = 0; k < count; ++k)
+        orc_ls_point(job, idx[k], z ? z + k * n * n : NULL, out + k * n);
+    return 0;
+}
+
 int orc_map_lle_list(const orc_job* job, const int64_t* idx, int64_t count, double* out, int nThreads)
 {
     if ((int)(job->tMax / job->NT) <= 0 || job->nIC <= 0)

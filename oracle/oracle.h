@@ -133,6 +133,13 @@ int orc_map_lle_list(const orc_job* job, const int64_t* idx, int64_t count, doub
  * regimeChaosLle > 0 and the LLE exceeds it,
  * 15 if more than maxAmountOfPeaks peaks, else min(dbscan, 15). */
 double orc_lle_regime_point(const orc_job* job, int64_t g, const double* z, int32_t* cls);
+/* Lyapunov spectrum (LSKernelCUDA, cudaLibrary.cu:913-1100). */
+void orc_projection(const double* a, const double* b, double* minuend, int n);
+void orc_gram_schmidt(const double* a, double* b, int n, double* den);
+void orc_ls_seed(const orc_job* job, int64_t g, double* z);
+void orc_ls_point(const orc_job* job, int64_t g, const double* z, double* out);
+int orc_map_ls_list(const orc_job* job, const int64_t* idx, int64_t count, const double* z,
+                    double* out, int nThreads);
 int orc_map_lle_regime_list(const orc_job* job, const int64_t* idx, int64_t count,
                             const double* z, double* outLle, int32_t* outCls, int nThreads);
 

@@ -156,6 +156,14 @@ def lib():
         L.orc_lle_seed.argtypes = [C.POINTER(OrcJob), C.c_int64, _dp]
         L.orc_map_lle_seeded.restype = C.c_int
         L.orc_map_lle_seeded.argtypes = [C.POINTER(OrcJob), C.c_int64, C.c_int64, _dp, _dp, C.c_int]
+        L.orc_map_ls_list.restype = C.c_int
+        L.orc_map_ls_list.argtypes = [C.POINTER(OrcJob), _lp, C.c_int64, C.c_void_p, _dp, C.c_int]
+        L.orc_ls_seed.restype = None
+        L.orc_ls_seed.argtypes = [C.POINTER(OrcJob), C.c_int64, _dp]
+        L.orc_gram_schmidt.restype = None
+        L.orc_gram_schmidt.argtypes = [_dp, _dp, C.c_int, C.c_void_p]
+        L.orc_projection.restype = None
+        L.orc_projection.argtypes = [_dp, _dp, _dp, C.c_int]
         L.orc_map_lle_regime_list.restype = C.c_int
         L.orc_map_lle_regime_list.argtypes = [C.POINTER(OrcJob), _lp, C.c_int64, C.c_void_p, _dp,
                                               _ip, C.c_int]
@@ -191,6 +199,11 @@ def ref():
         R.ref_distance.argtypes = [C.c_double] * 4
         R.ref_dbscan.restype = C.c_int
         R.ref_dbscan.argtypes = [_dp, _dp, _dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double]
+        if hasattr(R, "ref_gramSchmidtProcess"):
+            R.ref_gramSchmidtProcess.restype = None
+            R.ref_gramSchmidtProcess.argtypes = [_dp, _dp, C.c_int, C.c_void_p]
+            R.ref_projectionOperator.restype = None
+            R.ref_projectionOperator.argtypes = [_dp, _dp, _dp, C.c_int]
         _ref = R
     return _ref
 
@@ -302,6 +315,43 @@ def lle_seeds(job: OrcJob, first: int, count: int):
         lib().orc_lle_seed(C.byref(job), first + k, row)
         out[k] = row
     return out
+
+
+def map_ls(job: OrcJob, idx, z=None, threads: int = 0):
+    """Lyapunov spectra (nIC exponents) at grid indices idx; z (optional, per point
+    nIC x nIC seed rows) replaces the oracle's own seeds."""
+    idx = np.ascontiguousarray(idx, dtype=np.int64)
+    n = job.nIC
+    out = np.zeros((len(idx), n), np.float64)
+    zp = None
+    if z is not None:
+        z = np.ascontiguousarray(z, dtype=np.float64)
+        zp = z.ctypes.data_as(C.c_void_p)
+    rc = lib().orc_map_ls_list(C.byref(job), idx, len(idx), zp, out, threads)
+    if rc != 0:
+        raise RuntimeError(f"orc_map_ls_list failed: {rc}")
+    return out
+
+
+def ls_seeds(job: OrcJob, idx):
+    """The oracle's seed rows (glibc sinf) for grid indices idx: (len, nIC, nIC)."""
+    n = job.nIC
+    out = np.zeros((len(idx), n, n), np.float64)
+    for k, g in enumerate(idx):
+        row = np.zeros(n * n, np.float64)
+        lib().orc_ls_seed(C.byref(job), int(g), row)
+        out[k] = row.reshape(n, n)
+    return out
+
+
+def gram_schmidt(a, with_den: bool = True):
+    """orc_gram_schmidt on an (n, n) array: (b, den)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    n = a.shape[0]
+    b = np.zeros_like(a)
+    den = np.zeros(n, np.float64)
+    lib().orc_gram_schmidt(a, b, n, den.ctypes.data_as(C.c_void_p) if with_den else None)
+    return b, den
 
 
 def map_lle_regime(job: OrcJob, idx, z=None, threads: int = 0):

@@ -8,6 +8,12 @@
 // Nothing from the reference is copied: the header is included from its tree.
 #include "cudaLibrary.cuh"
 
+// Defined __device__ __host__ in cudaLibrary.cu (:913-956) without a header
+// declaration; declared here with the definition's signature.
+__device__ __host__ void projectionOperator(double* a, double* b, double* minuend, int amountOfValues);
+__device__ __host__ void gramSchmidtProcess(double* a, double* b, int amountOfVectorsAndValuesInVector,
+                                            double* denominators);
+
 extern "C" {
 
 // cudaLibrary.cu:210-216
@@ -57,6 +63,18 @@ int ref_dbscan(double* data, double* intervals, double* helpfulArray, int startD
 {
     return dbscan(data, intervals, helpfulArray, startDataIndex, amountOfPeaks, sizeOfHelpfulArray,
                   maxAmountOfPeaks, 0, eps, nullptr);
+}
+
+// cudaLibrary.cu:913-927
+void ref_projectionOperator(double* a, double* b, double* minuend, int n)
+{
+    projectionOperator(a, b, minuend, n);
+}
+
+// cudaLibrary.cu:931-956
+void ref_gramSchmidtProcess(double* a, double* b, int n, double* denominators)
+{
+    gramSchmidtProcess(a, b, n, denominators);
 }
 
 }  // extern "C"

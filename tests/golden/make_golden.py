@@ -151,6 +151,40 @@ def main() -> int:
     out.update(m5_vals=vals, m5_x0=x0, m5_pre=pre, m5_wv=wv, m5_max=mv, m5_steps=np.int32(steps),
                m5_x=np.array(xs), m5_data=np.array(datas), m5_ok=np.array(oks, np.int32))
 
+    # projectionOperator / gramSchmidtProcess (cudaLibrary.cu:913-956) of the
+    # Lyapunov-spectrum kernel, n = 3 and 5, including rank-deficient inputs (a
+    # zero row, a repeated row) and scales from 1e-9 to 10.
+    gs_n, gs_a, gs_b, gs_d = [], [], [], []
+    pj_a, pj_b, pj_m, pj_out = [], [], [], []
+    for r in range(60):
+        n = 3 if r % 2 == 0 else 5
+        a = rng.normal(size=(n, n)) * 10.0 ** float(rng.integers(-9, 2))
+        if r % 10 == 3:
+            a[1] = 0.0
+        if r % 10 == 7:
+            a[2] = a[0]
+        a = np.ascontiguousarray(a)
+        b = np.zeros((n, n))
+        d = np.zeros(n)
+        R.ref_gramSchmidtProcess(a.copy(), b, n, d.ctypes.data_as(C.c_void_p))
+        pad = lambda m: np.pad(m, ((0, 5 - n), (0, 5 - n)))
+        gs_n.append(n)
+        gs_a.append(pad(a))
+        gs_b.append(pad(b))
+        gs_d.append(np.pad(d, (0, 5 - n)))
+        m = rng.normal(size=n)
+        if r % 10 == 5:
+            a[1] = 0.0
+        mm = m.copy()
+        R.ref_projectionOperator(np.ascontiguousarray(a[0]), np.ascontiguousarray(a[1]), mm, n)
+        pj_a.append(np.pad(a[0], (0, 5 - n)))
+        pj_b.append(np.pad(a[1], (0, 5 - n)))
+        pj_m.append(np.pad(m, (0, 5 - n)))
+        pj_out.append(np.pad(mm, (0, 5 - n)))
+    out.update(gs_n=np.array(gs_n, np.int32), gs_a=np.array(gs_a), gs_b=np.array(gs_b),
+               gs_d=np.array(gs_d), pj_a=np.array(pj_a), pj_b=np.array(pj_b), pj_m=np.array(pj_m),
+               pj_out=np.array(pj_out))
+
     np.savez_compressed(OUT, **out)
     print(f"wrote {OUT} ({OUT.stat().st_size} bytes)")
     return 0

@@ -22,6 +22,8 @@ REFERENCE_ENTRY_POINTS = [
     "_Z7LLE1DICddiddPKdiS0_PKiiddS0_i",
     "_Z5LLE2DddiddPKdiS0_PKiiddS0_i",
     "_Z7LLE2DICddiddPKdiS0_PKiiddS0_i",
+    "_Z4LS1DddiddPKdiS0_PKiiddS0_i",
+    "_Z4LS2DddiddPKdiS0_PKiiddS0_i",
 ]
 
 
@@ -204,3 +206,20 @@ def test_csv_open_failure_is_reported(cbf, tmp_path):
     st = cbf.lib().cbf_csv_write_map(str(bad).encode(), buf.ctypes.data_as(C.c_void_p), 0, 4, 2,
                                      None, 6)
     assert st == 6  # CBF_ERR_IO
+
+
+def test_csv_rows_layout(cbf, orc, tmp_path):
+    """LS1D rows "param, l1, ..., lN\\n" at the default ostream precision
+    (hostLibrary.cu:1900-1910)."""
+    nPts, cols = 6, 3
+    ranges = np.array([0.05, 0.40], np.float64)
+    vals = np.random.default_rng(2).normal(size=(nPts, cols)) * 10.0 ** np.arange(-3, 3).reshape(nPts, 1)
+    vals = np.ascontiguousarray(vals)
+    path = tmp_path / "r.csv"
+    assert cbf.lib().cbf_csv_write_rows(str(path).encode(), nPts, ranges.ctypes.data, vals.ctypes.data,
+                                        nPts, cols, 6) == 0
+    want = []
+    for k in range(nPts):
+        par = orc.lib().orc_get_value_by_idx(k, nPts, 0.05, 0.40, 0)
+        want.append("%.6g" % par + "".join(", %.6g" % v for v in vals[k]) + "\n")
+    assert path.read_text() == "".join(want)

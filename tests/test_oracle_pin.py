@@ -162,3 +162,50 @@ def test_regime_amplitude_rule_on_oracle(orc):
     _, raw = orc.map_lle_regime(off, stable + cycle)
     _, ruled = orc.map_lle_regime(on, stable + cycle)
     assert np.all((ruled == raw) | (ruled == 0))
+
+
+def test_gram_schmidt_matches_reference(G, orc):
+    """projectionOperator and gramSchmidtProcess of the Lyapunov-spectrum kernel,
+    bit for bit against the reference's own functions (zero and repeated rows
+    included)."""
+    L = orc.lib()
+    for k, n in enumerate(G["gs_n"]):
+        n = int(n)
+        a = np.ascontiguousarray(G["gs_a"][k][:n, :n])
+        b, d = orc.gram_schmidt(a)
+        assert np.array_equal(b.view(np.int64), np.ascontiguousarray(G["gs_b"][k][:n, :n]).view(np.int64)), k
+        assert np.array_equal(d.view(np.int64), np.ascontiguousarray(G["gs_d"][k][:n]).view(np.int64)), k
+        m = np.ascontiguousarray(G["pj_m"][k][:n]).copy()
+        L.orc_projection(np.ascontiguousarray(G["pj_a"][k][:n]), np.ascontiguousarray(G["pj_b"][k][:n]), m, n)
+        assert np.array_equal(m.view(np.int64), np.ascontiguousarray(G["pj_out"][k][:n]).view(np.int64)), k
+
+
+def test_gram_schmidt_live_against_reference(orc):
+    R = orc.ref()
+    if R is None or not hasattr(R, "ref_gramSchmidtProcess"):
+        pytest.skip("reference shim not built")
+    import ctypes as C
+    rng = np.random.default_rng(11)
+    for _ in range(200):
+        n = int(rng.integers(2, 6))
+        a = np.ascontiguousarray(rng.normal(size=(n, n)) * 10.0 ** float(rng.integers(-6, 3)))
+        want_b, want_d = np.zeros((n, n)), np.zeros(n)
+        R.ref_gramSchmidtProcess(a.copy(), want_b, n, want_d.ctypes.data_as(C.c_void_p))
+        b, d = orc.gram_schmidt(a)
+        assert np.array_equal(b, want_b) and np.array_equal(d, want_d)
+
+
+def test_lyapunov_spectrum_oracle_is_physical(orc):
+    """Lorenz (10, 28, 8/3): one positive, one ~zero exponent, and the sum close
+    to the trace of the Jacobian, -(sigma + 1 + beta), as for any flow."""
+    job = orc.make_job(system="lorenz", nPts=2, ranges=[28.0, 29.0], idxMut=[2], ic=[0.1, 0.1, 0.1],
+                       values=[0.5, 10.0, 28.0, 8.0 / 3.0], h=0.005, NT=0.5, tMax=200.0,
+                       transientTime=50.0, lleEps=1e-8, maxValue=0.0)
+    ls = orc.map_ls(job, [0])[0]
+    assert 0.75 < ls[0] < 1.1, ls
+    assert abs(ls[1]) < 0.05, ls
+    assert abs(ls.sum() + (10.0 + 1.0 + 8.0 / 3.0)) < 0.05, ls
+    assert ls[0] >= ls[1] >= ls[2]
+    # seeds: unit rows
+    z = orc.ls_seeds(job, [0, 5, 12345])
+    assert np.allclose(np.linalg.norm(z, axis=2), 1.0, atol=1e-15)
