@@ -1,18 +1,28 @@
 // C++ drop-in facade: the reference's hostLibrary entry points over the C-ABI.
 //
 // Output layout, precision and error behaviour follow Library/hostLibrary.cu
-// (lines cited per function).  Numbers are formatted with "%.*g" / "%d", which is
-// what std::ostream's default float field uses, so the bytes are identical to
-// the reference's `outFileStream << value` at the same precision.
+// (lines cited per function).  Numbers are formatted as "%.*g" / "%d" -- what
+// std::ostream's default float field uses, so the bytes are identical to the
+// reference's `outFileStream << value` at the same precision -- by
+// std::to_chars (general format with a precision is specified as printf's %.*g;
+// tests compare the bytes with printf-style formatting).  2-D maps are formatted
+// by several threads in blocks and written in order: the text of value i is
+// determined by i alone (", " before every value but the first, "\n" before
+// each new row), so the file is the same bytes as the serial rule produces.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <sched.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <atomic>
+#include <charconv>
 #include <mutex>
 #include <string>
+#include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/cbf.h"
@@ -113,17 +123,24 @@ public:
     {
         if (!f_) return;
         char tmp[64];
-        int n = snprintf(tmp, sizeof(tmp), "%.*g", prec_, v);
-        buf_.append(tmp, (size_t)n);
+        const auto r = std::to_chars(tmp, tmp + sizeof(tmp), v, std::chars_format::general, prec_);
+        buf_.append(tmp, (size_t)(r.ptr - tmp));
         maybe_flush();
     }
     void i32(int v)
     {
         if (!f_) return;
         char tmp[16];
-        int n = snprintf(tmp, sizeof(tmp), "%d", v);
-        buf_.append(tmp, (size_t)n);
+        const auto r = std::to_chars(tmp, tmp + sizeof(tmp), v);
+        buf_.append(tmp, (size_t)(r.ptr - tmp));
         maybe_flush();
+    }
+    int precision() const { return prec_; }
+    // The underlying file with everything buffered so far written out.
+    FILE* file()
+    {
+        if (f_) flush();
+        return f_;
     }
     void close()
     {
@@ -163,21 +180,85 @@ void write_header(CsvOut& out, const double* ranges)
     out.str("\n");
 }
 
-// Values in index order with the reference's row-break rule (hostLibrary.cu:534-546):
-// ", " before every value but the first, "\n" before the first of each new row.
-template <class T, class Put>
-void write_map(CsvOut& out, const T* v, long long n, int nPts, Put put)
+// Map values in index order with the reference's row-break rule
+// (hostLibrary.cu:534-546): ", " before every value but the first, "\n" before
+// the first of each new row -- so the text of value i depends on i alone.
+// Values [i0, i1) of a map with their separators, appended to `out`.
+template <class T>
+void format_map_range(const T* v, long long i0, long long i1, int nPts, int prec, std::string& out)
 {
-    int stringCounter = 0;
-    for (long long i = 0; i < n; ++i) {
-        if (stringCounter != 0) out.str(", ");
-        if (stringCounter == nPts) {
-            out.str("\n");
-            stringCounter = 0;
+    char tmp[64];
+    for (long long i = i0; i < i1; ++i) {
+        if (i > 0) {
+            out.append(", ", 2);
+            if (i % nPts == 0) out.push_back('\n');
         }
-        put(out, v[i]);
-        ++stringCounter;
+        std::to_chars_result r;
+        if constexpr (std::is_same<T, double>::value)
+            r = std::to_chars(tmp, tmp + sizeof(tmp), v[i], std::chars_format::general, prec);
+        else
+            r = std::to_chars(tmp, tmp + sizeof(tmp), v[i]);
+        out.append(tmp, (size_t)(r.ptr - tmp));
     }
+}
+
+// Threads for the map formatter: CBF_CSV_THREADS if > 0, else the CPUs this
+// process may run on (<= 64).
+int csv_threads()
+{
+    const char* e = getenv("CBF_CSV_THREADS");
+    int t = (e && *e) ? atoi(e) : 0;
+    if (t <= 0) {
+        cpu_set_t set;
+        CPU_ZERO(&set);
+        t = sched_getaffinity(0, sizeof(set), &set) == 0 ? CPU_COUNT(&set)
+                                                          : (int)std::thread::hardware_concurrency();
+    }
+    return std::max(1, std::min(t, 64));
+}
+
+// The whole map after the header: rounds of `threads` blocks of kBlock values,
+// each block formatted by its own thread; the previous round's text is written
+// (in index order) by one more thread while the next round is formatted.
+template <class T>
+void write_map_parallel(CsvOut& out, const T* v, long long n, int nPts)
+{
+    FILE* f = out.file();
+    if (!f || n <= 0) return;
+    constexpr long long kBlock = 1 << 18;
+    const int threads = csv_threads();
+    const int prec = out.precision();
+    if (threads == 1 || n <= kBlock) {
+        std::string buf;
+        for (long long i0 = 0; i0 < n; i0 += kBlock) {
+            buf.clear();
+            format_map_range(v, i0, std::min(n, i0 + kBlock), nPts, prec, buf);
+            fwrite(buf.data(), 1, buf.size(), f);
+        }
+        return;
+    }
+    std::vector<std::string> bufs[2] = {std::vector<std::string>((size_t)threads),
+                                        std::vector<std::string>((size_t)threads)};
+    std::thread writer;
+    int side = 0;
+    for (long long base = 0; base < n; base += kBlock * threads, side ^= 1) {
+        const int used = (int)std::min<long long>(threads, (n - base + kBlock - 1) / kBlock);
+        std::vector<std::string>& cur = bufs[side];
+        auto work = [&, base](int t) {
+            const long long i0 = base + (long long)t * kBlock;
+            cur[(size_t)t].clear();
+            format_map_range(v, i0, std::min(n, i0 + kBlock), nPts, prec, cur[(size_t)t]);
+        };
+        std::vector<std::thread> pool;
+        pool.reserve((size_t)used);
+        for (int t = 0; t < used; ++t) pool.emplace_back(work, t);
+        for (auto& th : pool) th.join();
+        if (writer.joinable()) writer.join();  // the previous round is on disk
+        writer = std::thread([f, &cur, used] {
+            for (int t = 0; t < used; ++t) fwrite(cur[(size_t)t].data(), 1, cur[(size_t)t].size(), f);
+        });
+    }
+    if (writer.joinable()) writer.join();
 }
 
 void bif1d_common(bool ic, double tMax, int nPts, double h, int nIC, const double* icv,
@@ -525,6 +606,30 @@ cbf_status open_or_fail(CsvOut& out, long long nValues)
 }
 }  // namespace
 
+// NumPy .npy (format 1.0): magic, version, little-endian header length, a
+// Python dict literal padded with spaces to a 64-byte boundary, then the data.
+extern "C" cbf_status cbf_npy_write(const char* path, const void* values, int32_t isDouble,
+                                    int64_t rows, int64_t cols)
+{
+    if (!path || rows < 0 || cols < 0 || (rows * cols > 0 && !values)) return CBF_ERR_INVALID_ARG;
+    char dict[160];
+    int len = snprintf(dict, sizeof(dict), "{'descr': '%s', 'fortran_order': False, 'shape': (%lld, %lld), }",
+                       isDouble ? "<f8" : "<i4", (long long)rows, (long long)cols);
+    std::string hdr(dict, (size_t)len);
+    const size_t pre = 10;  // magic (6) + version (2) + length (2)
+    while ((pre + hdr.size() + 1) % 64 != 0) hdr.push_back(' ');
+    hdr.push_back('\n');
+    FILE* f = fopen(path, "wb");
+    if (!f) return CBF_ERR_IO;
+    const unsigned char head[10] = {0x93, 'N', 'U', 'M', 'P', 'Y', 1, 0, (unsigned char)(hdr.size() & 0xff),
+                                    (unsigned char)(hdr.size() >> 8)};
+    const size_t bytes = (size_t)(rows * cols) * (isDouble ? sizeof(double) : sizeof(int32_t));
+    bool ok = fwrite(head, 1, 10, f) == 10 && fwrite(hdr.data(), 1, hdr.size(), f) == hdr.size() &&
+              (bytes == 0 || fwrite(values, 1, bytes, f) == bytes);
+    ok = (fclose(f) == 0) && ok;
+    return ok ? CBF_OK : CBF_ERR_IO;
+}
+
 extern "C" cbf_status cbf_csv_write_map(const char* path, const void* values, int32_t isDouble,
                                         int64_t n, int32_t nPts, const double* headerRanges,
                                         int32_t precision)
@@ -535,9 +640,17 @@ extern "C" cbf_status cbf_csv_write_map(const char* path, const void* values, in
     if (headerRanges) write_header(out, headerRanges);
     if (open_or_fail(out, n) != CBF_OK) return CBF_ERR_IO;
     if (isDouble)
-        write_map(out, (const double*)values, n, nPts, [](CsvOut& o, double v) { o.dbl(v); });
+        write_map_parallel(out, (const double*)values, n, nPts);
     else
-        write_map(out, (const int32_t*)values, n, nPts, [](CsvOut& o, int32_t v) { o.i32(v); });
+        write_map_parallel(out, (const int32_t*)values, n, nPts);
+    // optional binary copy of the map beside the CSV (rows of nPts values)
+    const char* side = getenv("CBF_NPY_SIDECAR");
+    if (side && *side && strcmp(side, "0") != 0) {
+        const std::string np = std::string(path) + ".npy";
+        const long long rows = (n + nPts - 1) / nPts;
+        if (rows * nPts == n) return cbf_npy_write(np.c_str(), values, isDouble, rows, nPts);
+        return cbf_npy_write(np.c_str(), values, isDouble, 1, n);
+    }
     return CBF_OK;
 }
 

@@ -361,6 +361,12 @@ cbf_status cbf_ls2d(int32_t system, double tMax, double NT, int32_t nPts, double
                     const double* ranges, const int32_t* indicesOfMutVars, int32_t writableVar,
                     double maxValue, double transientTime, const double* values,
                     int32_t amountOfValues, int64_t seedChunk, double* out);
+/* NumPy .npy file (format 1.0, little-endian float64 or int32, C order) of a
+ * rows x cols array.  No counterpart in the reference.  cbf_csv_write_map -- so
+ * every 2-D map the facade writes -- also writes <path>.npy when the environment
+ * variable CBF_NPY_SIDECAR is set to anything but "0". */
+cbf_status cbf_npy_write(const char* path, const void* values, int32_t isDouble, int64_t rows,
+                         int64_t cols);
 /* CSV rows "param, v1, v2, ...\n" (LS1D layout, hostLibrary.cu:1900-1910) for n
  * points with nCols values each (row-major). */
 cbf_status cbf_csv_write_rows(const char* path, int32_t nPts, const double* ranges,
@@ -395,7 +401,8 @@ cbf_status cbf_run_host(const cbf_job* job, void* out, void* aux);
 /* 2-D map (hostLibrary.cu:534-546): values in index order, ", " between values,
  * "\n" before the first value of each new row of nPts, no final newline.
  * headerRanges (4 doubles) adds the "r0 r1\nr2 r3\n" header (:476-480); NULL
- * omits it.  isDouble selects double (%.*g) or int32 (%d) values. */
+ * omits it.  isDouble selects double (%.*g) or int32 (%d) values.  Formatted by
+ * CBF_CSV_THREADS threads (default: the CPUs the process may use), same bytes. */
 cbf_status cbf_csv_write_map(const char* path, const void* values, int32_t isDouble, int64_t n,
                              int32_t nPts, const double* headerRanges, int32_t precision);
 /* 1-D diagram rows "param, peak\n" at precision 12 (hostLibrary.cu:125-138) for

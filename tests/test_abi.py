@@ -223,3 +223,41 @@ def test_csv_rows_layout(cbf, orc, tmp_path):
         par = orc.lib().orc_get_value_by_idx(k, nPts, 0.05, 0.40, 0)
         want.append("%.6g" % par + "".join(", %.6g" % v for v in vals[k]) + "\n")
     assert path.read_text() == "".join(want)
+
+
+@pytest.mark.parametrize("is_double", [True, False])
+def test_csv_map_parallel_formatter_is_byte_compatible(cbf, tmp_path, monkeypatch, is_double):
+    """The threaded map formatter (several rounds of 2^18-value blocks, a ragged
+    last block) writes the same bytes as the reference's serial ostream rule."""
+    nPts = 1100
+    rng = np.random.default_rng(5)
+    n = nPts * nPts
+    if is_double:
+        buf = np.ascontiguousarray(rng.normal(size=n) * 10.0 ** rng.integers(-9, 9, n), np.float64)
+        buf[::997] = 0.0
+    else:
+        buf = np.ascontiguousarray(rng.integers(-5, 16, n), np.int32)
+    hdr = np.array([30.0, 45.0, 20.0, 30.0], np.float64)
+    want = _ref_map_csv(buf.tolist(), nPts, list(hdr), 6, is_double)
+    for threads in ("3", "1"):
+        monkeypatch.setenv("CBF_CSV_THREADS", threads)
+        path = tmp_path / f"p{threads}.csv"
+        assert cbf.lib().cbf_csv_write_map(str(path).encode(), buf.ctypes.data_as(C.c_void_p),
+                                           int(is_double), n, nPts, hdr.ctypes.data_as(C.c_void_p), 6) == 0
+        assert path.read_bytes() == want
+
+
+def test_npy_sidecar_and_writer(cbf, tmp_path, monkeypatch):
+    L = cbf.lib()
+    L.cbf_npy_write.argtypes = [C.c_char_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int64]
+    a = np.ascontiguousarray(np.random.default_rng(1).normal(size=(7, 5)))
+    p = tmp_path / "a.npy"
+    assert L.cbf_npy_write(str(p).encode(), a.ctypes.data_as(C.c_void_p), 1, 7, 5) == 0
+    assert np.array_equal(np.load(p), a)
+    b = np.ascontiguousarray(np.arange(36, dtype=np.int32))
+    monkeypatch.setenv("CBF_NPY_SIDECAR", "1")
+    m = tmp_path / "m.csv"
+    assert L.cbf_csv_write_map(str(m).encode(), b.ctypes.data_as(C.c_void_p), 0, 36, 6, None, 6) == 0
+    got = np.load(str(m) + ".npy")
+    assert got.dtype == np.int32 and got.shape == (6, 6) and np.array_equal(got.ravel(), b)
+    assert m.read_bytes() == _ref_map_csv(b.tolist(), 6, None, 6, False)
