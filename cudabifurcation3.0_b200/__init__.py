@@ -26,6 +26,7 @@ LIB_PATH = PKG_DIR / "libcbf.so"
 SYS_MEMRISTIVE5, SYS_ROSSLER, SYS_LORENZ, SYS_CHEN = 0, 1, 2, 3
 SYSTEMS = {"memristive5": 0, "rossler": 1, "lorenz": 2, "chen": 3}
 TASK_PEAKS, TASK_KDE, TASK_DBSCAN, TASK_LLE, TASK_TRAJECTORY, TASK_LLE_REGIME, TASK_LS = 0, 1, 2, 3, 4, 5, 6
+TASK_OSTROVSKY = 7
 FLAG_EXACT_GRID, FLAG_KDE_FIXED = 1, 2
 STATUS = {0: "ok", 1: "invalid argument", 2: "unknown system", 3: "CUDA error",
           4: "out of device memory", 5: "no CUDA device", 6: "I/O error",
@@ -48,7 +49,7 @@ EXPORTS = [
     "cbf_mlp_num_params", "cbf_mlp_create", "cbf_mlp_destroy", "cbf_mlp_get_params",
     "cbf_mlp_set_params", "cbf_mlp_forward_backward", "cbf_mlp_train", "cbf_mlp_predict",
     "cbf_surrogate_config_init", "cbf_lle_map_surrogate", "cbf_ls1d", "cbf_ls2d",
-    "cbf_csv_write_rows", "cbf_npy_write",
+    "cbf_csv_write_rows", "cbf_npy_write", "cbf_ostrovsky2d",
 ]
 
 
@@ -96,6 +97,7 @@ class Job(C.Structure):
         ("pointIndex", C.c_void_p),
         ("regimeMinAmp", C.c_double),
         ("regimeChaosLle", C.c_double),
+        ("ostrovskyThreshold", C.c_double),
     ]
 
 
@@ -297,7 +299,7 @@ def make_job(*, task, system, nPts, ranges, idxMut, ic, values, h, tMax=0.0, tra
              maxValue=0.0, writableVar=0, preScaller=1, sweepIC=False, maxAmountOfPeaks=0,
              kdeSampling=0, kdeI1=0.0, kdeI2=0.0, kdeH=0.0, dbscanEps=0.0, NT=0.0, lleEps=0.0,
              seedChunk=0, firstPoint=0, nPoints=0, flags=0, peakCapacity=0, regimeTime=0.0,
-             pointIndex=0, regimeMinAmp=0.0, regimeChaosLle=0.0) -> Job:
+             pointIndex=0, regimeMinAmp=0.0, regimeChaosLle=0.0, ostrovskyThreshold=0.0) -> Job:
     j = Job()
     lib().cbf_job_init(C.byref(j))
     dims = len(idxMut)
@@ -322,6 +324,7 @@ def make_job(*, task, system, nPts, ranges, idxMut, ic, values, h, tMax=0.0, tra
     j.pointIndex = pointIndex or None
     j.regimeMinAmp = regimeMinAmp
     j.regimeChaosLle = regimeChaosLle
+    j.ostrovskyThreshold = ostrovskyThreshold
     return j
 
 
@@ -338,6 +341,8 @@ def run_host(job: Job):
         aux = np.zeros(n, np.int32)
     elif job.task == TASK_LS:
         out = np.zeros((n, job.nIC), np.float64)
+    elif job.task == TASK_OSTROVSKY:
+        out = np.zeros(n, np.float64)
     elif job.task in (TASK_KDE, TASK_DBSCAN):
         out = np.zeros(n, np.int32)
     else:
@@ -676,6 +681,27 @@ def _lle(fn, dims, system, tMax, NT, nPts, h, eps, icv, nIC, ranges, idx, wv, ma
     check(fn(_sys(system), tMax, NT, nPts, h, eps, icp, nIC, rp, ixp, wv, maxValue, transient, vp,
              nV, seedChunk, out.ctypes.data_as(_dp)))
     return out.reshape((nPts, nPts) if dims == 2 else (nPts,))
+
+
+def calculationOfPeriodicityByOstrovsky(tMax, nPts, h, amountOfInitialConditions, initialConditions,
+                                        ranges, indicesOfMutVars, writableVar, maxValue,
+                                        maxAmountOfPeaks, transientTime, values, amountOfValues,
+                                        preScaller, eps, ostrovskyThreshold, *, system="memristive5"):
+    """hostLibrary.cuh:211-227: the periodicity map, shape (nPts, nPts) (row = axis 1)."""
+    ic, icp = _d(initialConditions)
+    r, rp = _d(ranges)
+    ix, ixp = _i(indicesOfMutVars)
+    v, vp = _d(values)
+    out = np.zeros(nPts * nPts, np.float64)
+    L = lib()
+    L.cbf_ostrovsky2d.restype = C.c_int32
+    L.cbf_ostrovsky2d.argtypes = [C.c_int32, C.c_double, C.c_int32, C.c_double, C.c_int32, _dp, _dp, _ip,
+                                  C.c_int32, C.c_double, C.c_int32, C.c_double, _dp, C.c_int32,
+                                  C.c_int32, C.c_double, C.c_double, _dp]
+    check(L.cbf_ostrovsky2d(_sys(system), tMax, nPts, h, amountOfInitialConditions, icp, rp, ixp,
+                            writableVar, maxValue, maxAmountOfPeaks, transientTime, vp, amountOfValues,
+                            preScaller, eps, ostrovskyThreshold, out.ctypes.data_as(_dp)))
+    return out.reshape(nPts, nPts)
 
 
 def _ls(fn, dims, system, tMax, NT, nPts, h, eps, icv, nIC, ranges, idx, wv, maxValue, transient,

@@ -124,9 +124,11 @@ cbf_status cbf_batch_create(const cbf_job* jobs, int32_t nJobs, void* const* d_o
             return st;
         }
         const DevJob& d = b->jobs[i];
-        if (d.task == CBF_TASK_TRAJECTORY) {
+        if (d.task != CBF_TASK_PEAKS && d.task != CBF_TASK_KDE && d.task != CBF_TASK_DBSCAN &&
+            d.task != CBF_TASK_LLE) {
             delete b;
-            return report_error(CBF_ERR_INVALID_ARG, "trajectory jobs cannot be batched");
+            return report_error(CBF_ERR_INVALID_ARG,
+                                "only PEAKS, KDE, DBSCAN and LLE jobs can be batched");
         }
         if (d_auxs) b->auxs[i] = d_auxs[i];
         if (!b->outs[i] || (d.task == CBF_TASK_PEAKS && !b->auxs[i])) {

@@ -68,9 +68,11 @@ __global__ void __launch_bounds__(kBifThreads) bif_kernel(const DevJob J, void* 
 
         const long long slot0 = warpId * 32;
         double* myPk = scrPeaks + (slot0 + lane) * (long long)cap;
-        double* myIv = (TASK == CBF_TASK_DBSCAN) ? scrInt + (slot0 + lane) * (long long)cap : nullptr;
-        int n = 0;
-        if (valid) n = integrate_point<S, TASK>(J, g, myPk, myIv, cap, nullptr, nullptr);
+        double* myIv = task_with_intervals(TASK) ? scrInt + (slot0 + lane) * (long long)cap : nullptr;
+        int n = 0, div = 0;
+        OstrovskyFlags of;
+        of.init(J.ostThr);
+        if (valid) n = integrate_point<S, TASK>(J, g, myPk, myIv, cap, nullptr, &div, &of);
         __syncwarp();
 
         int res = 0;
@@ -87,7 +89,12 @@ __global__ void __launch_bounds__(kBifThreads) bif_kernel(const DevJob J, void* 
             }
             if (lane == j) res = r;
         }
-        if (valid) ((int*)d_out)[p] = res;
+        if (valid) {
+            if (TASK == CBF_TASK_OSTROVSKY)
+                ((double*)d_out)[p] = ostrovsky_value(n, div != 0, of, res);
+            else
+                ((int*)d_out)[p] = res;
+        }
         __syncwarp();
     }
 }
@@ -97,8 +104,8 @@ cudaError_t launch_bif_t(const DevJob& J, void* d_out, int* d_aux, cudaStream_t 
 {
     const long long nTiles = (J.nPoints + 31) / 32;
     if (nTiles == 0) return cudaSuccess;
-    const bool needScratch = (TASK == CBF_TASK_KDE || TASK == CBF_TASK_DBSCAN);
-    const int bitWords = (TASK == CBF_TASK_DBSCAN) ? (J.peakCap + 31) / 32 : 0;
+    const bool needScratch = (TASK == CBF_TASK_KDE || task_with_intervals(TASK));
+    const int bitWords = task_with_intervals(TASK) ? (J.peakCap + 31) / 32 : 0;
     const size_t smemBytes = (size_t)kBifWarps * 2 * bitWords * sizeof(unsigned);
 
     auto kern = bif_kernel<S, TASK>;
@@ -124,7 +131,7 @@ cudaError_t launch_bif_t(const DevJob& J, void* d_out, int* d_aux, cudaStream_t 
     if (needScratch) {
         // Per-warp scratch: 32 points x cap peaks (x2 with intervals).  Bound it.
         const size_t perBlock = (size_t)kBifThreads * J.peakCap * sizeof(double) *
-                                (TASK == CBF_TASK_DBSCAN ? 2 : 1);
+                                (task_with_intervals(TASK) ? 2 : 1);
         size_t freeB = 0, totalB = 0;
         if ((e = cudaMemGetInfo(&freeB, &totalB)) != cudaSuccess) return e;
         size_t budget = freeB / 4;
@@ -135,7 +142,7 @@ cudaError_t launch_bif_t(const DevJob& J, void* d_out, int* d_aux, cudaStream_t 
         if (blocks > fit) blocks = fit;
         const size_t bytes = (size_t)blocks * perBlock;
         if ((e = cudaMallocAsync((void**)&scrPeaks, bytes + 256, s)) != cudaSuccess) return e;
-        if (TASK == CBF_TASK_DBSCAN) scrInt = scrPeaks + (size_t)blocks * kBifThreads * J.peakCap;
+        if (task_with_intervals(TASK)) scrInt = scrPeaks + (size_t)blocks * kBifThreads * J.peakCap;
         err = (int*)((char*)scrPeaks + bytes);
         if ((e = cudaMemsetAsync(err, 0, sizeof(int), s)) != cudaSuccess) return e;
     }
@@ -162,6 +169,7 @@ cudaError_t launch_bif_s(const DevJob& J, void* d_out, int* d_aux, cudaStream_t 
     case CBF_TASK_KDE: return launch_bif_t<S, CBF_TASK_KDE>(J, d_out, d_aux, s);
     case CBF_TASK_DBSCAN: return launch_bif_t<S, CBF_TASK_DBSCAN>(J, d_out, d_aux, s);
     case CBF_TASK_TRAJECTORY: return launch_bif_t<S, CBF_TASK_TRAJECTORY>(J, d_out, d_aux, s);
+    case CBF_TASK_OSTROVSKY: return launch_bif_t<S, CBF_TASK_OSTROVSKY>(J, d_out, d_aux, s);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -187,7 +195,7 @@ cudaError_t launch_bif_prealloc_t(const DevJob& J, void* d_out, double* scratch,
         return e;
     if (perSm < 1) return cudaErrorInvalidConfiguration;
     const size_t perBlock = (size_t)kBifThreads * J.peakCap * sizeof(double) *
-                            (TASK == CBF_TASK_DBSCAN ? 2 : 1);
+                            (task_with_intervals(TASK) ? 2 : 1);
     long long blocks = (nTiles + kBifWarps - 1) / kBifWarps;
     const long long resident = (long long)sms * perSm;
     if (blocks > resident) blocks = resident;

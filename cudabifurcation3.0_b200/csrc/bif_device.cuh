@@ -22,6 +22,66 @@ constexpr unsigned kFull = 0xffffffffu;
 // The first detected peak is dropped and intervals are (t[k+1]-t[k]) * 0.01
 // (:250-262).  NaN is absorbing for these systems, so the inner loop's
 // run-to-the-end case never yields a peak, as here.
+struct NoPeakHook {
+    __device__ __forceinline__ void operator()(double, int) const {}
+};
+
+// Flags of peakFinderCUDAForCalculationOfPeriodicityByOstrovsky
+// (cudaLibrary.cu:288-352) kept while the peaks stream by, over every peak:
+// non-increasing consecutive peaks (flag 0), peaks from the second on above /
+// not above the threshold (flags 1, 2), and the last recorded sample (flag 4).
+struct OstrovskyFlags {
+    double prev, last, thr;
+    bool nonInc, one, zero;
+    __device__ __forceinline__ void init(double threshold)
+    {
+        thr = threshold;
+        prev = last = 0.0;
+        nonInc = true;
+        one = zero = false;
+    }
+    __device__ __forceinline__ void operator()(double val, int k)
+    {
+        if (k >= 1) {
+            if (val - prev > 0) nonInc = false;
+            if (val > thr) one = true;
+            else zero = true;
+        }
+        prev = val;
+    }
+};
+
+// dbscanCUDAForCalculationOfPeriodicityByOstrovsky (cudaLibrary.cu:628-662):
+// the cluster count (dbscanDouble = dbscan as a double) rewritten by the flags.
+// A diverged point has flag 3 only: the reference never writes its other flags,
+// which are false on zero-filled memory.
+__device__ __forceinline__ double ostrovsky_value(int n, bool div, const OstrovskyFlags& f, int clusters)
+{
+    bool f0, f1, f2, f3, f4;
+    if (div) {
+        f0 = f1 = f2 = f4 = false;
+        f3 = true;
+    } else {
+        f0 = f.nonInc;
+        f1 = f.one && f.zero;
+        f2 = !(f.one && !f.zero);
+        f3 = (n == 0 || n == 1);
+        f4 = f.last > f.thr;
+    }
+    double out = (double)clusters;
+    if (f2) out = -1 * out;
+    if (f3) out = f4 ? 1 : -1;
+    if (f1) out = 0;
+    if (f0) out = out > 0 ? 0.5 : (out == 0 ? 0 : -0.5);
+    return out;
+}
+
+// Tasks whose peaks carry intervals (DBSCAN on (peak, interval) pairs).
+__host__ __device__ constexpr bool task_with_intervals(int task)
+{
+    return task == CBF_TASK_DBSCAN || task == CBF_TASK_OSTROVSKY;
+}
+
 struct PeakStream {
     double prev1, prev2, pval;
     int mode;       // 0 NORMAL, 1 PLATEAU, 2 SKIP
@@ -36,11 +96,13 @@ struct PeakStream {
         lastT = 0;
     }
 
-    template <bool WITH_INTERVALS>
-    __device__ __forceinline__ void emit(double val, int t, double* pk, double* iv, int cap)
+    // hook(value, k) sees every emitted peak k = 0, 1, ... (also past cap).
+    template <bool WITH_INTERVALS, class Hook>
+    __device__ __forceinline__ void emit(double val, int t, double* pk, double* iv, int cap, Hook& hook)
     {
         if (detected >= 1) {
             const int k = detected - 1;
+            hook(val, k);
             if (k < cap) {
                 pk[k] = val;
                 if (WITH_INTERVALS) iv[k] = (double)(t - lastT) * kPeakIntervalUnit;
@@ -53,6 +115,13 @@ struct PeakStream {
     template <bool WITH_INTERVALS>
     __device__ __forceinline__ void push(double v, int t, double* pk, double* iv, int cap)
     {
+        NoPeakHook h;
+        push<WITH_INTERVALS>(v, t, pk, iv, cap, h);
+    }
+
+    template <bool WITH_INTERVALS, class Hook>
+    __device__ __forceinline__ void push(double v, int t, double* pk, double* iv, int cap, Hook& hook)
+    {
         if (t >= 2) {
             if (mode == 2) {
                 mode = 0;
@@ -60,12 +129,12 @@ struct PeakStream {
                 if (pval < v) {
                     mode = 2;
                 } else if (pval > v) {
-                    emit<WITH_INTERVALS>(pval, t - 1, pk, iv, cap);
+                    emit<WITH_INTERVALS>(pval, t - 1, pk, iv, cap, hook);
                     mode = 2;
                 }
             } else if (prev1 > prev2 && prev1 >= v) {
                 if (prev1 > v) {
-                    emit<WITH_INTERVALS>(prev1, t - 1, pk, iv, cap);
+                    emit<WITH_INTERVALS>(prev1, t - 1, pk, iv, cap, hook);
                     mode = 2;
                 } else {
                     mode = 1;
@@ -95,7 +164,7 @@ __device__ __forceinline__ double pick(const double (&x)[D], int wv)
 // divergence (peakFinderCUDA turns the -1 flag into 0, :277-281).
 template <class S, int TASK>
 __device__ int integrate_point(const DevJob& J, long long g, double* pk, double* iv, int cap,
-                               double* traj, int* divFlag)
+                               double* traj, int* divFlag, OstrovskyFlags* of = nullptr)
 {
     constexpr int D = S::DIM;
     double x[D], v[CBF_MAX_VALUES];
@@ -112,10 +181,14 @@ __device__ int integrate_point(const DevJob& J, long long g, double* pk, double*
     int t = 0;
     for (; t < J.nRecord; ++t) {
         const double val = pick<D>(x, wv);
-        if (TASK == CBF_TASK_TRAJECTORY)
+        if (TASK == CBF_TASK_TRAJECTORY) {
             traj[t] = val;
-        else
-            ps.push<TASK == CBF_TASK_DBSCAN>(val, t, pk, iv, cap);
+        } else if (TASK == CBF_TASK_OSTROVSKY) {
+            of->last = val;
+            ps.push<true>(val, t, pk, iv, cap, *of);
+        } else {
+            ps.push<task_with_intervals(TASK)>(val, t, pk, iv, cap);
+        }
         for (int j = 0; j < J.preScaller - 1; ++j) S::step(x, c);
         S::step(x, c);
         if (J.checkDiv && diverged(pick<D>(x, wv), J.divThresh)) {
@@ -124,6 +197,7 @@ __device__ int integrate_point(const DevJob& J, long long g, double* pk, double*
             break;
         }
     }
+    if (TASK == CBF_TASK_OSTROVSKY) *divFlag = div ? 1 : 0;
     if (TASK == CBF_TASK_TRAJECTORY) {
         // Samples after a divergence are never written by the reference; make them NaN.
         for (; t < J.nRecord; ++t) traj[t] = __longlong_as_double(0x7ff8000000000000ll);

@@ -158,7 +158,7 @@ cbf_status lower_job(const cbf_job* j, DevJob* d)
     memset(d, 0, sizeof(*d));
     const int dim = system_dim(j->system);
     if (dim < 0) return fail(CBF_ERR_UNKNOWN_SYSTEM, "unknown system id %d", j->system);
-    if (j->task < CBF_TASK_PEAKS || j->task > CBF_TASK_LS)
+    if (j->task < CBF_TASK_PEAKS || j->task > CBF_TASK_OSTROVSKY)
         return fail(CBF_ERR_INVALID_ARG, "unknown task %d", j->task);
     if (j->dims != 1 && j->dims != 2) return fail(CBF_ERR_INVALID_ARG, "dims must be 1 or 2 (got %d)", j->dims);
     if (j->nPts < 1) return fail(CBF_ERR_INVALID_ARG, "nPts must be >= 1 (got %d)", j->nPts);
@@ -279,7 +279,8 @@ cbf_status lower_job(const cbf_job* j, DevJob* d)
             d->kdeH = j->kdeH;
             d->kdeSkip = 16.0 * fabs(j->kdeH);
         }
-        if (j->task == CBF_TASK_DBSCAN) {
+        if (j->task == CBF_TASK_OSTROVSKY) d->ostThr = j->ostrovskyThreshold;
+        if (j->task == CBF_TASK_DBSCAN || j->task == CBF_TASK_OSTROVSKY) {
             const double e = j->dbscanEps;
             d->dbEps = e;
             if (!(e > 0)) d->dbSkip = 0.0;                        // nothing is ever a neighbour
@@ -296,6 +297,7 @@ size_t out_bytes(const DevJob& d)
     case CBF_TASK_LLE:
     case CBF_TASK_LLE_REGIME: return (size_t)d.nPoints * sizeof(double);
     case CBF_TASK_LS: return (size_t)d.nPoints * (size_t)d.nIC * sizeof(double);
+    case CBF_TASK_OSTROVSKY: return (size_t)d.nPoints * sizeof(double);
     case CBF_TASK_KDE:
     case CBF_TASK_DBSCAN: return (size_t)d.nPoints * sizeof(int);
     default: return (size_t)d.nPoints * (size_t)d.peakCap * sizeof(double);
@@ -427,6 +429,25 @@ cbf_status map2d(bool ic_sweep, int task, int32_t system, double tMax, int32_t n
     j.kdeI2 = i2;
     j.kdeH = smooth;
     j.dbscanEps = eps;
+    return run_host_impl(&j, out, nullptr);
+}
+
+cbf_status ostrovsky(int32_t system, double tMax, int32_t nPts, double h, int32_t nIC, const double* ic,
+                     const double* ranges, const int32_t* idxMut, int32_t wv, double maxValue,
+                     int32_t maxPeaks, double transientTime, const double* values, int32_t nV,
+                     int32_t preScaller, double eps, double threshold, double* out)
+{
+    cbf_status st = check_ptrs(nIC, ic, ranges, idxMut, values, nV);
+    if (st != CBF_OK) return st;
+    cbf_job j;
+    fill_common(&j, system, 2, nPts, h, nIC, ic, ranges, idxMut, wv, maxValue, transientTime, values, nV);
+    j.task = CBF_TASK_OSTROVSKY;
+    j.sweepIC = 1;  // the reference integrates with calculateDiscreteModelICCUDA (hostLibrary.cu:843)
+    j.tMax = tMax;
+    j.preScaller = preScaller;
+    j.maxAmountOfPeaks = maxPeaks;
+    j.dbscanEps = eps;
+    j.ostrovskyThreshold = threshold;
     return run_host_impl(&j, out, nullptr);
 }
 
@@ -676,6 +697,16 @@ cbf_status cbf_lle2d_ic(int32_t system, double tMax, double NT, int32_t nPts, do
 {
     return lle(true, 2, system, tMax, NT, nPts, h, eps, ic, nIC, ranges, idxMut, wv, maxValue,
                transientTime, values, nV, seedChunk, out);
+}
+
+cbf_status cbf_ostrovsky2d(int32_t system, double tMax, int32_t nPts, double h, int32_t nIC,
+                           const double* ic, const double* ranges, const int32_t* idxMut, int32_t wv,
+                           double maxValue, int32_t maxPeaks, double transientTime,
+                           const double* values, int32_t nV, int32_t preScaller, double eps,
+                           double ostrovskyThreshold, double* out)
+{
+    return ostrovsky(system, tMax, nPts, h, nIC, ic, ranges, idxMut, wv, maxValue, maxPeaks, transientTime,
+                     values, nV, preScaller, eps, ostrovskyThreshold, out);
 }
 
 cbf_status cbf_ls1d(int32_t system, double tMax, double NT, int32_t nPts, double h, double eps,

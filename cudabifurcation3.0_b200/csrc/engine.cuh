@@ -32,6 +32,7 @@ struct DevJob {
     int regimeSteps;    // LLE_REGIME: recorded steps after the transient
     double regimeMinAmp;  // LLE_REGIME: window range below this -> class 0
     double regimeChaosLle;  // LLE_REGIME: > 0 and LLE above it -> class 15
+    double ostThr;      // OSTROVSKY: periodicity threshold
     int nPts, dims, nIC, nV;
     int idxMut0, idxMut1;
     int writableVar, preScaller;

@@ -551,6 +551,24 @@ void LLE2DIC(const double tMax, const double NT, const int nPts, const double h,
                indicesOfMutVars, writableVar, maxValue, transientTime, values, amountOfValues);
 }
 
+// hostLibrary.cu:748-925: header and values at the default precision (:805-809, :887-902)
+void calculationOfPeriodicityByOstrovsky(const double tMax, const int nPts, const double h,
+                                         const int amountOfInitialConditions,
+                                         const double* initialConditions, const double* ranges,
+                                         const int* indicesOfMutVars, const int writableVar,
+                                         const double maxValue, const int maxAmountOfPeaks,
+                                         const double transientTime, const double* values,
+                                         const int amountOfValues, const int preScaller,
+                                         const double eps, const double ostrovskyThreshold)
+{
+    std::vector<double> res((size_t)nPts * (size_t)nPts);
+    CBF_CHECK(cbf_ostrovsky2d(current_system(), tMax, nPts, h, amountOfInitialConditions, initialConditions,
+                              ranges, indicesOfMutVars, writableVar, maxValue, maxAmountOfPeaks,
+                              transientTime, values, amountOfValues, preScaller, eps, ostrovskyThreshold,
+                              res.data()));
+    io_check(cbf_csv_write_map(current_path().c_str(), res.data(), 1, (int64_t)res.size(), nPts, ranges, 6));
+}
+
 // hostLibrary.cu:1802-1924
 void LS1D(const double tMax, const double NT, const int nPts, const double h, const double eps,
           const double* initialConditions, const int amountOfInitialConditions,

@@ -64,6 +64,9 @@ typedef int32_t cbf_status;
 
 #define CBF_TASK_LS 6           /* Lyapunov spectrum: nIC exponents per point (double[n*nIC],
                                    point-major), LSKernelCUDA semantics */
+#define CBF_TASK_OSTROVSKY 7    /* Ostrovsky periodicity value per point (double): the DBSCAN
+                                   count rewritten by the threshold flags (cudaLibrary.cu:288-352,
+                                   628-662); dbscanEps, maxAmountOfPeaks, ostrovskyThreshold */
 
 /* Job flags. */
 #define CBF_FLAG_EXACT_GRID 1u  /* integer grid index instead of the FP32 quirk */
@@ -114,6 +117,7 @@ typedef struct cbf_job {
     double regimeChaosLle;          /* LLE_REGIME: if > 0, points (with an oscillation)
                                        whose LLE exceeds it are class 15 (chaotic) without
                                        clustering their peaks */
+    double ostrovskyThreshold;      /* OSTROVSKY: threshold of the periodicity flags */
 } cbf_job;
 
 /* ---- library ---------------------------------------------------------- */
@@ -347,6 +351,14 @@ cbf_status cbf_lle2d_ic(int32_t system, double tMax, double NT, int32_t nPts, do
                         double transientTime, const double* values, int32_t amountOfValues,
                         int64_t seedChunk, double* out);
 
+/* Periodicity map by Ostrovsky's rule (calculationOfPeriodicityByOstrovsky,
+ * hostLibrary.cu:748-925): a 2-D sweep of initial conditions, out double[nPts^2]. */
+cbf_status cbf_ostrovsky2d(int32_t system, double tMax, int32_t nPts, double h,
+                           int32_t amountOfInitialConditions, const double* initialConditions,
+                           const double* ranges, const int32_t* indicesOfMutVars, int32_t writableVar,
+                           double maxValue, int32_t maxAmountOfPeaks, double transientTime,
+                           const double* values, int32_t amountOfValues, int32_t preScaller,
+                           double eps, double ostrovskyThreshold, double* out);
 /* Lyapunov spectra (hostLibrary.cu:1802-1924 LS1D, :1928-2082 LS2D): out
  * double[points * amountOfInitialConditions], the exponents of point k at
  * out[k*nIC .. k*nIC+nIC).  seedChunk: the chunk the reference's seed index is

@@ -97,6 +97,17 @@ void LLE2DIC(const double tMax, const double NT, const int nPts, const double h,
              const double maxValue, const double transientTime, const double* values,
              const int amountOfValues);
 
+// Periodicity map by Ostrovsky's rule (a 2-D sweep of initial conditions):
+// header + map at the default precision (hostLibrary.cu:748-925).
+void calculationOfPeriodicityByOstrovsky(const double tMax, const int nPts, const double h,
+                                         const int amountOfInitialConditions,
+                                         const double* initialConditions, const double* ranges,
+                                         const int* indicesOfMutVars, const int writableVar,
+                                         const double maxValue, const int maxAmountOfPeaks,
+                                         const double transientTime, const double* values,
+                                         const int amountOfValues, const int preScaller,
+                                         const double eps, const double ostrovskyThreshold);
+
 // Lyapunov spectra.  LS1D writes "param, l1, ..., lN" rows to the output path;
 // LS2D writes one map per exponent to <output path><k>.csv, k = 1..N, with the
 // 2-D map layout (hostLibrary.cu:1802-2082).

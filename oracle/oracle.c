@@ -686,6 +686,90 @@ int orc_map_dbscan(const orc_job* job, int64_t first, int64_t count, int32_t* ou
     return err;
 }
 
+/* calculationOfPeriodicityByOstrovsky (hostLibrary.cu:748-925) per point:
+ * peakFinderCUDAForCalculationOfPeriodicityByOstrovsky (cudaLibrary.cu:288-352)
+ * then dbscanCUDAForCalculationOfPeriodicityByOstrovsky (:628-662) with
+ * dbscanDouble (:533-605, dbscan's algorithm with a double result).  `data`,
+ * `intervals`, `helpful` hold rec doubles.  A point whose recorded loop
+ * diverged is -1: the reference sets only flag 3 for it and leaves the other
+ * four flags as the allocation left them -- false for zero-filled memory. */
+double orc_ostrovsky_point(const orc_job* job, int64_t g, double* data, double* intervals,
+                           double* helpful)
+{
+    const int rec = orc_record_len(job);
+    const double thr = job->ostrovskyThreshold;
+    int f[5] = {0, 0, 0, 0, 0};
+    int n = 0;
+    if (orc_trajectory_point(job, g, data)) {
+        f[3] = 1;
+    } else {
+        const double lastPoint = rec > 0 ? data[rec - 1] : 0.0;
+        n = orc_peak_finder(data, 0, rec, data, intervals, 0.01);
+        f[0] = 1;
+        for (int i = 1; i < n; ++i)
+            if (data[i] - data[i - 1] > 0) {
+                f[0] = 0;
+                break;
+            }
+        int one = 0, zero = 0;
+        for (int i = 1; i < n; ++i) {
+            if (data[i] > thr)
+                one = 1;
+            else
+                zero = 1;
+            if (one && zero)
+                break;
+        }
+        f[1] = one && zero;
+        f[2] = !(one && !zero);
+        f[3] = (n == 0 || n == 1);
+        f[4] = lastPoint > thr;
+    }
+    double out = (double)orc_dbscan(data, intervals, helpful, 0, n, rec, job->maxAmountOfPeaks,
+                                    job->dbscanEps);
+    if (f[2])
+        out = -1 * out;
+    if (f[3])
+        out = f[4] ? 1 : -1;
+    if (f[1])
+        out = 0;
+    if (f[0]) {
+        if (out > 0)
+            out = 0.5;
+        else if (out == 0)
+            out = 0;
+        else
+            out = -0.5;
+    }
+    return out;
+}
+
+int orc_map_ostrovsky(const orc_job* job, int64_t first, int64_t count, double* out, int nThreads)
+{
+    const int rec = orc_record_len(job);
+    if (rec <= 0)
+        return -1;
+    int err = 0;
+#pragma omp parallel num_threads(threads_or_default(nThreads))
+    {
+        double* data = (double*)malloc(sizeof(double) * (size_t)rec);
+        double* intervals = (double*)malloc(sizeof(double) * (size_t)rec);
+        double* helpful = (double*)malloc(sizeof(double) * (size_t)rec);
+        if (!data || !intervals || !helpful) {
+#pragma omp atomic write
+            err = -2;
+        } else {
+#pragma omp for schedule(dynamic, 1)
+            for (int64_t k = 0; k < count; ++k)
+                out[k] = orc_ostrovsky_point(job, first + k, data, intervals, helpful);
+        }
+        free(data);
+        free(intervals);
+        free(helpful);
+    }
+    return err;
+}
+
 int orc_map_lle(const orc_job* job, int64_t first, int64_t count, double* out, int nThreads)
 {
     if ((int)(job->tMax / job->NT) <= 0 || job->nIC <= 0)

@@ -64,6 +64,7 @@ typedef struct orc_job {
     double regimeTime;  /* LLE + regime: window after the transient (time units) */
     double regimeMinAmp; /* LLE + regime: window range below this -> class 0 */
     double regimeChaosLle; /* LLE + regime: > 0 and LLE above it -> class 15 */
+    double ostrovskyThreshold; /* periodicity classifier threshold */
 } orc_job;
 
 /* cudaLibrary.cu:210-216 */
@@ -133,6 +134,10 @@ int orc_map_lle_list(const orc_job* job, const int64_t* idx, int64_t count, doub
  * regimeChaosLle > 0 and the LLE exceeds it,
  * 15 if more than maxAmountOfPeaks peaks, else min(dbscan, 15). */
 double orc_lle_regime_point(const orc_job* job, int64_t g, const double* z, int32_t* cls);
+/* Ostrovsky periodicity classifier (cudaLibrary.cu:288-352, 628-662). */
+double orc_ostrovsky_point(const orc_job* job, int64_t g, double* data, double* intervals,
+                           double* helpful);
+int orc_map_ostrovsky(const orc_job* job, int64_t first, int64_t count, double* out, int nThreads);
 /* Lyapunov spectrum (LSKernelCUDA, cudaLibrary.cu:913-1100). */
 void orc_projection(const double* a, const double* b, double* minuend, int n);
 void orc_gram_schmidt(const double* a, double* b, int n, double* den);

@@ -51,6 +51,7 @@ class OrcJob(C.Structure):
         ("regimeTime", C.c_double),
         ("regimeMinAmp", C.c_double),
         ("regimeChaosLle", C.c_double),
+        ("ostrovskyThreshold", C.c_double),
     ]
 
 
@@ -58,7 +59,7 @@ def make_job(*, system, nPts, ranges, idxMut, ic, values, h, tMax=0.0, transient
              maxValue=0.0, writableVar=0, preScaller=1, sweepIC=False, maxAmountOfPeaks=0,
              kdeSampling=0, kdeI1=0.0, kdeI2=0.0, kdeH=0.0, dbscanEps=0.0, NT=0.0,
              lleEps=0.0, seedChunk=0, regimeTime=0.0, regimeMinAmp=0.0,
-             regimeChaosLle=0.0) -> OrcJob:
+             regimeChaosLle=0.0, ostrovskyThreshold=0.0) -> OrcJob:
     j = OrcJob()
     dims = len(idxMut)
     j.system = SYSTEMS[system] if isinstance(system, str) else int(system)
@@ -84,6 +85,7 @@ def make_job(*, system, nPts, ranges, idxMut, ic, values, h, tMax=0.0, transient
     j.regimeTime = regimeTime
     j.regimeMinAmp = regimeMinAmp
     j.regimeChaosLle = regimeChaosLle
+    j.ostrovskyThreshold = ostrovskyThreshold
     return j
 
 
@@ -156,6 +158,8 @@ def lib():
         L.orc_lle_seed.argtypes = [C.POINTER(OrcJob), C.c_int64, _dp]
         L.orc_map_lle_seeded.restype = C.c_int
         L.orc_map_lle_seeded.argtypes = [C.POINTER(OrcJob), C.c_int64, C.c_int64, _dp, _dp, C.c_int]
+        L.orc_map_ostrovsky.restype = C.c_int
+        L.orc_map_ostrovsky.argtypes = [C.POINTER(OrcJob), C.c_int64, C.c_int64, _dp, C.c_int]
         L.orc_map_ls_list.restype = C.c_int
         L.orc_map_ls_list.argtypes = [C.POINTER(OrcJob), _lp, C.c_int64, C.c_void_p, _dp, C.c_int]
         L.orc_ls_seed.restype = None
@@ -314,6 +318,15 @@ def lle_seeds(job: OrcJob, first: int, count: int):
     for k in range(count):
         lib().orc_lle_seed(C.byref(job), first + k, row)
         out[k] = row
+    return out
+
+
+def map_ostrovsky(job: OrcJob, first: int, count: int, threads: int = 0) -> np.ndarray:
+    """Ostrovsky periodicity values of points [first, first + count)."""
+    out = np.zeros(count, np.float64)
+    rc = lib().orc_map_ostrovsky(C.byref(job), first, count, out, threads)
+    if rc != 0:
+        raise RuntimeError(f"orc_map_ostrovsky failed: {rc}")
     return out
 
 

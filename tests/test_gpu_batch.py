@@ -117,3 +117,9 @@ def test_batch_rejects_bad_jobs(cbf, gpu_ok):
                        **SYS["chen"])
     with pytest.raises(cbf.CbfError):
         cbf.Batch([bad], [outs[0].data_ptr()])
+    # tasks the persistent kernel does not run are refused, not silently skipped
+    for task, extra in ((cbf.TASK_LS, dict(NT=0.5)), (cbf.TASK_LLE_REGIME, dict(NT=0.5, regimeTime=1.0)),
+                        (cbf.TASK_OSTROVSKY, dict(maxAmountOfPeaks=10)), (cbf.TASK_TRAJECTORY, {})):
+        job = cbf.make_job(task=task, system="chen", nPts=4, h=0.01, tMax=1.0, **extra, **SYS["chen"])
+        with pytest.raises(cbf.CbfError, match="batched"):
+            cbf.Batch([job], [outs[0].data_ptr()], [outs[0].data_ptr()])
