@@ -49,7 +49,7 @@ EXPORTS = [
     "cbf_mlp_num_params", "cbf_mlp_create", "cbf_mlp_destroy", "cbf_mlp_get_params",
     "cbf_mlp_set_params", "cbf_mlp_forward_backward", "cbf_mlp_train", "cbf_mlp_predict",
     "cbf_surrogate_config_init", "cbf_lle_map_surrogate", "cbf_ls1d", "cbf_ls2d",
-    "cbf_csv_write_rows", "cbf_npy_write", "cbf_ostrovsky2d",
+    "cbf_csv_write_rows", "cbf_npy_write", "cbf_ostrovsky2d", "cbf_modeling_one_system",
 ]
 
 
@@ -681,6 +681,22 @@ def _lle(fn, dims, system, tMax, NT, nPts, h, eps, icv, nIC, ranges, idx, wv, ma
     check(fn(_sys(system), tMax, NT, nPts, h, eps, icp, nIC, rp, ixp, wv, maxValue, transient, vp,
              nV, seedChunk, out.ctypes.data_as(_dp)))
     return out.reshape((nPts, nPts) if dims == 2 else (nPts,))
+
+
+def modelingOneSystemDenis(tMax, h, hSpecial, amountOfInitialConditions, initialConditions, writableVar,
+                           values, amountOfValues, *, system="memristive5"):
+    """hostLibrary.cuh:59-67: the step-offset series, (int)(tMax/h) samples."""
+    ic, icp = _d(initialConditions)
+    v, vp = _d(values)
+    n = int(tMax / h)
+    out = np.zeros(max(n, 0), np.float64)
+    L = lib()
+    L.cbf_modeling_one_system.restype = C.c_int32
+    L.cbf_modeling_one_system.argtypes = [C.c_int32, C.c_double, C.c_double, C.c_double, C.c_int32, _dp,
+                                          C.c_int32, _dp, C.c_int32, _dp, C.c_int64]
+    check(L.cbf_modeling_one_system(_sys(system), tMax, h, hSpecial, amountOfInitialConditions, icp,
+                                    writableVar, vp, amountOfValues, out.ctypes.data_as(_dp), len(out)))
+    return out
 
 
 def calculationOfPeriodicityByOstrovsky(tMax, nPts, h, amountOfInitialConditions, initialConditions,

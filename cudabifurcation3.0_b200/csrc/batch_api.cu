@@ -20,7 +20,6 @@ void batch_plan(const DevJob* jobs, void* const* outs, void* const* auxs, int n,
                 std::vector<unsigned char>& packed, std::vector<long long>& tileEnd,
                 std::vector<int>& order);
 cbf_status run_job_lowered(const DevJob& d, void* d_out, void* d_aux, cudaStream_t s);
-cbf_status library_stream_for_batch(cudaStream_t* s);
 
 }  // namespace cbf
 
@@ -214,7 +213,7 @@ cbf_status cbf_batch_capture(cbf_batch* b, void* stream)
     if (!b) return report_error(CBF_ERR_INVALID_ARG, "null batch");
     cudaStream_t s = (cudaStream_t)stream;
     if (!s) {
-        cbf_status st = library_stream_for_batch(&s);
+        cbf_status st = library_default_stream(&s);
         if (st != CBF_OK) return st;
     }
     release_graph(b);

@@ -493,7 +493,7 @@ cbf_status run_job_lowered(const DevJob& d, void* d_out, void* d_aux, cudaStream
 {
     return run_lowered(d, d_out, d_aux, s);
 }
-cbf_status library_stream_for_batch(cudaStream_t* s) { return library_stream(s); }
+cbf_status library_default_stream(cudaStream_t* s) { return library_stream(s); }
 cbf_status report_error(cbf_status st, const char* message) { return fail(st, "%s", message); }
 cbf_status report_cuda_error(cudaError_t e, const char* where) { return cuda_fail(e, where); }
 

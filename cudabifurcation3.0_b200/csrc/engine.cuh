@@ -194,6 +194,8 @@ cudaError_t launch_bif_prealloc(const DevJob& J, void* d_out, double* scratch, s
 
 // Job lowering and error reporting shared with other translation units (capi.cu).
 cbf_status lower_job_for(const cbf_job* job, DevJob* d);
+// The library's stream for calls given no stream (created once per device).
+cbf_status library_default_stream(cudaStream_t* s);
 cbf_status report_error(cbf_status st, const char* message);
 cbf_status report_cuda_error(cudaError_t e, const char* where);
 

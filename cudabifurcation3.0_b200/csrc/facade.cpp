@@ -551,6 +551,28 @@ void LLE2DIC(const double tMax, const double NT, const int nPts, const double h,
                indicesOfMutVars, writableVar, maxValue, transientTime, values, amountOfValues);
 }
 
+// hostLibrary.cu:162-239: "h*j, value" rows at precision 12 (:224-233)
+void modelingOneSystemDenis(const double tMax, const double h, const double hSpecial,
+                            const int amountOfInitialConditions, const double* initialConditions,
+                            const int writableVar, const double* values, const int amountOfValues)
+{
+    const double nd = (h != 0) ? tMax / h : 0.0;
+    const long long n = (nd > 0 && nd < 2147483648.0) ? (long long)(int)nd : 0;
+    std::vector<double> res((size_t)n);
+    CBF_CHECK(cbf_modeling_one_system(current_system(), tMax, h, hSpecial, amountOfInitialConditions,
+                                      initialConditions, writableVar, values, amountOfValues, res.data(),
+                                      n));
+    CsvOut out(current_path());
+    out.precision(12);
+    if (n > 0 && !out.is_open()) io_check(CBF_ERR_IO);
+    for (long long j = 0; j < n; ++j) {
+        out.dbl(h * (double)(size_t)j);
+        out.str(", ");
+        out.dbl(res[(size_t)j]);
+        out.str("\n");
+    }
+}
+
 // hostLibrary.cu:748-925: header and values at the default precision (:805-809, :887-902)
 void calculationOfPeriodicityByOstrovsky(const double tMax, const int nPts, const double h,
                                          const int amountOfInitialConditions,

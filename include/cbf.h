@@ -351,6 +351,14 @@ cbf_status cbf_lle2d_ic(int32_t system, double tMax, double NT, int32_t nPts, do
                         double transientTime, const double* values, int32_t amountOfValues,
                         int64_t seedChunk, double* out);
 
+/* One system sampled with a step offset (modelingOneSystemDenis,
+ * hostLibrary.cu:162-239): out[(int)(tMax/h)] (outLen at least that) holds the
+ * series x[writableVar] at times h*j, integrated with step hSpecial from T =
+ * (int)(hSpecial/h) starting offsets; entries no offset reaches are NaN. */
+cbf_status cbf_modeling_one_system(int32_t system, double tMax, double h, double hSpecial,
+                                   int32_t amountOfInitialConditions, const double* initialConditions,
+                                   int32_t writableVar, const double* values, int32_t amountOfValues,
+                                   double* out, int64_t outLen);
 /* Periodicity map by Ostrovsky's rule (calculationOfPeriodicityByOstrovsky,
  * hostLibrary.cu:748-925): a 2-D sweep of initial conditions, out double[nPts^2]. */
 cbf_status cbf_ostrovsky2d(int32_t system, double tMax, int32_t nPts, double h,

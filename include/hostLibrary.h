@@ -97,6 +97,12 @@ void LLE2DIC(const double tMax, const double NT, const int nPts, const double h,
              const double maxValue, const double transientTime, const double* values,
              const int amountOfValues);
 
+// One system sampled with a step offset: rows "h*j, x" at precision 12
+// (hostLibrary.cu:162-239).
+void modelingOneSystemDenis(const double tMax, const double h, const double hSpecial,
+                            const int amountOfInitialConditions, const double* initialConditions,
+                            const int writableVar, const double* values, const int amountOfValues);
+
 // Periodicity map by Ostrovsky's rule (a 2-D sweep of initial conditions):
 // header + map at the default precision (hostLibrary.cu:748-925).
 void calculationOfPeriodicityByOstrovsky(const double tMax, const int nPts, const double h,

@@ -770,6 +770,38 @@ int orc_map_ostrovsky(const orc_job* job, int64_t first, int64_t count, double* 
     return err;
 }
 
+/* modelingOneSystemDenis (hostLibrary.cu:162-239) with calculateDiscreteModelDenisCUDA
+ * (cudaLibrary.cu:121-161): thread idx < T = (int)(hSpecial/h) runs idx steps of h
+ * from the initial conditions, then records x[writableVar] before each of
+ * (int)(tMax/hSpecial) steps of hSpecial into out[idx + i*T].  out has
+ * (int)(tMax/h) entries; writes past it are dropped and entries no thread
+ * writes are NaN (the reference leaves them uninitialised).  No divergence test. */
+int orc_modeling_one_system(int system, double tMax, double h, double hSpecial, const double* ic, int nIC,
+                            int writableVar, const double* values, int nV, double* out, int64_t n)
+{
+    const int T = (int)(hSpecial / h);
+    const int I = (int)(tMax / hSpecial);
+    if (nIC <= 0 || nIC > 8 || nV <= 0 || nV > 16)
+        return -1;
+    for (int64_t j = 0; j < n; ++j)
+        out[j] = NAN;
+    for (int idx = 0; idx < T; ++idx) {
+        double x[8], v[16];
+        for (int i = 0; i < nIC; ++i)
+            x[i] = ic[i];
+        for (int i = 0; i < nV; ++i)
+            v[i] = values[i];
+        orc_loop(system, x, v, h, idx, 1, 0, 0, NULL, 0, 1);
+        for (int i = 0; i < I; ++i) {
+            const int64_t j = (int64_t)idx + (int64_t)i * T;
+            if (j < n)
+                out[j] = x[writableVar];
+            orc_loop(system, x, v, hSpecial, 1, 1, 0, 0, NULL, 0, 1);
+        }
+    }
+    return 0;
+}
+
 int orc_map_lle(const orc_job* job, int64_t first, int64_t count, double* out, int nThreads)
 {
     if ((int)(job->tMax / job->NT) <= 0 || job->nIC <= 0)

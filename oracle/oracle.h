@@ -134,6 +134,9 @@ int orc_map_lle_list(const orc_job* job, const int64_t* idx, int64_t count, doub
  * regimeChaosLle > 0 and the LLE exceeds it,
  * 15 if more than maxAmountOfPeaks peaks, else min(dbscan, 15). */
 double orc_lle_regime_point(const orc_job* job, int64_t g, const double* z, int32_t* cls);
+/* modelingOneSystemDenis: one system, step-offset sampling (cudaLibrary.cu:121-161). */
+int orc_modeling_one_system(int system, double tMax, double h, double hSpecial, const double* ic, int nIC,
+                            int writableVar, const double* values, int nV, double* out, int64_t n);
 /* Ostrovsky periodicity classifier (cudaLibrary.cu:288-352, 628-662). */
 double orc_ostrovsky_point(const orc_job* job, int64_t g, double* data, double* intervals,
                            double* helpful);

@@ -158,6 +158,9 @@ def lib():
         L.orc_lle_seed.argtypes = [C.POINTER(OrcJob), C.c_int64, _dp]
         L.orc_map_lle_seeded.restype = C.c_int
         L.orc_map_lle_seeded.argtypes = [C.POINTER(OrcJob), C.c_int64, C.c_int64, _dp, _dp, C.c_int]
+        L.orc_modeling_one_system.restype = C.c_int
+        L.orc_modeling_one_system.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, _dp, C.c_int,
+                                              C.c_int, _dp, C.c_int, _dp, C.c_int64]
         L.orc_map_ostrovsky.restype = C.c_int
         L.orc_map_ostrovsky.argtypes = [C.POINTER(OrcJob), C.c_int64, C.c_int64, _dp, C.c_int]
         L.orc_map_ls_list.restype = C.c_int
@@ -318,6 +321,20 @@ def lle_seeds(job: OrcJob, first: int, count: int):
     for k in range(count):
         lib().orc_lle_seed(C.byref(job), first + k, row)
         out[k] = row
+    return out
+
+
+def modeling_one_system(system, tMax, h, hSpecial, ic, writableVar, values) -> np.ndarray:
+    """The step-offset trajectory of modelingOneSystemDenis ((int)(tMax/h) samples)."""
+    sysid = SYSTEMS[system] if isinstance(system, str) else int(system)
+    ic = np.ascontiguousarray(ic, np.float64)
+    values = np.ascontiguousarray(values, np.float64)
+    n = int(tMax / h)
+    out = np.zeros(max(n, 0), np.float64)
+    rc = lib().orc_modeling_one_system(sysid, tMax, h, hSpecial, ic, len(ic), writableVar, values,
+                                       len(values), out, n)
+    if rc != 0:
+        raise RuntimeError(f"orc_modeling_one_system failed: {rc}")
     return out
 
 

@@ -23,6 +23,7 @@ REFERENCE_ENTRY_POINTS = [
     "_Z5LLE2DddiddPKdiS0_PKiiddS0_i",
     "_Z7LLE2DICddiddPKdiS0_PKiiddS0_i",
     "_Z35calculationOfPeriodicityByOstrovskydidiPKdS0_PKiididS0_iidd",
+    "_Z22modelingOneSystemDenisdddiPKdiS0_i",
     "_Z4LS1DddiddPKdiS0_PKiiddS0_i",
     "_Z4LS2DddiddPKdiS0_PKiiddS0_i",
 ]
@@ -65,7 +66,8 @@ def test_facade_names_match_reference_header_when_available():
     text = ref.read_text()
     for name in ("bifurcation1D", "bifurcation1DIC", "bifurcation2DKDE", "bifurcation2DKDEIC",
                  "bifurcation2DDBSCAN", "bifurcation2DDBSCANIC", "LLE1D", "LLE1DIC", "LLE2D",
-                 "LLE2DIC", "calculationOfPeriodicityByOstrovsky", "LS1D", "LS2D"):
+                 "LLE2DIC", "calculationOfPeriodicityByOstrovsky", "LS1D", "LS2D",
+                 "modelingOneSystemDenis"):
         assert re.search(r"__host__ void " + name + r"\(", text), name
 
 
