@@ -48,7 +48,7 @@ EXPORTS = [
     "cbf_csv_write_map", "cbf_csv_write_peaks", "cbf_csv_write_pairs",
     "cbf_mlp_num_params", "cbf_mlp_create", "cbf_mlp_destroy", "cbf_mlp_get_params",
     "cbf_mlp_set_params", "cbf_mlp_forward_backward", "cbf_mlp_train", "cbf_mlp_predict",
-    "cbf_surrogate_config_init", "cbf_lle_map_surrogate", "cbf_ls1d", "cbf_ls2d",
+    "cbf_surrogate_config_init", "cbf_lle_map_surrogate", "cbf_surrogate_release", "cbf_ls1d", "cbf_ls2d",
     "cbf_csv_write_rows", "cbf_npy_write", "cbf_ostrovsky2d", "cbf_modeling_one_system",
 ]
 

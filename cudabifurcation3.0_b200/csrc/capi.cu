@@ -84,8 +84,28 @@ std::mutex g_stream_mu;
 cudaStream_t g_streams[64];
 bool g_stream_made[64];
 
+// The library's scratch buffers come from the device's default stream-ordered
+// pool (cudaMallocAsync).  With the pool's default release threshold (0) every
+// synchronisation hands the memory back to the driver and the next call maps it
+// again -- tens of milliseconds for the ~0.6 GB peak scratch of a map launch.
+// Keep up to 16 GB cached between calls instead (set once per device).
+std::atomic<bool> g_pool_set[64];
+
+void keep_pool_memory()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || g_pool_set[dev].load()) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t threshold = 16ull << 30;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+    }
+    g_pool_set[dev].store(true);
+}
+
 cbf_status library_stream(cudaStream_t* s)
 {
+    keep_pool_memory();
     int dev = 0;
     CBF_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return fail(CBF_ERR_INVALID_ARG, "device %d out of range", dev);
@@ -315,6 +335,7 @@ cbf_status run_lowered(const DevJob& d, void* d_out, void* d_aux, cudaStream_t s
 {
     cudaError_t e;
     if (d.nPoints == 0) return CBF_OK;
+    keep_pool_memory();
     if (d.task == CBF_TASK_LLE)
         e = launch_lle(d, (double*)d_out, s);
     else if (d.task == CBF_TASK_LLE_REGIME)

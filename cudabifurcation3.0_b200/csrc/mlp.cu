@@ -528,6 +528,7 @@ struct Mlp {
     float gLr = 0.f;
     int gHorizon = 0;
     float gW = 0.f;
+    unsigned long long gSeed = 0;
     // inference workspace (rows per chunk = kPredRows), no pre-activations
     bf16 *pxb = nullptr, *ph1 = nullptr, *ph2 = nullptr, *ph3 = nullptr;
     float* pout = nullptr;
@@ -815,7 +816,7 @@ cbf_status cbf_mlp_train(cbf_mlp* m, const float* dX, const float* dYl, const in
     const int B = m->B;
     cudaError_t e = cudaSuccess;
     if (!m->exec || m->gX != dX || m->gN != N || m->gLr != lr || m->gHorizon != horizon ||
-        m->gW != wLle) {
+        m->gW != wLle || m->gSeed != m->seed) {
         if (m->exec) cudaGraphExecDestroy(m->exec);
         if (m->graph) cudaGraphDestroy(m->graph);
         m->exec = nullptr;
@@ -857,6 +858,7 @@ cbf_status cbf_mlp_train(cbf_mlp* m, const float* dX, const float* dYl, const in
         m->gLr = lr;
         m->gHorizon = horizon;
         m->gW = wLle;
+        m->gSeed = m->seed;
     }
     for (int i = 0; i < steps && e == cudaSuccess; ++i) {
         if (hLosses) e = cudaMemsetAsync(m->loss, 0, sizeof(float), s);
@@ -936,6 +938,18 @@ cudaError_t mlp_predict_grid(cbf_mlp* m, const FeatureSpec& f, long long nPoints
                 head_grid_kernel<<<b, t, 0, s>>>(m->pout, n, lleMean, lleStd, lle + r0, cls + r0, conf + r0);
             });
     }
+    return e;
+}
+
+cudaError_t mlp_reset(cbf_mlp* m, unsigned long long seed)
+{
+    std::vector<float> p;
+    init_params(p, seed);
+    m->seed = seed;
+    cudaError_t e = cudaMemset(m->m1, 0, kNumParams * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemset(m->m2, 0, kNumParams * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemset(m->step, 0, sizeof(unsigned long long));
+    if (e == cudaSuccess && upload_params(m, p.data()) != CBF_OK) e = cudaErrorUnknown;
     return e;
 }
 

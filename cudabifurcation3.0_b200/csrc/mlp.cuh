@@ -29,4 +29,9 @@ cudaError_t mlp_features(const FeatureSpec& f, const long long* idx, long long n
 cudaError_t mlp_predict_grid(cbf_mlp* m, const FeatureSpec& f, long long nPoints, float lleMean,
                              float lleStd, double* lle, int* cls, float* conf, cudaStream_t s);
 
+// Parameters re-initialised from `seed` exactly as cbf_mlp_create does, Adam
+// state and step counter zeroed (the captured training graph is kept unless the
+// seed changed).
+cudaError_t mlp_reset(cbf_mlp* m, unsigned long long seed);
+
 }  // namespace cbf

@@ -21,6 +21,7 @@
 #include <math.h>
 #include <string.h>
 
+#include <mutex>
 #include <vector>
 
 #include "mlp.cuh"
@@ -273,22 +274,55 @@ cudaError_t launch1d(long long n, cudaStream_t s, F f)
     return cudaGetLastError();
 }
 
-struct DeviceBuffers {
-    std::vector<void*> ptrs;
+// The pipeline's buffers, kept per device between calls and grown on demand,
+// together with the network (and so its captured training graph): a repeated
+// map allocates nothing.  cbf_surrogate_release frees them.
+enum Slot {
+    kSlotIdx, kSlotLabLle, kSlotLabCls, kSlotX, kSlotYl, kSlotConf, kSlotFlag, kSlotSrc, kSlotBlock,
+    kSlotOffsets, kSlotStats, kSlotLsur, kSlotRule, kSlotList, kSlotRl, kSlotRc, kSlotSur, kNumSlots
+};
+
+struct Workspace {
+    void* ptr[kNumSlots] = {};
+    size_t bytes[kNumSlots] = {};
+    cbf_mlp* net = nullptr;
+    int netBatch = 0;
+
     template <class T>
-    cudaError_t get(T** p, long long n)
+    cudaError_t get(int slot, T** p, long long n)
     {
-        void* q = nullptr;
-        cudaError_t e = cudaMalloc(&q, (size_t)(n > 0 ? n : 1) * sizeof(T));
-        if (e == cudaSuccess) ptrs.push_back(q);
-        *p = (T*)q;
-        return e;
+        const size_t need = (size_t)(n > 0 ? n : 1) * sizeof(T);
+        if (bytes[slot] < need) {
+            if (ptr[slot]) cudaFree(ptr[slot]);
+            ptr[slot] = nullptr;
+            bytes[slot] = 0;
+            cudaError_t e = cudaMalloc(&ptr[slot], need);
+            if (e != cudaSuccess) {
+                ptr[slot] = nullptr;
+                *p = nullptr;
+                return e;
+            }
+            bytes[slot] = need;
+        }
+        *p = (T*)ptr[slot];
+        return cudaSuccess;
     }
-    ~DeviceBuffers()
+    void release()
     {
-        for (void* p : ptrs) cudaFree(p);
+        for (int i = 0; i < kNumSlots; ++i) {
+            if (ptr[i]) cudaFree(ptr[i]);
+            ptr[i] = nullptr;
+            bytes[i] = 0;
+        }
+        if (net) cbf_mlp_destroy(net);
+        net = nullptr;
+        netBatch = 0;
     }
 };
+
+constexpr int kMaxDevices = 64;
+Workspace g_ws[kMaxDevices];
+std::mutex g_ws_mu[kMaxDevices];
 
 }  // namespace
 }  // namespace cbf
@@ -369,7 +403,11 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
         }
     } evGuard{ev};
 
-    DeviceBuffers buf;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+        return report_error(CBF_ERR_INVALID_ARG, "no usable current device");
+    std::lock_guard<std::mutex> wsLock(g_ws_mu[dev]);  // one map at a time per device
+    Workspace& buf = g_ws[dev];
     long long* dIdx = nullptr;
     double* labLle = nullptr;
     int* labCls = nullptr;
@@ -379,17 +417,17 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
     long long* offsets = nullptr;
     Stats* stats = nullptr;
     const int nb = (int)((n + kChunk - 1) / kChunk);
-    cudaError_t e = buf.get(&dIdx, nLab);
-    if (e == cudaSuccess) e = buf.get(&labLle, nLab);
-    if (e == cudaSuccess) e = buf.get(&labCls, nLab);
-    if (e == cudaSuccess) e = buf.get(&X, nLab * 4);
-    if (e == cudaSuccess) e = buf.get(&yl, nLab);
-    if (e == cudaSuccess && !conf) e = buf.get(&conf, n);
-    if (e == cudaSuccess) e = buf.get(&flag, n);
-    if (e == cudaSuccess && !src) e = buf.get(&src, n);
-    if (e == cudaSuccess) e = buf.get(&blockCount, nb);
-    if (e == cudaSuccess) e = buf.get(&offsets, (long long)nb + 1);
-    if (e == cudaSuccess) e = buf.get(&stats, 1);
+    cudaError_t e = buf.get(kSlotIdx, &dIdx, nLab);
+    if (e == cudaSuccess) e = buf.get(kSlotLabLle, &labLle, nLab);
+    if (e == cudaSuccess) e = buf.get(kSlotLabCls, &labCls, nLab);
+    if (e == cudaSuccess) e = buf.get(kSlotX, &X, nLab * 4);
+    if (e == cudaSuccess) e = buf.get(kSlotYl, &yl, nLab);
+    if (e == cudaSuccess && !conf) e = buf.get(kSlotConf, &conf, n);
+    if (e == cudaSuccess) e = buf.get(kSlotFlag, &flag, n);
+    if (e == cudaSuccess && !src) e = buf.get(kSlotSrc, &src, n);
+    if (e == cudaSuccess) e = buf.get(kSlotBlock, &blockCount, nb);
+    if (e == cudaSuccess) e = buf.get(kSlotOffsets, &offsets, (long long)nb + 1);
+    if (e == cudaSuccess) e = buf.get(kSlotStats, &stats, 1);
     if (e != cudaSuccess) return report_cuda_error(e, "surrogate map buffers");
 
     // 1. plain labels
@@ -433,12 +471,17 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
     cudaEventRecord(ev[1], s);
 
     // 2. training
-    cbf_mlp* net = nullptr;
-    if ((st = cbf_mlp_create(cfg->batch, cfg->seed, &net)) != CBF_OK) return st;
-    struct NetGuard {
-        cbf_mlp* m;
-        ~NetGuard() { cbf_mlp_destroy(m); }
-    } netGuard{net};
+    if (buf.net && buf.netBatch != cfg->batch) {
+        cbf_mlp_destroy(buf.net);
+        buf.net = nullptr;
+    }
+    if (!buf.net) {
+        if ((st = cbf_mlp_create(cfg->batch, cfg->seed, &buf.net)) != CBF_OK) return st;
+        buf.netBatch = cfg->batch;
+    } else if ((e = mlp_reset(buf.net, cfg->seed)) != cudaSuccess) {
+        return report_cuda_error(e, "network reset");
+    }
+    cbf_mlp* net = buf.net;
     const int tail = cfg->trainSteps < 100 ? cfg->trainSteps : 100;
     std::vector<float> losses(tail > 0 ? tail : 1, 0.f);
     st = cbf_mlp_train(net, X, yl, labCls, nLab, cfg->trainSteps - tail, cfg->lr, cfg->trainSteps, cfg->wLle,
@@ -465,7 +508,7 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
     const int autoR = (nPts + 4095) / 4096;
     const int er = cfg->refine ? (cfg->expandRadius < 0 ? autoR : cfg->expandRadius) : 0;
     unsigned char* lsur = nullptr;
-    if ((e = buf.get(&lsur, nLab)) != cudaSuccess) return report_cuda_error(e, "label buffers");
+    if ((e = buf.get(kSlotLsur, &lsur, nLab)) != cudaSuccess) return report_cuda_error(e, "label buffers");
     e = launch1d(n, s, [&](unsigned b, int t) {
         mask_kernel<<<b, t, 0, s>>>(dCls, conf, nPts, n, radius, thr, auditCut,
                                     cfg->seed ^ 0xA0761D6478BD642Full, flag, src);
@@ -505,7 +548,7 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
     if ((e = select(kBoundary | kLowConf | kAudit, nullptr, &n0)) != cudaSuccess)
         return report_cuda_error(e, "recompute list");
     long long* rule = nullptr;
-    if ((e = buf.get(&rule, n0)) != cudaSuccess) return report_cuda_error(e, "recompute list");
+    if ((e = buf.get(kSlotRule, &rule, n0)) != cudaSuccess) return report_cuda_error(e, "recompute list");
     if (n0 > 0 && (e = select(kBoundary | kLowConf | kAudit, rule, &n0)) != cudaSuccess)
         return report_cuda_error(e, "recompute list");
     long long resident = lle_regime_resident_points(dj);
@@ -515,7 +558,7 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
     double* rl = nullptr;
     int* rc = nullptr;
     unsigned char* sur = nullptr;
-    long long cap = 0, refined = 0, pos = 0;
+    long long refined = 0, pos = 0;
     int waves = 0;
     for (int w = 0;; ++w) {
         // the expansion marks of the previous rounds (counted first: sizes the chunk)
@@ -525,14 +568,11 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
         if (nB > n0 - pos) nB = n0 - pos;
         const long long nSel = nA + nB;
         if (nSel == 0) break;
-        if (nSel > cap) {
-            cap = nSel > 2 * cap ? nSel : 2 * cap;
-            e = buf.get(&list, cap);
-            if (e == cudaSuccess) e = buf.get(&rl, cap);
-            if (e == cudaSuccess) e = buf.get(&rc, cap);
-            if (e == cudaSuccess) e = buf.get(&sur, cap);
-            if (e != cudaSuccess) return report_cuda_error(e, "recompute buffers");
-        }
+        e = buf.get(kSlotList, &list, nSel);
+        if (e == cudaSuccess) e = buf.get(kSlotRl, &rl, nSel);
+        if (e == cudaSuccess) e = buf.get(kSlotRc, &rc, nSel);
+        if (e == cudaSuccess) e = buf.get(kSlotSur, &sur, nSel);
+        if (e != cudaSuccess) return report_cuda_error(e, "recompute buffers");
         if (nA > 0 && (e = select(kExpand, list, &nA)) != cudaSuccess) return report_cuda_error(e, "expansion list");
         if (nB > 0 && (e = cudaMemcpyAsync(list + nA, rule + pos, nB * sizeof(long long), cudaMemcpyDeviceToDevice,
                                            s)) != cudaSuccess)
@@ -595,6 +635,14 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
         rep->msTotal = tot;
     }
     return CBF_OK;
+}
+
+void cbf_surrogate_release(void)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return;
+    std::lock_guard<std::mutex> lk(g_ws_mu[dev]);
+    g_ws[dev].release();
 }
 
 }  // extern "C"

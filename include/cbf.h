@@ -270,6 +270,10 @@ typedef struct cbf_surrogate_report {
 cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config* cfg, double* dLle,
                                  int32_t* dCls, uint8_t* dSource, float* dConf, int32_t* dPred,
                                  cbf_surrogate_report* report, void* stream);
+/* cbf_lle_map_surrogate keeps its work buffers and the network on the device
+ * between calls (about 1 GB at 8192^2; calls on one device run one at a time);
+ * this frees them for the current device. */
+void cbf_surrogate_release(void);
 
 /* ---- host-buffer entry points (drop-in for hostLibrary.cuh) ---------- */
 /* bifurcation1D, hostLibrary.cuh:29-42 / hostLibrary.cu:7-158.

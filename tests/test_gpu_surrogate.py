@@ -148,9 +148,12 @@ def test_surrogate_is_deterministic_and_ablation_is_worse(cbf, gpu_ok):
     torch = pytest.importorskip("torch")
     side = 256
     a = _plain_and_surrogate(cbf, torch, side, SMALL_CFG, **SMALL)
-    b = _plain_and_surrogate(cbf, torch, side, SMALL_CFG, **SMALL)
-    assert np.array_equal(a[2], b[2], equal_nan=True) and np.array_equal(a[3], b[3])
-    assert np.array_equal(a[4], b[4])
+    b = _plain_and_surrogate(cbf, torch, side, SMALL_CFG, **SMALL)  # reuses the cached workspace
+    cbf.lib().cbf_surrogate_release()
+    c = _plain_and_surrogate(cbf, torch, side, SMALL_CFG, **SMALL)  # allocates afresh
+    for x in (b, c):
+        assert np.array_equal(a[2], x[2], equal_nan=True) and np.array_equal(a[3], x[3])
+        assert np.array_equal(a[4], x[4])
     # network alone (no recompute): only labels are plain, agreement drops
     pl, pc, sl, sc, src, rep = _plain_and_surrogate(cbf, torch, side, dict(SMALL_CFG, refine=0), **SMALL)
     assert rep.refined == 0 and rep.waves == 0 and set(np.unique(src)) <= {0, 1}
