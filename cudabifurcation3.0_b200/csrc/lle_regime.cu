@@ -45,39 +45,9 @@ __device__ double lle_regime_point(const DevJob& J, long long g, double* pk, dou
 #pragma unroll
         for (int i = 0; i < D; ++i) y[0][i] = z[i] * J.lleEps + x[0][i];
     }
-    PeakStream ps;
-    ps.init();
-    double lo = INFINITY, hi = -INFINITY;
-    bool regimeDiv = false;
-    int t = 0;  // step index since the transient
     double result = 0;
-    for (int b = 0; b < J.nRecord; ++b) {
-        if (t < J.regimeSteps) {
-            // Intervals overlapping the window run the exact per-step path.
-            bool ax = true, ay = true;
-            for (int i = 0; i < J.nNT; ++i, ++t) {
-                if (ax) {
-                    if (t < J.regimeSteps) {
-                        const double v = pick<D>(x[0], J.writableVar);
-                        lo = fmin(lo, v);
-                        hi = fmax(hi, v);
-                        ps.push<true>(v, t, pk, iv, cap);
-                    }
-                    S::step(x[0], c[0]);
-                    if (J.checkDiv && diverged(x[0][0], J.divThresh)) {
-                        ax = false;
-                        if (t < J.regimeSteps) regimeDiv = true;
-                    }
-                }
-                if (ay) {
-                    S::step(y[0], c[0]);
-                    if (J.checkDiv && diverged(y[0][0], J.divThresh)) ay = false;
-                }
-            }
-        } else {
-            run_pair<S, 1>(x, y, c, J.nNT, J);
-            t += J.nNT;
-        }
+    // Renormalisation (cudaLibrary.cu:757-776) after each interval.
+    auto renorm = [&]() {
         double tt = 0;
 #pragma unroll
         for (int l = 0; l < D; ++l) tt += (x[0][l] - y[0][l]) * (x[0][l] - y[0][l]);
@@ -86,9 +56,78 @@ __device__ double lle_regime_point(const DevJob& J, long long g, double* pk, dou
         if (tt != 0) tt = (1 / tt);
 #pragma unroll
         for (int i = 0; i < D; ++i) y[0][i] = x[0][i] - ((x[0][i] - y[0][i]) * tt);
+    };
+    int b = 0;
+    {
+        // The intervals that overlap the window, with the peak stream; its state
+        // is dead after this block, so the loop below is the LLE kernel's loop.
+        PeakStream ps;
+        ps.init();
+        double lo = INFINITY, hi = -INFINITY;
+        bool regimeDiv = false;
+        int t = 0;  // step index since the transient
+        for (; b < J.nRecord && t < J.regimeSteps; ++b) {
+            // Intervals overlapping the window: x and y advanced together, the
+            // peak stream fed before every x step, only the high words of |x0|,
+            // |y0| tracked.  If the divergence bound's high word was reached, the
+            // interval is replayed from its start (state, peak stream and window
+            // range restored) with the exact per-step test.
+            const int t0 = t;
+            double x0[D], y0[D];
+            copy_state<D>(x0, x[0]);
+            copy_state<D>(y0, y[0]);
+            const PeakStream ps0 = ps;
+            const double lo0 = lo, hi0 = hi;
+            unsigned mx = 0, my = 0;
+            for (int i = 0; i < J.nNT; ++i, ++t) {
+                if (t < J.regimeSteps) {
+                    const double v = pick<D>(x[0], J.writableVar);
+                    lo = fmin(lo, v);
+                    hi = fmax(hi, v);
+                    ps.push<true>(v, t, pk, iv, cap);
+                }
+                S::step(x[0], c[0]);
+                S::step(y[0], c[0]);
+                mx = max(mx, abs_hi(x[0][0]));
+                my = max(my, abs_hi(y[0][0]));
+            }
+            if (J.checkDiv && (mx >= J.divHi || my >= J.divHi)) {
+                copy_state<D>(x[0], x0);
+                copy_state<D>(y[0], y0);
+                ps = ps0;
+                lo = lo0;
+                hi = hi0;
+                t = t0;
+                bool ax = true, ay = true;
+                for (int i = 0; i < J.nNT; ++i, ++t) {
+                    if (ax) {
+                        if (t < J.regimeSteps) {
+                            const double v = pick<D>(x[0], J.writableVar);
+                            lo = fmin(lo, v);
+                            hi = fmax(hi, v);
+                            ps.push<true>(v, t, pk, iv, cap);
+                        }
+                        S::step(x[0], c[0]);
+                        if (J.checkDiv && diverged(x[0][0], J.divThresh)) {
+                            ax = false;
+                            if (t < J.regimeSteps) regimeDiv = true;
+                        }
+                    }
+                    if (ay) {
+                        S::step(y[0], c[0]);
+                        if (J.checkDiv && diverged(y[0][0], J.divThresh)) ay = false;
+                    }
+                }
+            }
+            renorm();
+        }
+        *nOut = regimeDiv ? -1 : ps.emitted();
+        *amp = hi - lo;
     }
-    *nOut = regimeDiv ? -1 : ps.emitted();
-    *amp = hi - lo;
+    for (; b < J.nRecord; ++b) {
+        run_pair<S, 1>(x, y, c, J.nNT, J);
+        renorm();
+    }
     return result / J.tMax;
 }
 
