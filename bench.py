@@ -211,13 +211,29 @@ def steps_per_point(w) -> int:
     return skip + 2 * blocks * nt
 
 
-def rank_workload(rank: int, world: int) -> dict:
-    w = dict(WORKLOAD)
+def stripe(w: dict, rank: int, world: int) -> dict:
+    """Weak scaling: rank r maps the r-th of `world` equal c-stripes (axis 1) at the
+    full resolution; the stripes tile the c range with no overlap or gap."""
+    w = dict(w)
     if world > 1:
         lo, hi = w["ranges"][2], w["ranges"][3]
         step = (hi - lo) / world
-        w["ranges"] = [w["ranges"][0], w["ranges"][1], lo + rank * step, lo + (rank + 1) * step]
+        top = hi if rank == world - 1 else lo + (rank + 1) * step
+        w["ranges"] = [w["ranges"][0], w["ranges"][1], lo + rank * step, top]
     return w
+
+
+def rank_workload(rank: int, world: int) -> dict:
+    return stripe(WORKLOAD, rank, world)
+
+
+def max_over_ranks(values, dist=None, device=None):
+    """Element-wise maximum of per-rank timings (all ranks take part)."""
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
 
 
 class ClockSampler:
@@ -520,11 +536,7 @@ def run_surrogate(args) -> int:
                                 device_id=torch.device("cuda", local))
     cbf = load_cbf()
     cbf.check(cbf.lib().cbf_set_device(local))
-    w = dict(SUR_WORKLOAD)
-    if world > 1:  # weak scaling: each rank maps its own c-stripe at full resolution
-        lo, hi = w["ranges"][2], w["ranges"][3]
-        step = (hi - lo) / world
-        w["ranges"] = [w["ranges"][0], w["ranges"][1], lo + rank * step, lo + (rank + 1) * step]
+    w = stripe(SUR_WORKLOAD, rank, world)
     if args.nPts:
         w["nPts"] = args.nPts
     n = w["nPts"] ** 2
@@ -594,10 +606,7 @@ def run_surrogate(args) -> int:
     launches = cbf.kernel_launches() - launches0
     clocks = sampler.stop()
     step_ms = [a.elapsed_time(b) for a, b in evs]
-    t = torch.tensor([sum(step_ms), plain_ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms, plain_max = float(t[0].item()), float(t[1].item())
+    total_ms, plain_max = max_over_ranks([sum(step_ms), plain_ms], dist, "cuda")
     value = world * n * args.steps / (total_ms / 1e3)
     plain_value = world * n / (plain_max / 1e3)
 

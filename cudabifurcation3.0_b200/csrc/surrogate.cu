@@ -341,7 +341,7 @@ void cbf_surrogate_config_init(cbf_surrogate_config* c)
     c->trainSteps = 2500;
     c->lr = 2e-3f;
     c->wLle = 1.0f;
-    c->confThreshold = 0.7f;
+    c->confThreshold = 0.5f;
     c->auditFraction = 0.01f;
     c->boundaryRadius = 1;
     c->refine = 1;

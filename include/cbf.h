@@ -231,7 +231,7 @@ typedef struct cbf_surrogate_config {
     int32_t trainSteps;      /* Adam steps, cosine learning-rate decay over them (2500) */
     float lr;                /* peak learning rate (2e-3) */
     float wLle;              /* weight of the LLE squared error in the loss (1) */
-    float confThreshold;     /* recompute points whose softmax maximum is below it (0.7) */
+    float confThreshold;     /* recompute points whose softmax maximum is below it (0.5) */
     float auditFraction;     /* random audit sample of the grid, recomputed (0.01) */
     int32_t boundaryRadius;  /* a neighbour within this Chebyshev radius with another
                                 predicted class marks a boundary point (1) */
