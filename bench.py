@@ -18,7 +18,8 @@ chen-lle2d-2048: the plain LLE map alone on 2048x2048 (the FP64 roofline case).
 Inputs are synthetic by nature: the grid itself.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-    python bench.py --workload chen-lle2d-2048|lorenz-dbscan-1024|lorenz-kde256-1024|lorenz-kde-1024|rossler-bif1d-1000|batch64
+    python bench.py --workload chen-lle2d-2048|lorenz-dbscan-1024|lorenz-kde256-1024|lorenz-kde-1024|
+                               lorenz-ls2d-1024|rossler-bif1d-1000|batch64
 
 Multi-GPU (torchrun, one rank per GPU): every rank computes its own 2048x2048 map
 of one c-stripe (weak scaling, no data-path collective); time = max over ranks.
@@ -78,6 +79,10 @@ SECONDARY = {
                                kdeI2=60.0, kdeH=1.0),
     # the same with the reference's per-peak sampling (k1 = 4 * peaks)
     "lorenz-kde-1024": dict(_LORENZ, task=1, kdeSampling=4, kdeI1=-60.0, kdeI2=60.0, kdeH=0.5),
+    # 2-D Lyapunov-spectrum map (LS2D), Lorenz (sigma, rho) 1024^2, 3 exponents per point
+    "lorenz-ls2d-1024": dict(system="lorenz", nPts=1024, ranges=[5.0, 20.0, 20.0, 200.0], idxMut=[1, 2],
+                             ic=[0.1, 0.1, 0.1], values=[0.5, 10.0, 28.0, 8.0 / 3.0], h=0.005, NT=0.5,
+                             tMax=1000.0, transientTime=50.0, lleEps=1e-8, maxValue=1e4, task=6),
     # 1-D bifurcation diagram, Rossler a in [0.05, 0.40], 1000 points
     "rossler-bif1d-1000": dict(system="rossler", nPts=1000, ranges=[0.05, 0.40], idxMut=[1],
                                ic=[0.1, 0.1, 0.1], values=[0.5, 0.2, 0.2, 5.7], h=0.01,
@@ -433,8 +438,14 @@ def run_secondary(args, name: str) -> int:
     dims = len(w["idxMut"])
     n = w["nPts"] ** dims
     rec = cbf.record_length(job)
-    spp = int(w["transientTime"] / w["h"]) + rec * w["preScaller"]
-    if task == cbf.TASK_PEAKS:
+    if task == cbf.TASK_LS:  # the base + D perturbed trajectories per interval
+        spp = int(w["transientTime"] / w["h"]) + (len(w["ic"]) + 1) * rec * int(w["NT"] / w["h"])
+    else:
+        spp = int(w["transientTime"] / w["h"]) + rec * w.get("preScaller", 1)
+    if task == cbf.TASK_LS:
+        out = torch.empty(n * len(w["ic"]), dtype=torch.float64, device="cuda")
+        aux_ptr = 0
+    elif task == cbf.TASK_PEAKS:
         cap = cbf.lib().cbf_peak_capacity(C.byref(job))
         job.peakCapacity = cap
         out = torch.empty(n * cap, dtype=torch.float64, device="cuda")
@@ -470,7 +481,9 @@ def run_secondary(args, name: str) -> int:
     probe = cbf.probe_fp64_peak(300.0)
     roof = fp64_roofline(torch, 0, w["system"], n, spp, t, clocks, probe)
     roof["traffic"] = None
-    roof["note"] = "integration flops only; the peak/KDE/DBSCAN work is on top"
+    roof["note"] = ("integration flops only (base + perturbed trajectories); Gram-Schmidt and log "
+                    "per interval on top") if task == cbf.TASK_LS else \
+        "integration flops only; the peak/KDE/DBSCAN work is on top"
     # oracle on a small contiguous sample
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
@@ -478,7 +491,9 @@ def run_secondary(args, name: str) -> int:
     oj = O.make_job(**{k: v for k, v in w.items() if k != "flags"})
     cnt = min(n, threads * 2)
     t0 = time.perf_counter()
-    if task == cbf.TASK_DBSCAN:
+    if task == cbf.TASK_LS:
+        O.map_ls(oj, np.arange(n // 2, n // 2 + cnt), threads=threads)
+    elif task == cbf.TASK_DBSCAN:
         O.map_dbscan(oj, n // 2, cnt, threads)
     elif task == cbf.TASK_KDE and not (w.get("flags", 0) & 2):
         O.map_kde(oj, n // 2, cnt, threads)
