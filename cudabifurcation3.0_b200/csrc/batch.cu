@@ -1,9 +1,12 @@
-// Ragged batches: many map jobs in one persistent launch.
+// Ragged batches: many map jobs in one persistent launch per kernel family.
 //
 // The reference runs one map per host call, one chunk and three kernels at a
 // time.  A batch here is any mix of jobs -- systems, tasks (LLE, KDE, DBSCAN,
-// 1-D peaks), grid sizes, record lengths, step sizes -- executed by ONE
-// persistent kernel:
+// 1-D peaks), grid sizes, record lengths, step sizes.  Its jobs form two
+// families, LLE jobs and peak-based jobs, each executed by ONE persistent
+// kernel compiled with that family's code only (so each gets its tasks'
+// register count and occupancy); with both present the two kernels run
+// concurrently on forked streams:
 //   * every job is cut into tiles of 32 points (one warp: a lane per point);
 //   * jobs are ordered by estimated cost per point, longest first, and a prefix
 //     table of tile counts maps a global tile number to (job, tile);
@@ -12,9 +15,9 @@
 //     cheapest tiles;
 //   * a tile runs exactly the per-point code of the map kernels (lle_device.cuh,
 //     bif_device.cuh), so batch results equal one-by-one results bit for bit.
-// One batch run is "reset counter + error flag, launch" and is captured once as
-// a CUDA graph for repeated sweeps.  The grid (blocks per SM) is chosen by
-// cbf_batch_autotune on a shortened copy of the batch.
+// One batch run is "reset error flag; per family: reset counter, launch" and is
+// captured once as a CUDA graph for repeated sweeps.  Each family's grid
+// (blocks per SM) is chosen by cbf_batch_autotune on a shortened copy of it.
 #include <string.h>
 
 #include <algorithm>
@@ -30,6 +33,7 @@ constexpr int kBatchWarps = 4;
 constexpr int kBatchThreads = kBatchWarps * 32;
 constexpr int kMaxBatchJobs = 1024;
 constexpr int kTile = 32;
+constexpr int kFamLle = 0, kFamPeaks = 1;
 
 struct BatchJob {
     DevJob job;
@@ -73,20 +77,23 @@ __device__ __forceinline__ void bif_tile(const DevJob& J, void* out, int* aux, l
     __syncwarp();
 }
 
-template <class S>
+// FAM: the kernel family -- kFamLle runs LLE jobs only, kFamPeaks the
+// peak-based tasks (PEAKS, KDE, DBSCAN).  Each family is compiled with its own
+// code only, so its register count and occupancy are those of its tasks.
+template <class S, int FAM>
 __device__ __forceinline__ void run_tile(const DevJob& J, void* out, int* aux, long long p0, int lane,
                                          double* slotPk, double* slotIv, int stride, unsigned* L,
                                          unsigned* Sb, int* err)
 {
-    switch (J.task) {
-    case CBF_TASK_LLE: {
+    if constexpr (FAM == kFamLle) {
         const long long p = p0 + lane;
         if (p < J.nPoints) {
             const long long g = grid_index(J, p);
             ((double*)out)[p] = J.sweepIC ? lle_point<S, true>(J, g) : lle_point<S, false>(J, g);
         }
-        break;
-    }
+        return;
+    } else {
+    switch (J.task) {
     case CBF_TASK_KDE:
         bif_tile<S, CBF_TASK_KDE>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, err);
         break;
@@ -99,13 +106,16 @@ __device__ __forceinline__ void run_tile(const DevJob& J, void* out, int* aux, l
     default:
         break;
     }
+    }
 }
 
 // WITH_M5: also dispatch the 5-D shipped model.  Its wider state raises the
-// register count of the whole kernel (128 vs 96), so batches of 3-D systems use
-// the instantiation without it.
-template <bool WITH_M5>
-__global__ void __launch_bounds__(kBatchThreads) batch_kernel(
+// register count of the whole kernel, so batches of 3-D systems use the
+// instantiation without it.
+// The LLE family is bounded to the occupancy of the autotuned LLE map kernel
+// (6 blocks of 128 threads per SM).
+template <int FAM, bool WITH_M5>
+__global__ void __launch_bounds__(kBatchThreads, FAM == kFamLle ? 6 : 1) batch_kernel(
     const BatchJob* __restrict__ jobs, int nJobs, const long long* __restrict__ tileEnd,
     unsigned long long* counter, double* scrPk, double* scrIv, int stride, int bitWords, int* err)
 {
@@ -135,17 +145,26 @@ __global__ void __launch_bounds__(kBatchThreads) batch_kernel(
         }
         const long long firstTile = lo ? sEnd[lo - 1] : 0;
         const long long p0 = ((long long)t - firstTile) * kTile;
-        const DevJob J = jobs[lo].job;
         void* out = jobs[lo].out;
         int* aux = jobs[lo].aux;
-        switch (J.system) {
-        case CBF_SYS_MEMRISTIVE5:
-            if (WITH_M5) run_tile<Memristive5>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, err);
-            break;
-        case CBF_SYS_ROSSLER: run_tile<Rossler>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, err); break;
-        case CBF_SYS_LORENZ: run_tile<Lorenz>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, err); break;
-        case CBF_SYS_CHEN: run_tile<Chen>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, err); break;
-        default: break;
+        auto go = [&](const DevJob& J) {
+            switch (J.system) {
+            case CBF_SYS_MEMRISTIVE5:
+                if (WITH_M5) run_tile<Memristive5, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, err);
+                break;
+            case CBF_SYS_ROSSLER: run_tile<Rossler, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, err); break;
+            case CBF_SYS_LORENZ: run_tile<Lorenz, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, err); break;
+            case CBF_SYS_CHEN: run_tile<Chen, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, err); break;
+            default: break;
+            }
+        };
+        // The LLE family reads its descriptor in place (read-only cache); the
+        // peak family keeps a copy (fewer registers in its epilogues).
+        if constexpr (FAM == kFamLle) {
+            go(jobs[lo].job);
+        } else {
+            const DevJob J = jobs[lo].job;
+            go(J);
         }
     }
 }
@@ -159,29 +178,37 @@ double steps_per_point(const DevJob& d)
 
 }  // namespace
 
+using BatchKernel = void (*)(const BatchJob*, int, const long long*, unsigned long long*, double*, double*,
+                            int, int, int*);
+
+BatchKernel batch_kernel_for(int fam, bool withM5)
+{
+    if (fam == kFamLle) return withM5 ? batch_kernel<kFamLle, true> : batch_kernel<kFamLle, false>;
+    return withM5 ? batch_kernel<kFamPeaks, true> : batch_kernel<kFamPeaks, false>;
+}
+
 cudaError_t batch_launch(const void* jobs, int nJobs, const long long* tileEnd,
                          unsigned long long* counter, double* scrPk, double* scrIv, int stride,
-                         int bitWords, int* err, int grid, bool withM5, cudaStream_t s)
+                         int bitWords, int* err, int grid, bool withM5, int fam, cudaStream_t s)
 {
     const size_t smem = (size_t)kBatchWarps * 2 * bitWords * sizeof(unsigned);
-    auto kern = withM5 ? batch_kernel<true> : batch_kernel<false>;
+    auto kern = batch_kernel_for(fam, withM5);
     cudaError_t e;
     if (smem > 48 * 1024) {
         e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
     if ((e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(err, 0, sizeof(int), s)) != cudaSuccess) return e;
     kern<<<grid, kBatchThreads, smem, s>>>((const BatchJob*)jobs, nJobs, tileEnd, counter, scrPk, scrIv,
                                            stride, bitWords, err);
     note_launch();
     return cudaGetLastError();
 }
 
-int batch_max_blocks_per_sm(int bitWords, bool withM5)
+int batch_max_blocks_per_sm(int bitWords, bool withM5, int fam)
 {
     const size_t smem = (size_t)kBatchWarps * 2 * bitWords * sizeof(unsigned);
-    auto kern = withM5 ? batch_kernel<true> : batch_kernel<false>;
+    auto kern = batch_kernel_for(fam, withM5);
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int perSm = 0;

@@ -19,6 +19,8 @@
 //             (its iterations are independent in the reference), popcount
 //             updates the neighbour counter.
 // Results leave as one coalesced 32-wide store per warp.
+#include <type_traits>
+
 #include "bif_device.cuh"
 
 namespace cbf {
@@ -27,6 +29,19 @@ namespace {
 
 constexpr int kBifWarps = 4;
 constexpr int kBifThreads = kBifWarps * 32;
+// Peak slots per lane in the first pass of a KDE/DBSCAN/Ostrovsky map.  The
+// reference's bound min(maxAmountOfPeaks, record/2) can be 10 000 and more;
+// sizing every lane's scratch for it leaves room for 2-3 blocks per SM.  Points
+// with more peaks than this (but not more than maxAmountOfPeaks, which only
+// need the count) are listed and recomputed in a second pass at full capacity.
+constexpr int kFirstPassPeaks = 1024;
+
+// Points whose first-pass peak list was truncated: grid index and output slot.
+struct Overflow {
+    long long* g;
+    long long* p;
+    unsigned long long* count;
+};
 
 // ---------------------------------------------------------------------------
 template <class S, int TASK>
@@ -34,7 +49,8 @@ __global__ void __launch_bounds__(kBifThreads) bif_kernel(const DevJob J, void* 
                                                           int* __restrict__ d_aux,
                                                           double* scrPeaks,
                                                           double* scrInt,
-                                                          int bitWords, int* __restrict__ err)
+                                                          int bitWords, int* __restrict__ err,
+                                                          const Overflow ov)
 {
     extern __shared__ unsigned smem[];
     const int lane = threadIdx.x & 31;
@@ -73,12 +89,19 @@ __global__ void __launch_bounds__(kBifThreads) bif_kernel(const DevJob J, void* 
         OstrovskyFlags of;
         of.init(J.ostThr);
         if (valid) n = integrate_point<S, TASK>(J, g, myPk, myIv, cap, nullptr, &div, &of);
+        // A truncated peak list whose result needs every peak goes to the second pass.
+        const bool over = valid && ov.count && n > cap && n <= J.maxPeaks;
+        if (over) {
+            const unsigned long long k = atomicAdd(ov.count, 1ull);
+            ov.g[k] = g;
+            ov.p[k] = p;
+        }
         __syncwarp();
 
         int res = 0;
         const int live = (int)min(32ll, J.nPoints - tile * 32);
         for (int j = 0; j < live; ++j) {
-            const int nj = __shfl_sync(kFull, n, j);
+            const int nj = __shfl_sync(kFull, over ? 0 : n, j);
             const double* pk = scrPeaks + (slot0 + j) * (long long)cap;
             int r;
             if (TASK == CBF_TASK_KDE) {
@@ -89,7 +112,7 @@ __global__ void __launch_bounds__(kBifThreads) bif_kernel(const DevJob J, void* 
             }
             if (lane == j) res = r;
         }
-        if (valid) {
+        if (valid && !over) {
             if (TASK == CBF_TASK_OSTROVSKY)
                 ((double*)d_out)[p] = ostrovsky_value(n, div != 0, of, res);
             else
@@ -99,8 +122,17 @@ __global__ void __launch_bounds__(kBifThreads) bif_kernel(const DevJob J, void* 
     }
 }
 
+template <class T>
+__global__ void scatter_kernel(const T* __restrict__ src, const long long* __restrict__ slot, long long n,
+                               T* __restrict__ dst)
+{
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) dst[slot[k]] = src[k];
+}
+
+// One launch of the fused kernel over the job's points (synchronises `s`).
 template <class S, int TASK>
-cudaError_t launch_bif_t(const DevJob& J, void* d_out, int* d_aux, cudaStream_t s)
+cudaError_t bif_pass(const DevJob& J, void* d_out, int* d_aux, const Overflow& ov, cudaStream_t s)
 {
     const long long nTiles = (J.nPoints + 31) / 32;
     if (nTiles == 0) return cudaSuccess;
@@ -146,7 +178,7 @@ cudaError_t launch_bif_t(const DevJob& J, void* d_out, int* d_aux, cudaStream_t 
         err = (int*)((char*)scrPeaks + bytes);
         if ((e = cudaMemsetAsync(err, 0, sizeof(int), s)) != cudaSuccess) return e;
     }
-    kern<<<(unsigned)blocks, kBifThreads, smemBytes, s>>>(J, d_out, d_aux, scrPeaks, scrInt, bitWords, err);
+    kern<<<(unsigned)blocks, kBifThreads, smemBytes, s>>>(J, d_out, d_aux, scrPeaks, scrInt, bitWords, err, ov);
     note_launch();
     e = cudaGetLastError();
     if (needScratch) {
@@ -158,6 +190,54 @@ cudaError_t launch_bif_t(const DevJob& J, void* d_out, int* d_aux, cudaStream_t 
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e == cudaSuccess && hostErr) return cudaErrorAssert;
     }
+    return e;
+}
+
+// KDE / DBSCAN / Ostrovsky maps whose peak capacity exceeds kFirstPassPeaks run
+// a first pass with that capacity -- more blocks per SM -- listing the points
+// whose peaks did not fit, then a second pass over that list at full capacity,
+// whose results are scattered into place.  Every point runs the same per-point
+// code as in a single pass, so the output is identical.
+template <class S, int TASK>
+cudaError_t launch_bif_t(const DevJob& J, void* d_out, int* d_aux, cudaStream_t s)
+{
+    constexpr bool split = TASK == CBF_TASK_KDE || TASK == CBF_TASK_DBSCAN || TASK == CBF_TASK_OSTROVSKY;
+    if (!split || J.peakCap <= kFirstPassPeaks || J.nPoints == 0)
+        return bif_pass<S, TASK>(J, d_out, d_aux, Overflow{nullptr, nullptr, nullptr}, s);
+    using Out = typename std::conditional<TASK == CBF_TASK_OSTROVSKY, double, int>::type;
+    const long long n = J.nPoints;
+    char* mem = nullptr;
+    // list of grid indices and slots, count, and the second pass's outputs
+    const size_t bytes = (size_t)n * (2 * sizeof(long long) + sizeof(Out)) + 256;
+    cudaError_t e = cudaMallocAsync((void**)&mem, bytes, s);
+    if (e != cudaSuccess) return e;
+    Overflow ov{(long long*)mem, (long long*)mem + n, (unsigned long long*)((long long*)mem + 2 * n)};
+    Out* tmp = (Out*)((char*)mem + (size_t)n * 2 * sizeof(long long) + 256);
+    unsigned long long count = 0;
+    e = cudaMemsetAsync(ov.count, 0, sizeof(unsigned long long), s);
+    if (e == cudaSuccess) {
+        DevJob J1 = J;
+        J1.peakCap = kFirstPassPeaks;
+        e = bif_pass<S, TASK>(J1, d_out, d_aux, ov, s);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&count, ov.count, sizeof(count), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess && count > 0) {
+        DevJob J2 = J;
+        J2.pointIndex = ov.g;
+        J2.firstPoint = 0;
+        J2.nPoints = (long long)count;
+        e = bif_pass<S, TASK>(J2, tmp, nullptr, Overflow{nullptr, nullptr, nullptr}, s);
+        if (e == cudaSuccess) {
+            scatter_kernel<Out><<<(unsigned)(((long long)count + 255) / 256), 256, 0, s>>>(tmp, ov.p, (long long)count,
+                                                                                         (Out*)d_out);
+            note_launch();
+            e = cudaGetLastError();
+        }
+    }
+    cudaError_t e2 = cudaFreeAsync(mem, s);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     return e;
 }
 
@@ -203,7 +283,8 @@ cudaError_t launch_bif_prealloc_t(const DevJob& J, void* d_out, double* scratch,
     if (fit < 1) return cudaErrorInvalidValue;
     if (blocks > fit) blocks = fit;
     double* scrInt = (TASK == CBF_TASK_DBSCAN) ? scratch + (size_t)blocks * kBifThreads * J.peakCap : nullptr;
-    kern<<<(unsigned)blocks, kBifThreads, smemBytes, s>>>(J, d_out, nullptr, scratch, scrInt, bitWords, err);
+    kern<<<(unsigned)blocks, kBifThreads, smemBytes, s>>>(J, d_out, nullptr, scratch, scrInt, bitWords, err,
+                                                          Overflow{nullptr, nullptr, nullptr});
     note_launch();
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     int hostErr = 0;

@@ -181,6 +181,33 @@ def test_kde_dbscan_ic_sweep_and_divergence(cbf, orc, gpu_ok):
     assert np.array_equal(got, orc.map_kde(o, 0, 100))
 
 
+# Long records: 985..2849 peaks per point, so with maxAmountOfPeaks 2500 the
+# map has points that fit the first pass (<= 1024 peaks), points recomputed in
+# the second pass (1025..2500) and points that only need their count (> 2500).
+SPLIT_MAP = dict(nPts=6, ranges=[5, 20, 20, 200], idxMut=[1, 2], h=0.01, tMax=900.0, transientTime=20.0,
+                 maxValue=1e4, writableVar=0, preScaller=1, maxAmountOfPeaks=2500, **LORENZ)
+
+
+@pytest.mark.parametrize("task", ["dbscan", "kde", "ostrovsky"])
+def test_two_pass_maps_bit_exact(cbf, orc, gpu_ok, task):
+    kw = dict(SPLIT_MAP)
+    n = kw["nPts"] ** 2
+    if task == "dbscan":
+        j, o = both(cbf, orc, task=cbf.TASK_DBSCAN, dbscanEps=0.05, **kw)
+        want = orc.map_dbscan(o, 0, n)
+    elif task == "kde":
+        j, o = both(cbf, orc, task=cbf.TASK_KDE, kdeSampling=2, kdeI1=-20.0, kdeI2=60.0, kdeH=0.5, **kw)
+        want = orc.map_kde(o, 0, n)
+    else:
+        kw.update(sweepIC=True, idxMut=[0, 2], ranges=[-10.0, 10.0, 5.0, 40.0])
+        j, o = both(cbf, orc, task=cbf.TASK_OSTROVSKY, dbscanEps=0.05, ostrovskyThreshold=12.0, **kw)
+        want = orc.map_ostrovsky(o, 0, n)
+    got, _ = cbf.run_host(j)
+    assert np.array_equal(got, want), np.nonzero(got != want)
+    if task == "ostrovsky":
+        assert np.array_equal(np.signbit(got), np.signbit(want))
+
+
 CHEN_LLE = dict(nPts=8, ranges=[30, 45, 20, 30], idxMut=[1, 3], h=0.002, NT=0.5, tMax=40.0,
                 transientTime=10.0, lleEps=1e-8, maxValue=1e4, **CHEN)
 
