@@ -36,6 +36,17 @@ constexpr int kBifThreads = kBifWarps * 32;
 // need the count) are listed and recomputed in a second pass at full capacity.
 constexpr int kFirstPassPeaks = 1024;
 
+// Sort buffer of the DBSCAN neighbour scans (keys per warp, a power of two
+// >= 32): only where the peak capacity is at most kFirstPassPeaks, so that a
+// block's shared memory stays at most 18 KB and eight blocks fit an SM.
+__host__ __device__ inline int bif_sort_cap(int task, int peakCap)
+{
+    if (!task_with_intervals(task) || peakCap > kFirstPassPeaks) return 0;
+    int c = 32;
+    while (c < peakCap && c < kDbscanSortCap) c <<= 1;
+    return c;
+}
+
 // Points whose first-pass peak list was truncated: grid index and output slot.
 struct Overflow {
     long long* g;
@@ -49,8 +60,8 @@ __global__ void __launch_bounds__(kBifThreads) bif_kernel(const DevJob J, void* 
                                                           int* __restrict__ d_aux,
                                                           double* scrPeaks,
                                                           double* scrInt,
-                                                          int bitWords, int* __restrict__ err,
-                                                          const Overflow ov)
+                                                          int bitWords, int sortCap,
+                                                          int* __restrict__ err, const Overflow ov)
 {
     extern __shared__ unsigned smem[];
     const int lane = threadIdx.x & 31;
@@ -59,8 +70,9 @@ __global__ void __launch_bounds__(kBifThreads) bif_kernel(const DevJob J, void* 
     const long long nWarps = (long long)gridDim.x * kBifWarps;
     const long long nTiles = (J.nPoints + 31) / 32;
     const int cap = J.peakCap;
-    unsigned* L = smem + (size_t)wib * 2 * bitWords;
+    unsigned* L = smem + (size_t)wib * dbscan_warp_words(bitWords, sortCap);
     unsigned* Sb = L + bitWords;
+    const DbscanSort so = dbscan_sort_area(L, bitWords, sortCap);
 
     for (long long tile = warpId; tile < nTiles; tile += nWarps) {
         const long long p = tile * 32 + lane;
@@ -108,7 +120,7 @@ __global__ void __launch_bounds__(kBifThreads) bif_kernel(const DevJob J, void* 
                 r = kde_warp(J, pk, nj, lane);
             } else {
                 const double* iv = scrInt + (slot0 + j) * (long long)cap;
-                r = dbscan_warp(J, pk, iv, nj, lane, L, Sb, err);
+                r = dbscan_warp(J, pk, iv, nj, lane, L, Sb, err, so);
             }
             if (lane == j) res = r;
         }
@@ -138,7 +150,8 @@ cudaError_t bif_pass(const DevJob& J, void* d_out, int* d_aux, const Overflow& o
     if (nTiles == 0) return cudaSuccess;
     const bool needScratch = (TASK == CBF_TASK_KDE || task_with_intervals(TASK));
     const int bitWords = task_with_intervals(TASK) ? (J.peakCap + 31) / 32 : 0;
-    const size_t smemBytes = (size_t)kBifWarps * 2 * bitWords * sizeof(unsigned);
+    const int sortCap = bif_sort_cap(TASK, J.peakCap);
+    const size_t smemBytes = (size_t)kBifWarps * dbscan_warp_words(bitWords, sortCap) * sizeof(unsigned);
 
     auto kern = bif_kernel<S, TASK>;
     cudaError_t e;
@@ -178,7 +191,8 @@ cudaError_t bif_pass(const DevJob& J, void* d_out, int* d_aux, const Overflow& o
         err = (int*)((char*)scrPeaks + bytes);
         if ((e = cudaMemsetAsync(err, 0, sizeof(int), s)) != cudaSuccess) return e;
     }
-    kern<<<(unsigned)blocks, kBifThreads, smemBytes, s>>>(J, d_out, d_aux, scrPeaks, scrInt, bitWords, err, ov);
+    kern<<<(unsigned)blocks, kBifThreads, smemBytes, s>>>(J, d_out, d_aux, scrPeaks, scrInt, bitWords, sortCap,
+                                                          err, ov);
     note_launch();
     e = cudaGetLastError();
     if (needScratch) {
@@ -261,7 +275,8 @@ cudaError_t launch_bif_prealloc_t(const DevJob& J, void* d_out, double* scratch,
     const long long nTiles = (J.nPoints + 31) / 32;
     if (nTiles == 0) return cudaSuccess;
     const int bitWords = (TASK == CBF_TASK_DBSCAN) ? (J.peakCap + 31) / 32 : 0;
-    const size_t smemBytes = (size_t)kBifWarps * 2 * bitWords * sizeof(unsigned);
+    const int sortCap = bif_sort_cap(TASK, J.peakCap);
+    const size_t smemBytes = (size_t)kBifWarps * dbscan_warp_words(bitWords, sortCap) * sizeof(unsigned);
     auto kern = bif_kernel<S, TASK>;
     cudaError_t e;
     if (smemBytes > 48 * 1024) {
@@ -283,8 +298,8 @@ cudaError_t launch_bif_prealloc_t(const DevJob& J, void* d_out, double* scratch,
     if (fit < 1) return cudaErrorInvalidValue;
     if (blocks > fit) blocks = fit;
     double* scrInt = (TASK == CBF_TASK_DBSCAN) ? scratch + (size_t)blocks * kBifThreads * J.peakCap : nullptr;
-    kern<<<(unsigned)blocks, kBifThreads, smemBytes, s>>>(J, d_out, nullptr, scratch, scrInt, bitWords, err,
-                                                          Overflow{nullptr, nullptr, nullptr});
+    kern<<<(unsigned)blocks, kBifThreads, smemBytes, s>>>(J, d_out, nullptr, scratch, scrInt, bitWords, sortCap,
+                                                          err, Overflow{nullptr, nullptr, nullptr});
     note_launch();
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     int hostErr = 0;

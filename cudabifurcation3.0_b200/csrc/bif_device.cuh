@@ -227,21 +227,37 @@ __device__ int kde_warp(const DevJob& J, const double* pk, int n, int lane)
     int res = 0;
     for (int base = 0; base < W; base += 32) {
         const int w = base + lane;
+        const int cnt = min(32, W - base);
+        const double delt = w * k2 + J.kdeI1;
+        // delt is monotone in w (rounded products and sums are), so the chunk's
+        // samples lie in [dlo, dhi], and rounded subtraction is monotone too: a
+        // peak with fl(p - dhi) > skip or fl(p - dlo) < -skip has |fl(p - delt)|
+        // > skip for every lane, i.e. it adds exactly +0 everywhere.  One ballot
+        // per 32 peaks drops those; the rest are summed in ascending m as before.
+        // A NaN bound fails both comparisons and keeps every peak.
+        const double dFirst = __shfl_sync(kFull, delt, 0);
+        const double dLast = __shfl_sync(kFull, delt, cnt - 1);
+        const double dlo = k2 >= 0 ? dFirst : dLast;
+        const double dhi = k2 >= 0 ? dLast : dFirst;
         double d2 = 0;
-        if (w < W) {
-            const double delt = w * k2 + J.kdeI1;
-            for (int m = 0; m < n; ++m) {
-                const double dd = pk[m] - delt;
+        for (int g = 0; g < n; g += 32) {
+            const int m = g + lane;
+            const double pv = m < n ? pk[m] : 0.0;
+            const bool near = m < n && !(pv - dhi > skip) && !(pv - dlo < -skip);
+            unsigned mask = __ballot_sync(kFull, near);
+            while (mask) {
+                const int j = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const double dd = __shfl_sync(kFull, pv, j) - delt;
                 // |dd| > 16|H| makes the FP32 exponent argument <= -128, where expf
                 // is exactly +0 (checked exhaustively on the device by
                 // cbf_probe_expf_zero), and adding +0 leaves the sum unchanged.
-                if (!(fabs(dd) > skip)) {
+                if (w < W && !(fabs(dd) > skip)) {
                     const double tmp = dd / H;
                     d2 += (double)expf((float)(-((tmp * tmp) / 2)));
                 }
             }
         }
-        const int cnt = min(32, W - base);
         for (int j = 0; j < cnt; ++j) {
             const double val = __shfl_sync(kFull, d2, j);
             pp = pr;
@@ -266,12 +282,291 @@ __device__ int kde_warp(const DevJob& J, const double* pk, int n, int lane)
 }
 
 // ---------------------------------------------------------------------------
-// DBSCAN cluster count of one point (dbscan, cudaLibrary.cu:457-529), whole warp.
+// DBSCAN (dbscan, cudaLibrary.cu:457-529), whole warp per point.
+//
 // helpfulArray[k] (label, nonzero once set) -> bitset L; helpfulArray[n+k] (the
 // "stack", holds k or 0) -> bitset S: popping slot m yields m if set, else 0.
+// One scan of a centre c adds to L and S exactly the set
+//     {k < n-1 : k != c, k unlabelled, near(c, k)}
+// and counts it into the stack depth.  The reference visits k in ascending
+// order, but each k once, and nothing it sets is read again within the scan,
+// so the order is immaterial.  Three facts make most scans avoidable without
+// changing any label, stack bit or count:
+//   * a scan of a centre with no near k at all adds nothing ("scan-empty");
+//   * a second scan of a centre adds nothing (its near k are all labelled
+//     after the first, and labels are never cleared);
+//   * once every k < n-1 is labelled, no scan adds anything.
+// A neighbour has |fl(p_k - p_c)| < skip (skip = 4 eps bounds the FP32 hypot
+// from below), hence p_k in [A, B] = p_c -/+ (2 skip + 4 ulp(p_c)) (rounded).
+// The peaks are sorted by a 32-bit key: the top 22 bits of an order-preserving
+// encoding of float(p_k) over the 10-bit index k.  Rounding to float and
+// truncating are monotone, so every candidate's key lies between the keys of A
+// and B: one window of sorted positions.  The scan-empty marks come from a few
+// probes per peak, and a real scan tests the window only, each candidate with
+// the exact test.  Chaotic points -- hundreds of peaks, almost all of them
+// singleton clusters -- then cost a sort and a word-wise walk instead of n
+// scans over n peaks.
+constexpr int kDbscanIdxBits = 10;
+constexpr int kDbscanSortCap = 1 << kDbscanIdxBits;  // scanned peaks (n - 1) a warp sorts
+constexpr unsigned kDbscanIdxMask = (1u << kDbscanIdxBits) - 1u;
+constexpr int kDbscanProbes = 32;  // per peak, in the scan-empty test; more: not marked
+
+struct DbscanSort {
+    unsigned* key = nullptr;  // sorted (coarse value << 10 | index)
+    unsigned* E = nullptr;    // scan-empty marks (bitset)
+    unsigned* D = nullptr;    // centres scanned once (bitset)
+    int cap = 0;              // entries of key; 0: no sorted path
+};
+
+// 32-bit words of shared memory per warp: the bitsets L and S of `bitWords`
+// words each, and with `sortCap` > 0 (a power of two, 32..1024) also E, D and
+// the sort keys.
+__host__ __device__ inline int dbscan_warp_words(int bitWords, int sortCap)
+{
+    return sortCap > 0 ? 4 * bitWords + sortCap : 2 * bitWords;
+}
+
+__device__ inline DbscanSort dbscan_sort_area(unsigned* warpWords, int bitWords, int sortCap)
+{
+    DbscanSort so;
+    if (sortCap > 0) {
+        so.E = warpWords + 2 * bitWords;
+        so.D = so.E + bitWords;
+        so.key = so.D + bitWords;
+        so.cap = sortCap;
+    }
+    return so;
+}
+
+// Top 22 bits of an order-preserving encoding of float(v): non-decreasing in v
+// (-0 is folded onto +0).
+__device__ __forceinline__ unsigned dbscan_coarse(double v)
+{
+    float f = (float)v;
+    if (f == 0.0f) f = 0.0f;
+    const unsigned u = __float_as_uint(f);
+    return ((u & 0x80000000u) ? ~u : (u | 0x80000000u)) >> kDbscanIdxBits;
+}
+
+// distance(...) < eps of the reference (cudaLibrary.cu:445-453) with c = (x1, y1)
+// the centre: 0 on exact equality, else the FP32 hypot of the double
+// differences.  hypotf(dx, dy) >= max(|dx|, |dy|) up to a few ulps, so a
+// coordinate gap >= skip = 4 eps can never be closer than eps.
+__device__ __forceinline__ bool dbscan_near(double x1, double y1, double x2, double y2, double eps,
+                                            double skip)
+{
+    if (x1 == x2 && y1 == y2) return 0.0 < eps;
+    const double dx = x2 - x1;
+    const double dy = y2 - y1;
+    if (fabs(dx) >= skip || fabs(dy) >= skip) return false;
+    return (double)hypotf((float)dx, (float)dy) < eps;
+}
+
+// Bitonic sort of the first P = 2^k >= M keys; the entries past M are
+// 0xffffffff and sort last (no finite value reaches that key).  Returns false
+// if a value is not finite (the caller then keeps the chunked scans).
+__device__ bool dbscan_sort(const DbscanSort& so, const double* pk, int M, int P, int lane)
+{
+    bool bad = false;
+    for (int k = lane; k < P; k += 32) {
+        unsigned key = 0xffffffffu;
+        if (k < M) {
+            const double v = pk[k];
+            if (!isfinite(v)) bad = true;
+            key = (dbscan_coarse(v) << kDbscanIdxBits) | (unsigned)k;
+        }
+        so.key[k] = key;
+    }
+    if (__any_sync(kFull, bad)) return false;
+    __syncwarp();
+    for (int size = 2; size <= P; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = lane; t < (P >> 1); t += 32) {
+                const int i = 2 * t - (t & (stride - 1));
+                const int j = i + stride;
+                const unsigned ki = so.key[i], kj = so.key[j];
+                if ((ki > kj) == ((i & size) == 0)) {
+                    so.key[i] = kj;
+                    so.key[j] = ki;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    return true;
+}
+
+// Coarse keys bounding the candidates of a centre at x1 (finite): every k with
+// |fl(p_k - x1)| < skip has p_k within x1 -/+ (2 skip + 4 ulp(x1)).
+__device__ __forceinline__ void dbscan_bounds(double x1, double skip, unsigned& cA, unsigned& cB)
+{
+    const double half = 2.0 * skip + fabs(x1) * 0x1p-50;
+    cA = dbscan_coarse(x1 - half);
+    cB = dbscan_coarse(x1 + half);
+}
+
+// Scan-empty marks: E[c] set iff no k < M (k != c) is near c, found by probing
+// the sorted neighbours of c outwards while their keys stay within c's bounds.
+// A peak with more than kDbscanProbes probes, and the unsorted last peak, stay
+// unmarked (their scans run).  E and D are cleared here.
+__device__ void dbscan_mark_empty(const DbscanSort& so, const double* pk, const double* iv, int n, int M,
+                                  double eps, double skip, int lane)
+{
+    const int words = (n + 31) >> 5;
+    for (int w = lane; w < words; w += 32) {
+        so.E[w] = 0u;
+        so.D[w] = 0u;
+    }
+    __syncwarp();
+    for (int pos = lane; pos < M; pos += 32) {
+        const int c = (int)(so.key[pos] & kDbscanIdxMask);
+        const double x1 = pk[c];
+        const double y1 = iv[c];
+        unsigned cA, cB;
+        dbscan_bounds(x1, skip, cA, cB);
+        bool near = false;
+        int probes = 0;
+        for (int q = pos + 1; q < M && !near; ++q) {
+            const unsigned kq = so.key[q];
+            if ((kq >> kDbscanIdxBits) > cB) break;
+            if (++probes > kDbscanProbes) { near = true; break; }
+            const int k = (int)(kq & kDbscanIdxMask);
+            near = dbscan_near(x1, y1, pk[k], iv[k], eps, skip);
+        }
+        for (int q = pos - 1; q >= 0 && !near; --q) {
+            const unsigned kq = so.key[q];
+            if ((kq >> kDbscanIdxBits) < cA) break;
+            if (++probes > kDbscanProbes) { near = true; break; }
+            const int k = (int)(kq & kDbscanIdxMask);
+            near = dbscan_near(x1, y1, pk[k], iv[k], eps, skip);
+        }
+        if (!near) atomicOr(&so.E[c >> 5], 1u << (c & 31));
+    }
+    __syncwarp();
+}
+
+// Number of sorted positions < M whose coarse value c satisfies pred(c), for a
+// predicate true on a prefix: the last entry of each of 32 segments first (the
+// non-empty segments whose last entry passes are a prefix of the lanes), then
+// the entries of the first segment whose last entry fails.
+template <class Pred>
+__device__ int dbscan_prefix(const unsigned* key, int M, int lane, Pred pred)
+{
+    const int seg = (M + 31) >> 5;
+    const int first = lane * seg;
+    const bool in1 = first < M && pred(key[min(first + seg, M) - 1] >> kDbscanIdxBits);
+    const int c = __popc(__ballot_sync(kFull, in1));
+    const int pos = c * seg + lane;
+    const bool in2 = lane < seg && pos < M && pred(key[pos] >> kDbscanIdxBits);
+    return min(M, c * seg + __popc(__ballot_sync(kFull, in2)));
+}
+
+// The scan of `center` over k = 0..M-1 in chunks of 32 (label word per chunk).
+// Returns the number of indices added to L and S.
+__device__ int dbscan_scan_chunked(const double* pk, const double* iv, int M, int center, double x1,
+                                   double y1, double eps, double skip, unsigned* L, unsigned* Sb,
+                                   int lane)
+{
+    int added = 0;
+    for (int base = 0; base < M; base += 32) {
+        const int k = base + lane;
+        bool cand = false;
+        if (k < M && k != center && !((L[base >> 5] >> lane) & 1u))
+            cand = dbscan_near(x1, y1, pk[k], iv[k], eps, skip);
+        const unsigned b = __ballot_sync(kFull, cand);
+        if (b) {
+            if (lane == 0) {
+                L[base >> 5] |= b;
+                Sb[base >> 5] |= b;
+            }
+            added += __popc(b);
+        }
+    }
+    return added;
+}
+
+// The scan of `center` over the sorted positions [lo, hi) that hold every
+// candidate.  Returns the number of indices added to L and S.
+__device__ int dbscan_scan_window(const DbscanSort& so, const double* pk, const double* iv, int lo, int hi,
+                                  int center, double x1, double y1, double eps, double skip, unsigned* L,
+                                  unsigned* Sb, int lane)
+{
+    int added = 0;
+    for (int base = lo; base < hi; base += 32) {
+        const int pos = base + lane;
+        bool cand = false;
+        int k = 0;
+        if (pos < hi) {
+            k = (int)(so.key[pos] & kDbscanIdxMask);
+            if (k != center && !((L[k >> 5] >> (k & 31)) & 1u))
+                cand = dbscan_near(x1, y1, pk[k], iv[k], eps, skip);
+        }
+        const unsigned b = __ballot_sync(kFull, cand);
+        if (b) {
+            if (cand) {
+                atomicOr(&L[k >> 5], 1u << (k & 31));
+                atomicOr(&Sb[k >> 5], 1u << (k & 31));
+            }
+            added += __popc(b);
+        }
+    }
+    return added;
+}
+
+// First index j >= i that is unlabelled and not scan-empty, or n.
+__device__ int dbscan_next_open(const unsigned* L, const unsigned* E, int n, int i, int lane)
+{
+    const int words = (n + 31) >> 5;
+    for (int w0 = i >> 5; w0 < words; w0 += 32) {
+        const int w = w0 + lane;
+        unsigned open = 0u;
+        if (w < words) {
+            open = ~L[w] & ~E[w];
+            if (w == (i >> 5)) open &= ~0u << (i & 31);
+            if (w == words - 1 && (n & 31)) open &= (1u << (n & 31)) - 1u;
+        }
+        const unsigned b = __ballot_sync(kFull, open != 0u);
+        if (b) {
+            const int f = __ffs(b) - 1;
+            const unsigned ow = __shfl_sync(kFull, open, f);
+            return ((w0 + f) << 5) + __ffs(ow) - 1;
+        }
+    }
+    return n;
+}
+
+// The reference's walk over i in [i, j) with an empty stack, where every
+// unlabelled index is scan-empty: labelled ones are no-ops, each unlabelled one
+// opens a cluster, is labelled, and its scan adds nothing.  Labels them all;
+// returns (clusters opened, of which among the scanned indices < M).
+__device__ int2 dbscan_open_run(unsigned* L, int i, int j, int M, int lane)
+{
+    int opened = 0, openedScanned = 0;
+    const int wEnd = (j - 1) >> 5;
+    for (int w0 = i >> 5; w0 <= wEnd; w0 += 32) {
+        const int w = w0 + lane;
+        unsigned m = 0u;
+        if (w <= wEnd) {
+            m = ~L[w];
+            if (w == (i >> 5)) m &= ~0u << (i & 31);
+            const int top = j - (w << 5);  // >= 1: bits below it lie in [i, j)
+            if (top < 32) m &= (1u << top) - 1u;
+            if (m) L[w] |= m;
+        }
+        const int c = __popc(m);
+        const int cLast = (w <= wEnd && (M >> 5) == w) ? (int)((m >> (M & 31)) & 1u) : 0;
+        opened += __reduce_add_sync(kFull, c);
+        openedScanned += __reduce_add_sync(kFull, c - cLast);
+    }
+    __syncwarp();
+    return make_int2(opened, openedScanned);
+}
+
+// DBSCAN cluster count of one point; `so` (shared memory of this warp) enables
+// the sorted path for points with n - 1 <= so.cap peaks.
 __device__ int dbscan_warp(const DevJob& J, const double* pk,
                            const double* iv, int n, int lane, unsigned* L,
-                           unsigned* Sb, int* err)
+                           unsigned* Sb, int* err, DbscanSort so = DbscanSort())
 {
     if (n <= 0) return 0;
     if (n == 1) return 1;
@@ -282,17 +577,36 @@ __device__ int dbscan_warp(const DevJob& J, const double* pk,
         L[w] = 0u;
         Sb[w] = 0u;
     }
-    __syncwarp();
 
     const double eps = J.dbEps;
     const double skip = J.dbSkip;
+    const int M = n - 1;  // indices 0..n-2 are scanned; the last peak never is
+    int P = 32;
+    while (P < M) P <<= 1;
+    const bool sorted = so.cap > 0 && M <= so.cap && skip > 0 && isfinite(skip) &&
+                        dbscan_sort(so, pk, M, P, lane);
+    if (sorted) dbscan_mark_empty(so, pk, iv, n, M, eps, skip, lane);
+    __syncwarp();
+
     int cluster = 0;
     int num = 0;
+    int nlab = 0;  // labels set among the scanned indices 0..n-2
     long long guard = (long long)n * n + 4ll * n + 16;
     for (int i = 0; i < n; i++) {
         if (--guard < 0) {
             if (lane == 0) atomicExch(err, 1);
             return 0;
+        }
+        if (sorted && num == 0) {
+            const int j = dbscan_next_open(L, so.E, n, i, lane);
+            if (j > i) {
+                const int2 r = dbscan_open_run(L, i, j, M, lane);
+                cluster += r.x;
+                nlab += r.y;
+                guard -= j - i;
+                i = j;
+                if (i >= n) break;
+            }
         }
         int center = -1;
         if (num >= 1) {
@@ -311,37 +625,32 @@ __device__ int dbscan_warp(const DevJob& J, const double* pk,
             if (lane == 0) L[i >> 5] |= 1u << (i & 31);
             __syncwarp();
             center = i;
+            if (i < M) ++nlab;
         }
-        if (center < 0) continue;
+        if (center < 0 || nlab >= M) continue;
 
         const double x1 = pk[center];
         const double y1 = iv[center];
-        for (int base = 0; base < n - 1; base += 32) {
-            const int k = base + lane;
-            bool cand = false;
-            if (k < n - 1 && k != center && !((L[base >> 5] >> lane) & 1u)) {
-                const double x2 = pk[k];
-                const double y2 = iv[k];
-                if (x1 == x2 && y1 == y2) {
-                    cand = 0.0 < eps;  // distance() returns 0 on exact equality (:447-448)
-                } else {
-                    const double dx = x2 - x1;
-                    const double dy = y2 - y1;
-                    // hypotf(dx, dy) >= max(|dx|, |dy|) up to a few ulps, so pairs with
-                    // a coordinate gap >= 4*eps can never be closer than eps.
-                    if (!(fabs(dx) >= skip || fabs(dy) >= skip))
-                        cand = (double)hypotf((float)dx, (float)dy) < eps;
-                }
-            }
-            const unsigned b = __ballot_sync(kFull, cand);
-            if (b) {
-                if (lane == 0) {
-                    L[base >> 5] |= b;
-                    Sb[base >> 5] |= b;
-                }
-                num += __popc(b);
-            }
+        int added;
+        if (sorted) {
+            const unsigned bit = 1u << (center & 31);
+            if ((so.E[center >> 5] | so.D[center >> 5]) & bit) continue;
+            if (lane == 0) so.D[center >> 5] |= bit;
         }
+        if (sorted && isfinite(x1)) {
+            unsigned cA, cB;
+            dbscan_bounds(x1, skip, cA, cB);
+            const int lo = dbscan_prefix(so.key, M, lane, [cA](unsigned c) { return c < cA; });
+            const int hi = dbscan_prefix(so.key, M, lane, [cB](unsigned c) { return c <= cB; });
+            if (2 * (hi - lo) <= M)
+                added = dbscan_scan_window(so, pk, iv, lo, hi, center, x1, y1, eps, skip, L, Sb, lane);
+            else
+                added = dbscan_scan_chunked(pk, iv, M, center, x1, y1, eps, skip, L, Sb, lane);
+        } else {
+            added = dbscan_scan_chunked(pk, iv, M, center, x1, y1, eps, skip, L, Sb, lane);
+        }
+        num += added;
+        nlab += added;
         __syncwarp();
     }
     return cluster - 1;

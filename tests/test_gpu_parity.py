@@ -142,6 +142,9 @@ LORENZ_MAP = dict(nPts=10, ranges=[5, 20, 20, 200], idxMut=[1, 2], h=0.005, tMax
     (10000, 4, -30.0, 60.0, 0.5, 0),
     (40, 10, -20.0, 60.0, 0.05, 0),          # some points exceed maxAmountOfPeaks
     (10000, 256, -20.0, 60.0, 0.05, 2),      # fixed 256-sample extension
+    (10000, 4, 60.0, -30.0, 0.5, 0),         # reversed interval: samples run downwards
+    (10000, 10, -20.0, 60.0, 2.0, 0),        # wide kernel: most peaks reach most chunks
+    (10000, 64, -20.0, 60.0, 0.005, 0),      # narrow kernel: most chunks see no peak
 ])
 def test_kde_map_bit_exact(cbf, orc, gpu_ok, maxPeaks, samp, i1, i2, hh, flags):
     kw = dict(LORENZ_MAP, maxAmountOfPeaks=maxPeaks, kdeSampling=samp, kdeI1=i1, kdeI2=i2, kdeH=hh)
@@ -166,6 +169,30 @@ def test_dbscan_map_bit_exact(cbf, orc, gpu_ok, maxPeaks, eps):
     j, o = both(cbf, orc, task=cbf.TASK_DBSCAN, **kw)
     got, _ = cbf.run_host(j)
     want = orc.map_dbscan(o, 0, kw["nPts"] ** 2)
+    assert np.array_equal(got, want), np.nonzero(got != want)
+
+
+@pytest.mark.parametrize("tMax,eps", [(300.0, 1e-3), (300.0, 0.3), (300.0, 3.0), (500.0, 1e-3)])
+def test_dbscan_long_records_bit_exact(cbf, orc, gpu_ok, tMax, eps):
+    """Hundreds of peaks per point: about 400 (sorted-window scans, with small and
+    large windows) and about 670 (more than a warp sorts: chunked scans)."""
+    kw = dict(LORENZ_MAP, nPts=8, tMax=tMax, maxAmountOfPeaks=10000, dbscanEps=eps)
+    j, o = both(cbf, orc, task=cbf.TASK_DBSCAN, **kw)
+    got, _ = cbf.run_host(j)
+    want = orc.map_dbscan(o, 0, 64)
+    assert np.array_equal(got, want), np.nonzero(got != want)
+    assert len(np.unique(want)) > 3
+
+
+@pytest.mark.parametrize("first", [200_000, 530_000, 1_000_000])
+def test_dbscan_full_workload_slices(cbf, orc, gpu_ok, first):
+    """Slices of the 1024^2 Lorenz DBSCAN map (sigma in [5,20], rho in [20,200],
+    transient 500, record 200, eps 1e-3), through the two-pass launch."""
+    kw = dict(nPts=1024, ranges=[5, 20, 20, 200], idxMut=[1, 2], h=0.005, tMax=200.0, transientTime=500.0,
+              maxValue=1e4, writableVar=0, preScaller=1, maxAmountOfPeaks=10000, dbscanEps=1e-3, **LORENZ)
+    j, o = both(cbf, orc, task=cbf.TASK_DBSCAN, firstPoint=first, nPoints=48, **kw)
+    got, _ = cbf.run_host(j)
+    want = orc.map_dbscan(o, first, 48)
     assert np.array_equal(got, want), np.nonzero(got != want)
 
 
