@@ -44,7 +44,7 @@ struct BatchJob {
 template <class S, int TASK>
 __device__ __forceinline__ void bif_tile(const DevJob& J, void* out, int* aux, long long p0, int lane,
                                          double* slotPk, double* slotIv, int stride, unsigned* L,
-                                         unsigned* Sb, int* err)
+                                         unsigned* Sb, const DbscanSort& so, int* err)
 {
     const long long p = p0 + lane;
     const bool valid = p < J.nPoints;
@@ -70,7 +70,7 @@ __device__ __forceinline__ void bif_tile(const DevJob& J, void* out, int* aux, l
         if (TASK == CBF_TASK_KDE)
             r = kde_warp(J, pk, nj, lane);
         else
-            r = dbscan_warp(J, pk, slotIv + (long long)j * stride, nj, lane, L, Sb, err);
+            r = dbscan_warp(J, pk, slotIv + (long long)j * stride, nj, lane, L, Sb, err, so);
         if (lane == j) res = r;
     }
     if (valid) ((int*)out)[p] = res;
@@ -83,7 +83,7 @@ __device__ __forceinline__ void bif_tile(const DevJob& J, void* out, int* aux, l
 template <class S, int FAM>
 __device__ __forceinline__ void run_tile(const DevJob& J, void* out, int* aux, long long p0, int lane,
                                          double* slotPk, double* slotIv, int stride, unsigned* L,
-                                         unsigned* Sb, int* err)
+                                         unsigned* Sb, const DbscanSort& so, int* err)
 {
     if constexpr (FAM == kFamLle) {
         const long long p = p0 + lane;
@@ -95,13 +95,13 @@ __device__ __forceinline__ void run_tile(const DevJob& J, void* out, int* aux, l
     } else {
     switch (J.task) {
     case CBF_TASK_KDE:
-        bif_tile<S, CBF_TASK_KDE>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, err);
+        bif_tile<S, CBF_TASK_KDE>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err);
         break;
     case CBF_TASK_DBSCAN:
-        bif_tile<S, CBF_TASK_DBSCAN>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, err);
+        bif_tile<S, CBF_TASK_DBSCAN>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err);
         break;
     case CBF_TASK_PEAKS:
-        bif_tile<S, CBF_TASK_PEAKS>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, err);
+        bif_tile<S, CBF_TASK_PEAKS>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err);
         break;
     default:
         break;
@@ -117,7 +117,7 @@ __device__ __forceinline__ void run_tile(const DevJob& J, void* out, int* aux, l
 template <int FAM, bool WITH_M5>
 __global__ void __launch_bounds__(kBatchThreads, FAM == kFamLle ? 6 : 1) batch_kernel(
     const BatchJob* __restrict__ jobs, int nJobs, const long long* __restrict__ tileEnd,
-    unsigned long long* counter, double* scrPk, double* scrIv, int stride, int bitWords, int* err)
+    unsigned long long* counter, double* scrPk, double* scrIv, int stride, int bitWords, int sortCap, int* err)
 {
     extern __shared__ unsigned smem[];
     __shared__ long long sEnd[kMaxBatchJobs];
@@ -127,8 +127,9 @@ __global__ void __launch_bounds__(kBatchThreads, FAM == kFamLle ? 6 : 1) batch_k
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const long long warpId = (long long)blockIdx.x * kBatchWarps + wib;
-    unsigned* L = smem + (size_t)wib * 2 * bitWords;
+    unsigned* L = smem + (size_t)wib * dbscan_warp_words(bitWords, sortCap);
     unsigned* Sb = L + bitWords;
+    const DbscanSort so = dbscan_sort_area(L, bitWords, sortCap);
     double* slotPk = scrPk ? scrPk + warpId * kTile * (long long)stride : nullptr;
     double* slotIv = scrIv ? scrIv + warpId * kTile * (long long)stride : nullptr;
 
@@ -150,11 +151,11 @@ __global__ void __launch_bounds__(kBatchThreads, FAM == kFamLle ? 6 : 1) batch_k
         auto go = [&](const DevJob& J) {
             switch (J.system) {
             case CBF_SYS_MEMRISTIVE5:
-                if (WITH_M5) run_tile<Memristive5, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, err);
+                if (WITH_M5) run_tile<Memristive5, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err);
                 break;
-            case CBF_SYS_ROSSLER: run_tile<Rossler, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, err); break;
-            case CBF_SYS_LORENZ: run_tile<Lorenz, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, err); break;
-            case CBF_SYS_CHEN: run_tile<Chen, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, err); break;
+            case CBF_SYS_ROSSLER: run_tile<Rossler, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err); break;
+            case CBF_SYS_LORENZ: run_tile<Lorenz, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err); break;
+            case CBF_SYS_CHEN: run_tile<Chen, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err); break;
             default: break;
             }
         };
@@ -179,7 +180,7 @@ double steps_per_point(const DevJob& d)
 }  // namespace
 
 using BatchKernel = void (*)(const BatchJob*, int, const long long*, unsigned long long*, double*, double*,
-                            int, int, int*);
+                            int, int, int, int*);
 
 BatchKernel batch_kernel_for(int fam, bool withM5)
 {
@@ -191,7 +192,8 @@ cudaError_t batch_launch(const void* jobs, int nJobs, const long long* tileEnd,
                          unsigned long long* counter, double* scrPk, double* scrIv, int stride,
                          int bitWords, int* err, int grid, bool withM5, int fam, cudaStream_t s)
 {
-    const size_t smem = (size_t)kBatchWarps * 2 * bitWords * sizeof(unsigned);
+    const int sortCap = bitWords > 0 ? dbscan_sort_cap(bitWords * 32) : 0;
+    const size_t smem = (size_t)kBatchWarps * dbscan_warp_words(bitWords, sortCap) * sizeof(unsigned);
     auto kern = batch_kernel_for(fam, withM5);
     cudaError_t e;
     if (smem > 48 * 1024) {
@@ -200,14 +202,15 @@ cudaError_t batch_launch(const void* jobs, int nJobs, const long long* tileEnd,
     }
     if ((e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s)) != cudaSuccess) return e;
     kern<<<grid, kBatchThreads, smem, s>>>((const BatchJob*)jobs, nJobs, tileEnd, counter, scrPk, scrIv,
-                                           stride, bitWords, err);
+                                           stride, bitWords, sortCap, err);
     note_launch();
     return cudaGetLastError();
 }
 
 int batch_max_blocks_per_sm(int bitWords, bool withM5, int fam)
 {
-    const size_t smem = (size_t)kBatchWarps * 2 * bitWords * sizeof(unsigned);
+    const int sortCap = bitWords > 0 ? dbscan_sort_cap(bitWords * 32) : 0;
+    const size_t smem = (size_t)kBatchWarps * dbscan_warp_words(bitWords, sortCap) * sizeof(unsigned);
     auto kern = batch_kernel_for(fam, withM5);
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -41,10 +41,7 @@ constexpr int kFirstPassPeaks = 1024;
 // block's shared memory stays at most 18 KB and eight blocks fit an SM.
 __host__ __device__ inline int bif_sort_cap(int task, int peakCap)
 {
-    if (!task_with_intervals(task) || peakCap > kFirstPassPeaks) return 0;
-    int c = 32;
-    while (c < peakCap && c < kDbscanSortCap) c <<= 1;
-    return c;
+    return task_with_intervals(task) && peakCap <= kFirstPassPeaks ? dbscan_sort_cap(peakCap) : 0;
 }
 
 // Points whose first-pass peak list was truncated: grid index and output slot.

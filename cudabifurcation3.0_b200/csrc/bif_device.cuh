@@ -221,6 +221,7 @@ __device__ int kde_warp(const DevJob& J, const double* pk, int n, int lane)
     const int W = (k1 - 1 > 0) ? (int)ceil(k1 - 1) : 0;
     const double skip = J.kdeSkip;
     const double H = J.kdeH;
+    const double invH = J.kdeInvH;
 
     double pp = 0, pr = 0, cur = 0;
     bool strange = false;
@@ -253,7 +254,7 @@ __device__ int kde_warp(const DevJob& J, const double* pk, int n, int lane)
                 // is exactly +0 (checked exhaustively on the device by
                 // cbf_probe_expf_zero), and adding +0 leaves the sum unchanged.
                 if (w < W && !(fabs(dd) > skip)) {
-                    const double tmp = dd / H;
+                    const double tmp = invH != 0.0 ? dd * invH : dd / H;
                     d2 += (double)expf((float)(-((tmp * tmp) / 2)));
                 }
             }
@@ -324,6 +325,16 @@ struct DbscanSort {
 __host__ __device__ inline int dbscan_warp_words(int bitWords, int sortCap)
 {
     return sortCap > 0 ? 4 * bitWords + sortCap : 2 * bitWords;
+}
+
+// Sort keys per warp for peak lists of up to `peakCap` peaks: a power of two
+// >= 32, or 0 (no sorted path) when peakCap exceeds kDbscanSortCap.
+__host__ __device__ inline int dbscan_sort_cap(int peakCap)
+{
+    if (peakCap > kDbscanSortCap) return 0;
+    int c = 32;
+    while (c < peakCap) c <<= 1;
+    return c;
 }
 
 __device__ inline DbscanSort dbscan_sort_area(unsigned* warpWords, int bitWords, int sortCap)

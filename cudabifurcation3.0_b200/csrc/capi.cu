@@ -298,6 +298,12 @@ cbf_status lower_job(const cbf_job* j, DevJob* d)
             d->kdeI2 = j->kdeI2;
             d->kdeH = j->kdeH;
             d->kdeSkip = 16.0 * fabs(j->kdeH);
+            // For H = +-2^k, x / H and x * (1/H) are the same exact real rounded
+            // once, so the epilogue may multiply (bit-identical, no FP64 divide).
+            int ex = 0;
+            const double mant = frexp(fabs(j->kdeH), &ex);
+            const double inv = 1.0 / j->kdeH;
+            d->kdeInvH = (mant == 0.5 && std::isnormal(inv)) ? inv : 0.0;
         }
         if (j->task == CBF_TASK_OSTROVSKY) d->ostThr = j->ostrovskyThreshold;
         if (j->task == CBF_TASK_DBSCAN || j->task == CBF_TASK_OSTROVSKY) {

@@ -23,6 +23,7 @@ struct DevJob {
     double tMax;
     double kdeI1, kdeI2, kdeH;
     double kdeSkip;     // terms with |peak - delta| > kdeSkip are exactly 0 (see kde epilogue)
+    double kdeInvH;     // 1/kdeH when kdeH = +-2^k and 1/kdeH is a normal double, else 0
     double dbEps;
     double dbSkip;      // pairs with |dx| or |dy| >= dbSkip are never neighbours
     long long firstPoint;

@@ -134,7 +134,8 @@ __device__ double lle_regime_point(const DevJob& J, long long g, double* pk, dou
 template <class S, bool IC>
 __global__ void __launch_bounds__(kRegThreads) lle_regime_kernel(const DevJob J, double* __restrict__ lle,
                                                                  int* __restrict__ cls, double* scrPk,
-                                                                 double* scrIv, int bitWords, int* err)
+                                                                 double* scrIv, int bitWords, int sortCap,
+                                                                 int* err)
 {
     extern __shared__ unsigned smem[];
     const int lane = threadIdx.x & 31;
@@ -143,8 +144,9 @@ __global__ void __launch_bounds__(kRegThreads) lle_regime_kernel(const DevJob J,
     const long long nWarps = (long long)gridDim.x * kRegWarps;
     const long long nTiles = (J.nPoints + 31) / 32;
     const int cap = J.peakCap;
-    unsigned* L = smem + (size_t)wib * 2 * bitWords;
+    unsigned* L = smem + (size_t)wib * dbscan_warp_words(bitWords, sortCap);
     unsigned* Sb = L + bitWords;
+    const DbscanSort so = dbscan_sort_area(L, bitWords, sortCap);
     const long long slot0 = warpId * 32;
 
     for (long long tile = warpId; tile < nTiles; tile += nWarps) {
@@ -169,7 +171,7 @@ __global__ void __launch_bounds__(kRegThreads) lle_regime_kernel(const DevJob J,
             else {
                 const double* pk = scrPk + (slot0 + j) * (long long)cap;
                 const double* iv = scrIv + (slot0 + j) * (long long)cap;
-                r = min(dbscan_warp(J, pk, iv, nj, lane, L, Sb, err), kNumClasses - 1);
+                r = min(dbscan_warp(J, pk, iv, nj, lane, L, Sb, err, so), kNumClasses - 1);
             }
             if (lane == j) res = r;
         }
@@ -187,7 +189,8 @@ cudaError_t launch_t(const DevJob& J, double* d_lle, int* d_cls, cudaStream_t s)
     const long long nTiles = (J.nPoints + 31) / 32;
     if (nTiles == 0) return cudaSuccess;
     const int bitWords = (J.peakCap + 31) / 32;
-    const size_t smemBytes = (size_t)kRegWarps * 2 * bitWords * sizeof(unsigned);
+    const int sortCap = dbscan_sort_cap(J.peakCap);
+    const size_t smemBytes = (size_t)kRegWarps * dbscan_warp_words(bitWords, sortCap) * sizeof(unsigned);
     auto kern = lle_regime_kernel<S, IC>;
     cudaError_t e;
     if (smemBytes > 48 * 1024) {
@@ -216,7 +219,7 @@ cudaError_t launch_t(const DevJob& J, double* d_lle, int* d_cls, cudaStream_t s)
     double* scrIv = scr + (size_t)blocks * kRegThreads * J.peakCap;
     int* err = (int*)((char*)scr + bytes);
     if ((e = cudaMemsetAsync(err, 0, sizeof(int), s)) == cudaSuccess) {
-        kern<<<(unsigned)blocks, kRegThreads, smemBytes, s>>>(J, d_lle, d_cls, scr, scrIv, bitWords, err);
+        kern<<<(unsigned)blocks, kRegThreads, smemBytes, s>>>(J, d_lle, d_cls, scr, scrIv, bitWords, sortCap, err);
         note_launch();
         e = cudaGetLastError();
     }
@@ -240,7 +243,8 @@ template <class S>
 long long resident_s(const DevJob& J)
 {
     const int bitWords = (J.peakCap + 31) / 32;
-    const size_t smemBytes = (size_t)kRegWarps * 2 * bitWords * sizeof(unsigned);
+    const int sortCap = dbscan_sort_cap(J.peakCap);
+    const size_t smemBytes = (size_t)kRegWarps * dbscan_warp_words(bitWords, sortCap) * sizeof(unsigned);
     auto kern = J.sweepIC ? lle_regime_kernel<S, true> : lle_regime_kernel<S, false>;
     if (smemBytes > 48 * 1024)
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBytes);
