@@ -48,6 +48,7 @@ EXPORTS = [
     "cbf_csv_write_map", "cbf_csv_write_peaks", "cbf_csv_write_pairs",
     "cbf_mlp_num_params", "cbf_mlp_create", "cbf_mlp_destroy", "cbf_mlp_get_params",
     "cbf_mlp_set_params", "cbf_mlp_forward_backward", "cbf_mlp_train", "cbf_mlp_predict",
+    "cbf_mlp_predict_grid", "cbf_mlp_grid_features",
     "cbf_surrogate_config_init", "cbf_lle_map_surrogate", "cbf_surrogate_release", "cbf_ls1d", "cbf_ls2d",
     "cbf_csv_write_rows", "cbf_npy_write", "cbf_ostrovsky2d", "cbf_modeling_one_system",
 ]
@@ -264,6 +265,11 @@ def lib():
         L.cbf_mlp_predict.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_float, C.c_float,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.cbf_mlp_predict.restype = C.c_int32
+        L.cbf_mlp_predict_grid.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p]
+        L.cbf_mlp_predict_grid.restype = C.c_int32
+        L.cbf_mlp_grid_features.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
+        L.cbf_mlp_grid_features.restype = C.c_int32
         L.cbf_surrogate_config_init.argtypes = [C.POINTER(SurrogateConfig)]
         L.cbf_surrogate_config_init.restype = None
         L.cbf_lle_map_surrogate.argtypes = [C.POINTER(Job), C.POINTER(SurrogateConfig), C.c_void_p,
@@ -356,6 +362,12 @@ def run_host(job: Job):
     check(L.cbf_run_host(C.byref(job), out.ctypes.data_as(C.c_void_p),
                          None if aux is None else aux.ctypes.data_as(C.c_void_p)))
     return out, aux
+
+
+def grid_features(job: Job, d_idx: int, n: int, d_x: int, stream: int = 0) -> None:
+    """The surrogate network's input features of grid points d_idx[0..n) (FP32, 4 per point)."""
+    check(lib().cbf_mlp_grid_features(C.byref(job), C.c_void_p(d_idx), n, C.c_void_p(d_x),
+                                      C.c_void_p(stream or None)))
 
 
 def run_device(job: Job, d_out: int, d_aux: int = 0, stream: int = 0) -> None:
@@ -492,6 +504,12 @@ class Mlp:
         check(lib().cbf_mlp_predict(self.handle, C.c_void_p(d_x), n, lle_mean, lle_std,
                                     C.c_void_p(d_lle or None), C.c_void_p(d_cls or None),
                                     C.c_void_p(d_conf or None), C.c_void_p(stream or None)))
+
+    def predict_grid(self, job: "Job", lle_mean: float, lle_std: float, d_lle: int, d_cls: int, d_conf: int,
+                     stream: int = 0) -> None:
+        """Predictions for every point of the job's 2-D grid (tcgen05 kernel)."""
+        check(lib().cbf_mlp_predict_grid(self.handle, C.byref(job), lle_mean, lle_std, C.c_void_p(d_lle),
+                                         C.c_void_p(d_cls), C.c_void_p(d_conf), C.c_void_p(stream or None)))
 
     def close(self):
         if self.handle:

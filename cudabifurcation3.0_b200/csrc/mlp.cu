@@ -453,36 +453,7 @@ __global__ void features_kernel(const FeatureSpec f, const long long* __restrict
     for (int i = 0; i < kIn; ++i) X[k * kIn + i] = x[i];
 }
 
-// BF16 feature rows of grid points g0 .. g0+n-1.
-__global__ void grid_features_kernel(const FeatureSpec f, long long g0, long long n, bf16* __restrict__ xb)
-{
-    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    float x[kIn];
-    point_features(f, g0 + k, x);
-#pragma unroll
-    for (int i = 0; i < kIn; ++i) xb[k * kIn + i] = __float2bfloat16_rn(x[i]);
-}
-
-__global__ void head_grid_kernel(const float* __restrict__ out, long long n, float lleMean, float lleStd,
-                                 double* __restrict__ lle, int* __restrict__ cls, float* __restrict__ conf)
-{
-    const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n) return;
-    const float* o = out + r * kOut;
-    int best = 0;
-    float mx = o[1];
-    for (int c = 1; c < kClasses; ++c)
-        if (o[1 + c] > mx) {
-            mx = o[1 + c];
-            best = c;
-        }
-    float sum = 0.f;
-    for (int c = 0; c < kClasses; ++c) sum += __expf(o[1 + c] - mx);
-    lle[r] = (double)(o[0] * lleStd + lleMean);
-    cls[r] = best;
-    conf[r] = 1.0f / sum;
-}
+#include "mlp_tc.cuh"
 
 template <class F>
 cudaError_t launch1d(long long n, cudaStream_t s, F f)
@@ -532,6 +503,9 @@ struct Mlp {
     // inference workspace (rows per chunk = kPredRows), no pre-activations
     bf16 *pxb = nullptr, *ph1 = nullptr, *ph2 = nullptr, *ph3 = nullptr;
     float* pout = nullptr;
+    // grid prediction on tcgen05: weights in the shared-memory operand layout
+    unsigned char* wpack = nullptr;
+    int* tcErr = nullptr;
 };
 
 constexpr int kPredRows = 262144;
@@ -683,7 +657,8 @@ void mlp_free(cbf_mlp* m)
     if (m->graph) cudaGraphDestroy(m->graph);
     void* ptrs[] = {m->params, m->grads, m->m1, m->m2, m->pb, m->xb, m->yl, m->yc, m->z1, m->z2,
                     m->z3, m->h1, m->h2, m->h3, m->out, m->dOut, m->dOutB, m->dz, m->dz3,
-                    m->dz2, m->dz1, m->loss, m->ws, m->step, m->pxb, m->ph1, m->ph2, m->ph3, m->pout};
+                    m->dz2, m->dz1, m->loss, m->ws, m->step, m->pxb, m->ph1, m->ph2, m->ph3, m->pout,
+                    m->wpack, m->tcErr};
     for (void* p : ptrs) cudaFree(p);
 }
 
@@ -899,6 +874,32 @@ cbf_status cbf_mlp_predict(cbf_mlp* m, const float* dX, int64_t N, float lleMean
     return CBF_OK;
 }
 
+cbf_status cbf_mlp_predict_grid(cbf_mlp* m, const cbf_job* job, float lleMean, float lleStd, double* dLle,
+                                int32_t* dCls, float* dConf, void* stream)
+{
+    if (!m || !job || !dLle || !dCls || !dConf) return report_error(CBF_ERR_INVALID_ARG, "bad prediction arguments");
+    cbf::DevJob d;
+    cbf_status st = cbf::lower_job_for(job, &d);
+    if (st != CBF_OK) return st;
+    if (d.dims != 2 || d.nIC != 3) return report_error(CBF_ERR_INVALID_ARG, "grid prediction needs a 2-D sweep of a 3-D system");
+    const long long n = (long long)d.nPts * d.nPts;
+    cudaError_t e = cbf::mlp_predict_grid(m, cbf::feature_spec(d), n, lleMean, lleStd, dLle, (int*)dCls, dConf,
+                                          (cudaStream_t)stream);
+    if (e != cudaSuccess) return report_cuda_error(e, "grid prediction");
+    return CBF_OK;
+}
+
+cbf_status cbf_mlp_grid_features(const cbf_job* job, const int64_t* dIdx, int64_t n, float* dX, void* stream)
+{
+    if (!job || n < 0 || (n > 0 && (!dIdx || !dX))) return report_error(CBF_ERR_INVALID_ARG, "bad feature arguments");
+    cbf::DevJob d;
+    cbf_status st = cbf::lower_job_for(job, &d);
+    if (st != CBF_OK) return st;
+    cudaError_t e = cbf::mlp_features(cbf::feature_spec(d), (const long long*)dIdx, n, dX, (cudaStream_t)stream);
+    if (e != cudaSuccess) return report_cuda_error(e, "grid features");
+    return CBF_OK;
+}
+
 }  // extern "C"
 
 namespace cbf {
@@ -924,20 +925,36 @@ cudaError_t mlp_features(const FeatureSpec& f, const long long* idx, long long n
     return launch1d(n, s, [&](unsigned b, int t) { features_kernel<<<b, t, 0, s>>>(f, idx, n, X); });
 }
 
+// One fused tcgen05 kernel over the whole grid (mlp_tc.cuh), after packing the
+// current BF16 weights into the operand layout.  A wait that ran out inside
+// the kernel is reported as cudaErrorLaunchTimeout.
 cudaError_t mlp_predict_grid(cbf_mlp* m, const FeatureSpec& f, long long nPoints, float lleMean,
                              float lleStd, double* lle, int* cls, float* conf, cudaStream_t s)
 {
-    cudaError_t e = pred_workspace(m);
-    for (long long r0 = 0; r0 < nPoints && e == cudaSuccess; r0 += kPredRows) {
-        const int n = (int)((nPoints - r0) < kPredRows ? (nPoints - r0) : kPredRows);
-        e = launch1d(n, s, [&](unsigned b, int t) { grid_features_kernel<<<b, t, 0, s>>>(f, r0, n, m->pxb); });
-        if (e == cudaSuccess)
-            e = forward(*m, n, m->pxb, m->pout, nullptr, nullptr, nullptr, m->ph1, m->ph2, m->ph3, s);
-        if (e == cudaSuccess)
-            e = launch1d(n, s, [&](unsigned b, int t) {
-                head_grid_kernel<<<b, t, 0, s>>>(m->pout, n, lleMean, lleStd, lle + r0, cls + r0, conf + r0);
-            });
-    }
+    if (nPoints <= 0) return cudaSuccess;
+    cudaError_t e = cudaSuccess;
+    if (!m->wpack) e = cudaMalloc((void**)&m->wpack, kTcPackBytes);
+    if (e == cudaSuccess && !m->tcErr) e = cudaMalloc((void**)&m->tcErr, sizeof(int));
+    if (e != cudaSuccess) return e;
+    e = launch1d(kTcPackBytes / 2, s,
+                 [&](unsigned b, int t) { tc_pack_kernel<<<b, t, 0, s>>>(m->pb, (bf16*)m->wpack); });
+    if (e == cudaSuccess) e = cudaMemsetAsync(m->tcErr, 0, sizeof(int), s);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(mlp_predict_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+    int dev = 0, sms = 0;
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    const long long tiles = (nPoints + kTcM - 1) / kTcM;
+    const unsigned grid = (unsigned)(tiles < sms ? tiles : sms);
+    mlp_predict_tc_kernel<<<grid, kTcThreads, kTcSmem, s>>>(f, nPoints, m->wpack, m->params, lleMean, lleStd, lle,
+                                                            cls, conf, m->tcErr);
+    note_launch();
+    e = cudaGetLastError();
+    int h = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, m->tcErr, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess && h) e = cudaErrorLaunchTimeout;
     return e;
 }
 

@@ -214,6 +214,13 @@ cbf_status cbf_mlp_train(cbf_mlp* mlp, const float* dX, const float* dYLle, cons
  * (argmax), confidence (softmax maximum); each output optional. */
 cbf_status cbf_mlp_predict(cbf_mlp* mlp, const float* dX, int64_t n, float lleMean, float lleStd,
                            float* dLle, int32_t* dCls, float* dConf, void* stream);
+/* The same outputs for every grid point 0..points-1 of a 2-D sweep of a 3-D
+ * system (the surrogate map's prediction step), features generated on the fly,
+ * one fused tcgen05 tensor-core kernel (mlp_tc.cuh). */
+cbf_status cbf_mlp_predict_grid(cbf_mlp* mlp, const cbf_job* job, float lleMean, float lleStd,
+                                double* dLle, int32_t* dCls, float* dConf, void* stream);
+/* The network's input features (4 FP32 per point) of grid points dIdx[0..n). */
+cbf_status cbf_mlp_grid_features(const cbf_job* job, const int64_t* dIdx, int64_t n, float* dX, void* stream);
 
 /* ---- surrogate-refined LLE + regime map -------------------------------- */
 /* No counterpart in the reference.  The plain method (CBF_TASK_LLE_REGIME)

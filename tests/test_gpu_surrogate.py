@@ -83,6 +83,47 @@ def test_mlp_predict_matches_forward(cbf, gpu_ok):
     assert np.allclose(conf.cpu().numpy(), 1.0 / pm.sum(axis=1), rtol=1e-5)
 
 
+@pytest.mark.parametrize("side,seed", [(37, 3), (256, 8)])
+def test_mlp_grid_prediction_tcgen05_matches_list_path(cbf, gpu_ok, side, seed):
+    """The fused tcgen05 grid kernel against the mma.sync GEMM path on the same
+    grid points and weights: the same BF16 rounding points, FP32 accumulation in
+    another order, so outputs agree to accumulation error (a rare BF16 rounding
+    flip of a hidden unit moves an output by ~1e-3), classes up to near-ties.
+    side 37: a ragged last tile of 128 points."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(seed)
+    net = cbf.Mlp(512, seed=seed)
+    p = M.init_params(seed)
+    off = M.offsets()
+    for b in ("b1", "b2", "b3", "b4"):
+        o, shape = off[b]
+        p[o:o + shape[0]] = rng.normal(scale=0.3, size=shape[0])
+    net.set_params(p.astype(np.float32))
+    job = cbf.make_job(task=cbf.TASK_LLE_REGIME, nPts=side, tMax=1.0, transientTime=1.0, regimeTime=1.0,
+                       **CHEN_REGIME)
+    n = side * side
+    idx = torch.arange(n, dtype=torch.int64, device="cuda")
+    X = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    cbf.grid_features(job, idx.data_ptr(), n, X.data_ptr())
+    want_l = torch.empty(n, dtype=torch.float32, device="cuda")
+    want_c = torch.empty(n, dtype=torch.int32, device="cuda")
+    want_f = torch.empty(n, dtype=torch.float32, device="cuda")
+    net.predict(X.data_ptr(), n, 0.25, 2.0, want_l.data_ptr(), want_c.data_ptr(), want_f.data_ptr())
+    got_l = torch.empty(n, dtype=torch.float64, device="cuda")
+    got_c = torch.empty(n, dtype=torch.int32, device="cuda")
+    got_f = torch.empty(n, dtype=torch.float32, device="cuda")
+    net.predict_grid(job, 0.25, 2.0, got_l.data_ptr(), got_c.data_ptr(), got_f.data_ptr())
+    torch.cuda.synchronize()
+    wl, wc, wf = want_l.cpu().numpy(), want_c.cpu().numpy(), want_f.cpu().numpy()
+    gl, gc, gf = got_l.cpu().numpy(), got_c.cpu().numpy(), got_f.cpu().numpy()
+    assert np.all(np.isfinite(gl)) and np.all((gc >= 0) & (gc < 16))
+    assert np.max(np.abs(gl - wl)) < 0.02, np.max(np.abs(gl - wl))
+    assert np.mean(np.abs(gl - wl)) < 1e-3
+    assert np.mean(gc == wc) >= 0.99, np.mean(gc == wc)
+    assert np.max(np.abs(gf - wf)) < 0.02
+    assert len(np.unique(wc)) > 1  # the comparison sees more than one class
+
+
 def test_mlp_training_reduces_loss(cbf, gpu_ok):
     torch = pytest.importorskip("torch")
     rng = np.random.default_rng(4)
