@@ -4,7 +4,7 @@
 // Included by mlp.cu inside its anonymous namespace (uses its constants,
 // point_features and silu).
 //
-// One persistent CTA per SM (256 threads, 192 KB of shared memory) takes tiles
+// One persistent CTA per SM (512 threads, 192 KB of shared memory) takes tiles
 // of 128 grid points:
 //   features (4 inputs, zero-padded to K = 16) -> A buffer
 //   layer 1: 1 MMA (K 16, N 256) | layers 2, 3: 16 MMAs (K 256, N 256)
@@ -24,7 +24,7 @@
 // memory, so each layer's copy is a plain contiguous bulk copy.
 
 constexpr int kTcM = 128;        // grid points per tile (MMA M, tensor-memory lanes)
-constexpr int kTcThreads = 256;  // 8 warps: two per tensor-memory lane quarter
+constexpr int kTcThreads = 512;  // 16 warps: four per tensor-memory lane quarter
 constexpr int kTcCols = 256;     // tensor-memory columns allocated (FP32 accumulator N = 256)
 constexpr int kTcN4 = 32;        // layer-4 MMA N: 17 outputs padded with zero rows
 constexpr uint32_t kTcABytes = kTcM * kHid * 2;      // 65536
@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const uint32_t tmem = *tslot;
 
     const int q = warp & 3;      // tensor-memory lane quarter: tile rows 32q .. 32q+31
-    const int half = warp >> 2;  // column half of the hidden-layer epilogues
+    const int part = warp >> 2;  // column quarter (64 columns) of the hidden-layer epilogues
     const int row = 32 * q + lane;
     const uint32_t laneBase = tmem + ((uint32_t)(32 * q) << 16);
     const unsigned char* wNext[4] = {wpack, wpack + kTcW1Bytes, wpack + kTcW1Bytes + kTcBBytes,
@@ -286,10 +286,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             }
             if (L < 3) {
                 fetch(L + 1);
-                // bias + SiLU of 128 columns of this thread's row, BF16 into A
+                // bias + SiLU of 64 columns of this thread's row, BF16 into A
                 const float* bL = bias[L];
-                for (int c = 0; c < 4; ++c) {
-                    const int col0 = half * 128 + c * 32;
+                for (int c = 0; c < 2; ++c) {
+                    const int col0 = part * 64 + c * 32;
                     float v[32];
                     tmem_ld32(laneBase + (uint32_t)col0, v);
                     uint32_t pk[16];
@@ -301,7 +301,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         *reinterpret_cast<uint4*>(A + tc_off(kTcM, row, col0 + 8 * i)) =
                             make_uint4(pk[4 * i], pk[4 * i + 1], pk[4 * i + 2], pk[4 * i + 3]);
                 }
-            } else if (half == 0) {
+            } else if (part == 0) {
                 // prediction head, as head_kernel
                 float v[32];
                 tmem_ld32(laneBase, v);
