@@ -3,8 +3,10 @@
 //
 // Output 0 is the (normalised) LLE, outputs 1..16 the logits of the 16-way
 // peak-count regime class.  Parameters live as FP32 masters (Adam state next to
-// them) plus BF16 copies that feed the tensor cores.  Every matrix product --
-// forward, input gradients, weight gradients -- goes through one tensor-core
+// them) plus BF16 copies that feed the tensor cores.  Prediction over a whole
+// grid runs as one fused tcgen05 kernel (mlp_tc.cuh).  Training and the
+// prediction of explicit feature rows put every matrix product -- forward,
+// input gradients, weight gradients -- through one tensor-core
 // GEMM: mma.sync m16n8k16 BF16 x BF16 -> FP32, 64x64 CTA tiles, operands staged
 // in shared memory in their memory order (k- or m/n-contiguous) by double-buffered
 // 16-byte cp.async copies and read with ldmatrix (.trans for m/n-contiguous
