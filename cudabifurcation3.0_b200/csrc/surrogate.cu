@@ -341,13 +341,13 @@ void cbf_surrogate_config_init(cbf_surrogate_config* c)
     c->trainSteps = 2500;
     c->lr = 2e-3f;
     c->wLle = 1.0f;
-    c->confThreshold = 0.5f;
+    c->confThreshold = 0.4f;
     c->auditFraction = 0.01f;
     c->boundaryRadius = 1;
     c->refine = 1;
     c->seed = 20240101ull;
     c->expandRadius = -1;
-    c->maxWaves = 20;
+    c->maxWaves = 12;
 }
 
 cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config* cfg, double* dLle,

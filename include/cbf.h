@@ -238,7 +238,7 @@ typedef struct cbf_surrogate_config {
     int32_t trainSteps;      /* Adam steps, cosine learning-rate decay over them (2500) */
     float lr;                /* peak learning rate (2e-3) */
     float wLle;              /* weight of the LLE squared error in the loss (1) */
-    float confThreshold;     /* recompute points whose softmax maximum is below it (0.5) */
+    float confThreshold;     /* recompute points whose softmax maximum is below it (0.4) */
     float auditFraction;     /* random audit sample of the grid, recomputed (0.01) */
     int32_t boundaryRadius;  /* a neighbour within this Chebyshev radius with another
                                 predicted class marks a boundary point (1) */
@@ -247,7 +247,7 @@ typedef struct cbf_surrogate_config {
     int32_t expandRadius;    /* neighbours within this radius of a point whose plain class
                                 differs from the prediction are recomputed next; -1 (default):
                                 ceil(nPts / 4096); 0: no expansion */
-    int32_t maxWaves;        /* recompute rounds that may mark expansions (20) */
+    int32_t maxWaves;        /* recompute rounds that may mark expansions (12) */
 } cbf_surrogate_config;
 void cbf_surrogate_config_init(cbf_surrogate_config* cfg);
 
