@@ -67,56 +67,31 @@ __device__ double lle_regime_point(const DevJob& J, long long g, double* pk, dou
         bool regimeDiv = false;
         int t = 0;  // step index since the transient
         for (; b < J.nRecord && t < J.regimeSteps; ++b) {
-            // Intervals overlapping the window: x and y advanced together, the
-            // peak stream fed before every x step, only the high words of |x0|,
-            // |y0| tracked.  If the divergence bound's high word was reached, the
-            // interval is replayed from its start (state, peak stream and window
-            // range restored) with the exact per-step test.
-            const int t0 = t;
-            double x0[D], y0[D];
-            copy_state<D>(x0, x[0]);
-            copy_state<D>(y0, y[0]);
-            const PeakStream ps0 = ps;
-            const double lo0 = lo, hi0 = hi;
-            unsigned mx = 0, my = 0;
+            // Intervals overlapping the window: the peak stream fed before every
+            // x step and the divergence test after every step; a trajectory's
+            // interval ends at its first failed test (loopCalculateDiscreteModel,
+            // cudaLibrary.cu:55-74).  The window is ~2 % of the steps, so it uses
+            // the exact per-step test directly instead of the run-then-replay
+            // scheme of the loop below, whose state snapshots would set the
+            // register count of the whole kernel.
+            bool ax = true, ay = true;
             for (int i = 0; i < J.nNT; ++i, ++t) {
-                if (t < J.regimeSteps) {
-                    const double v = pick<D>(x[0], J.writableVar);
-                    lo = fmin(lo, v);
-                    hi = fmax(hi, v);
-                    ps.push<true>(v, t, pk, iv, cap);
+                if (ax) {
+                    if (t < J.regimeSteps) {
+                        const double v = pick<D>(x[0], J.writableVar);
+                        lo = fmin(lo, v);
+                        hi = fmax(hi, v);
+                        ps.push<true>(v, t, pk, iv, cap);
+                    }
+                    S::step(x[0], c[0]);
+                    if (J.checkDiv && diverged(x[0][0], J.divThresh)) {
+                        ax = false;
+                        if (t < J.regimeSteps) regimeDiv = true;
+                    }
                 }
-                S::step(x[0], c[0]);
-                S::step(y[0], c[0]);
-                mx = max(mx, abs_hi(x[0][0]));
-                my = max(my, abs_hi(y[0][0]));
-            }
-            if (J.checkDiv && (mx >= J.divHi || my >= J.divHi)) {
-                copy_state<D>(x[0], x0);
-                copy_state<D>(y[0], y0);
-                ps = ps0;
-                lo = lo0;
-                hi = hi0;
-                t = t0;
-                bool ax = true, ay = true;
-                for (int i = 0; i < J.nNT; ++i, ++t) {
-                    if (ax) {
-                        if (t < J.regimeSteps) {
-                            const double v = pick<D>(x[0], J.writableVar);
-                            lo = fmin(lo, v);
-                            hi = fmax(hi, v);
-                            ps.push<true>(v, t, pk, iv, cap);
-                        }
-                        S::step(x[0], c[0]);
-                        if (J.checkDiv && diverged(x[0][0], J.divThresh)) {
-                            ax = false;
-                            if (t < J.regimeSteps) regimeDiv = true;
-                        }
-                    }
-                    if (ay) {
-                        S::step(y[0], c[0]);
-                        if (J.checkDiv && diverged(y[0][0], J.divThresh)) ay = false;
-                    }
+                if (ay) {
+                    S::step(y[0], c[0]);
+                    if (J.checkDiv && diverged(y[0][0], J.divThresh)) ay = false;
                 }
             }
             renorm();
@@ -132,7 +107,8 @@ __device__ double lle_regime_point(const DevJob& J, long long g, double* pk, dou
 }
 
 template <class S, bool IC>
-__global__ void __launch_bounds__(kRegThreads) lle_regime_kernel(const DevJob J, double* __restrict__ lle,
+// Six blocks per SM, like the autotuned LLE map kernel: 80 registers, no spill.
+__global__ void __launch_bounds__(kRegThreads, 6) lle_regime_kernel(const DevJob J, double* __restrict__ lle,
                                                                  int* __restrict__ cls, double* scrPk,
                                                                  double* scrIv, int bitWords, int sortCap,
                                                                  int* err)
