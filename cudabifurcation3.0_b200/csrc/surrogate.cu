@@ -338,7 +338,7 @@ void cbf_surrogate_config_init(cbf_surrogate_config* c)
     c->coarseSide = 512;
     c->randomPoints = 65536;
     c->batch = 4096;
-    c->trainSteps = 2500;
+    c->trainSteps = 1500;
     c->lr = 2e-3f;
     c->wLle = 1.0f;
     c->confThreshold = 0.4f;

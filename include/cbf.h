@@ -235,7 +235,7 @@ typedef struct cbf_surrogate_config {
     int32_t coarseSide;      /* training sub-grid side (512) */
     int32_t randomPoints;    /* extra random training points (65536) */
     int32_t batch;           /* training minibatch rows (4096) */
-    int32_t trainSteps;      /* Adam steps, cosine learning-rate decay over them (2500) */
+    int32_t trainSteps;      /* Adam steps, cosine learning-rate decay over them (1500) */
     float lr;                /* peak learning rate (2e-3) */
     float wLle;              /* weight of the LLE squared error in the loss (1) */
     float confThreshold;     /* recompute points whose softmax maximum is below it (0.4) */
