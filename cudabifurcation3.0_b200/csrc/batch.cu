@@ -112,10 +112,12 @@ __device__ __forceinline__ void run_tile(const DevJob& J, void* out, int* aux, l
 // WITH_M5: also dispatch the 5-D shipped model.  Its wider state raises the
 // register count of the whole kernel, so batches of 3-D systems use the
 // instantiation without it.
-// The LLE family is bounded to the occupancy of the autotuned LLE map kernel
-// (6 blocks of 128 threads per SM).
+// Both families are bounded to 6 blocks of 128 threads per SM (80 registers):
+// the occupancy of the autotuned LLE map kernel, and for the peak family 1.5x
+// what its register count would otherwise allow, which is worth the small
+// spill of its epilogue paths (batch64: 43.6 s instead of 49.2 s).
 template <int FAM, bool WITH_M5>
-__global__ void __launch_bounds__(kBatchThreads, FAM == kFamLle ? 6 : 1) batch_kernel(
+__global__ void __launch_bounds__(kBatchThreads, 6) batch_kernel(
     const BatchJob* __restrict__ jobs, int nJobs, const long long* __restrict__ tileEnd,
     unsigned long long* counter, double* scrPk, double* scrIv, int stride, int bitWords, int sortCap, int* err)
 {
