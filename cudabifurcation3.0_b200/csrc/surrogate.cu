@@ -347,7 +347,7 @@ void cbf_surrogate_config_init(cbf_surrogate_config* c)
     c->refine = 1;
     c->seed = 20240101ull;
     c->expandRadius = -1;
-    c->maxWaves = 12;
+    c->maxWaves = 20;
 }
 
 cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config* cfg, double* dLle,
@@ -503,9 +503,9 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
         frac >= 1.0 ? ~0ull : (unsigned long long)(frac * 18446744073709551616.0);
     const float thr = cfg->refine ? cfg->confThreshold : -1.0f;
     const int radius = cfg->refine ? cfg->boundaryRadius : 0;  // radius 0 marks no boundary
-    // expansion radius: automatic = one grid step per 4096 points of side, so
+    // expansion radius: automatic = one grid step per 8192 points of side, so
     // that the rounds needed to trace a structure grow slower than nPts
-    const int autoR = (nPts + 4095) / 4096;
+    const int autoR = (nPts + 8191) / 8192;
     const int er = cfg->refine ? (cfg->expandRadius < 0 ? autoR : cfg->expandRadius) : 0;
     unsigned char* lsur = nullptr;
     if ((e = buf.get(kSlotLsur, &lsur, nLab)) != cudaSuccess) return report_cuda_error(e, "label buffers");

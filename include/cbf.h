@@ -246,8 +246,8 @@ typedef struct cbf_surrogate_config {
     uint64_t seed;           /* training points, minibatches, weights and audit sample */
     int32_t expandRadius;    /* neighbours within this radius of a point whose plain class
                                 differs from the prediction are recomputed next; -1 (default):
-                                ceil(nPts / 4096); 0: no expansion */
-    int32_t maxWaves;        /* recompute rounds that may mark expansions (12) */
+                                ceil(nPts / 8192); 0: no expansion */
+    int32_t maxWaves;        /* recompute rounds that may mark expansions (20) */
 } cbf_surrogate_config;
 void cbf_surrogate_config_init(cbf_surrogate_config* cfg);
 
