@@ -106,8 +106,8 @@ __device__ double lle_regime_point(const DevJob& J, long long g, double* pk, dou
     return result / J.tMax;
 }
 
-template <class S, bool IC>
 // Six blocks per SM, like the autotuned LLE map kernel: 80 registers, no spill.
+template <class S, bool IC>
 __global__ void __launch_bounds__(kRegThreads, 6) lle_regime_kernel(const DevJob J, double* __restrict__ lle,
                                                                  int* __restrict__ cls, double* scrPk,
                                                                  double* scrIv, int bitWords, int sortCap,
