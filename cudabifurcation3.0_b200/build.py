@@ -12,6 +12,7 @@ from __future__ import annotations
 import argparse
 import os
 import shutil
+from concurrent.futures import ThreadPoolExecutor
 import subprocess
 import sys
 from pathlib import Path
@@ -55,7 +56,7 @@ def _stale(obj: Path, deps) -> bool:
 def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
     hdrs = headers()
-    objs = []
+    objs, cmds = [], []
     for src in sources():
         obj = BUILD / (src.name + ".o")
         objs.append(obj)
@@ -67,7 +68,16 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
                 cmd[1:1] = ["-x", "cu"]
             if verbose:
                 print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
+            cmds.append(cmd)
+    # translation units are independent: compile them concurrently
+    jobs = max(1, min(len(cmds), os.cpu_count() or 1))
+    with ThreadPoolExecutor(max_workers=jobs) as pool:
+        for r in pool.map(lambda c: subprocess.run(c, capture_output=ptxas_info, text=True), cmds):
+            if ptxas_info:
+                sys.stdout.write(r.stdout)
+                sys.stderr.write(r.stderr)
+            if r.returncode != 0:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     if force or _stale(LIB, objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs)]
         if verbose:

@@ -6,8 +6,12 @@
 // synchronisation, or an out-of-memory failure half-way through a run, is not
 // acceptable.  cbf_bifurcation2d_dbscan_noalloc serves them: the caller passes
 // the output buffer, and the per-warp peak/interval scratch the fused kernel
-// needs comes from one file-scope device array of fixed size, reserved when the
-// library's module is loaded and held by every GPU that loads it until exit.
+// needs comes from one file-scope device array of fixed size.  The array sits in
+// this translation unit's own module; under lazy module loading (the CUDA
+// default) a device reserves it at the first call made on that device -- the
+// address lookup loads the module -- so that first call can fail with out of
+// memory and belongs at start-up.  A device keeps the array until the process
+// exits.  Each call waits for its stream to finish, to read the error flag.
 //
 // The array is shared by every call: calls that overlap on the GPU (from several
 // host threads, or on several streams) race on it and must be serialised by the
@@ -33,7 +37,8 @@ void* g_scratch_addr[64];  // device address of g_noalloc_scratch, per device
 
 // Host code must not use g_noalloc_scratch directly: there it names a host-side
 // stand-in, not device memory.  The device address is looked up once per device,
-// with that device current, on the first call made on it.
+// with that device current, on the first call made on it, and cached; a
+// cudaDeviceReset invalidates the cached address.
 cbf_status scratch_address(void** out)
 {
     int dev = 0;

@@ -409,13 +409,19 @@ cbf_status cbf_csv_write_rows(const char* path, int32_t nPts, const double* rang
  * latency-critical loops that cannot afford an allocation's implicit
  * synchronisation or an out-of-memory failure mid-run.  Arguments as
  * cbf_bifurcation2d_dbscan (ic/ranges/indices/values are host arrays); d_out is
- * caller-owned device memory of nPts*nPts int32; runs on `stream` and returns
- * when the map is complete.  Scratch: a fixed 64 MiB device array inside the
- * library (held by every GPU that loads it until exit); maps whose
- * min(maxAmountOfPeaks, record/2) exceeds 32 767 peaks per point are rejected with
- * CBF_ERR_INVALID_ARG.  The first call on a device looks up the array's device
- * address, so make it before any stream capture.  All calls share the array:
- * calls that overlap on the GPU race and must be serialised by the caller. */
+ * caller-owned device memory of nPts*nPts int32; runs on `stream` (a
+ * cudaStream_t; NULL is the legacy default stream, as for cbf_run).  Every call
+ * waits on the host until its stream has finished the map, because it reads the
+ * kernel's error flag back.  Scratch: a fixed 64 MiB device array inside the
+ * library; maps whose min(maxAmountOfPeaks, record/2) exceeds 32 767 peaks per
+ * point are rejected with CBF_ERR_INVALID_ARG.  The first call on a device looks
+ * up the array's device address; with lazy module loading (the CUDA default)
+ * that first call is also when the device reserves the 64 MiB, so it can fail
+ * with CBF_ERR_OUT_OF_MEMORY: make it at start-up, before any stream capture.
+ * The device keeps the array until the process exits; the looked-up address is
+ * cached per device and does not survive a cudaDeviceReset.  All calls share
+ * the array: calls that overlap on the GPU race and must be serialised by the
+ * caller. */
 cbf_status cbf_bifurcation2d_dbscan_noalloc(int32_t system, double tMax, int32_t nPts, double h,
                                             int32_t amountOfInitialConditions,
                                             const double* initialConditions, const double* ranges,

@@ -89,11 +89,24 @@ def make_job(*, system, nPts, ranges, idxMut, ic, values, h, tMax=0.0, transient
     return j
 
 
+def reference_dir() -> Path | None:
+    """The reference checkout the Makefile's `ref` target compiles from (the
+    Makefile is the one place that locates it; CBF_REFERENCE_DIR overrides it),
+    or None when it is not present on this machine."""
+    try:
+        out = subprocess.run(["make", "-s", "-C", str(HERE), "ref-dir"], check=True,
+                             capture_output=True, text=True).stdout.strip()
+    except (OSError, subprocess.CalledProcessError):
+        return None
+    p = Path(out) if out else None
+    return p if p is not None and (p / "Library" / "cudaLibrary.cu").exists() else None
+
+
 def build(with_ref: bool | None = None) -> None:
     """Compile liboracle.so (and the reference shim when its sources are present)."""
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
     if with_ref is None:
-        with_ref = Path("/root/reference/Library/cudaLibrary.cu").exists()
+        with_ref = reference_dir() is not None
     if with_ref:
         subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
 

@@ -70,6 +70,26 @@ def test_noalloc_matches_regular_entry_point_twice(cbf, gpu_ok, eps):
     assert free_after >= free_before
 
 
+def test_noalloc_long_records_match_two_pass_entry_point(cbf, gpu_ok):
+    """Peak lists longer than the regular entry point's 1024-slot first pass.
+
+    h = 0.01 over 900 time units gives 985..2849 peaks per point; with
+    maxAmountOfPeaks 2500 the regular call computes some points in its first
+    pass, recomputes the 1025..2500-peak points in its second pass and returns
+    only the count-based result for the rest, while the no-allocation call runs
+    every point once at the full capacity of 2500.  The maps must be equal."""
+    torch = pytest.importorskip("torch")
+    p = dict(LORENZ, nPts=6, h=0.01, tMax=900.0, transient=20.0, maxPeaks=2500, eps=0.05)
+    n = p["nPts"] ** 2
+    out = torch.full((n,), -7, dtype=torch.int32, device="cuda")
+    s = torch.cuda.Stream()
+    for _ in range(2):
+        out.fill_(-7)
+        torch.cuda.synchronize()
+        cbf.check(_call_noalloc(cbf, p, out.data_ptr(), s.cuda_stream))
+        assert np.array_equal(out.cpu().numpy(), _regular(cbf, p))
+
+
 def test_noalloc_rejects_maps_beyond_its_scratch(cbf, gpu_ok):
     torch = pytest.importorskip("torch")
     # record 200 000 samples, maxAmountOfPeaks 100 000 -> 100 000 peaks per point > 32 767
