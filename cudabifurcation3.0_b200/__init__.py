@@ -50,6 +50,8 @@ EXPORTS = [
     "cbf_mlp_set_params", "cbf_mlp_forward_backward", "cbf_mlp_train", "cbf_mlp_predict",
     "cbf_mlp_predict_grid", "cbf_mlp_grid_features",
     "cbf_surrogate_config_init", "cbf_lle_map_surrogate", "cbf_surrogate_release", "cbf_ls1d", "cbf_ls2d",
+    "cbf_regime_rules_init", "cbf_lle2d_surrogate", "cbf_facade_set_system", "cbf_facade_set_output_path",
+    "cbf_facade_set_surrogate",
     "cbf_csv_write_rows", "cbf_npy_write", "cbf_ostrovsky2d", "cbf_modeling_one_system",
 ]
 
@@ -543,6 +545,64 @@ def lle_map_surrogate(job: Job, cfg: SurrogateConfig, d_lle: int, d_cls: int, d_
                                       C.c_void_p(d_pred or None), C.byref(rep),
                                       C.c_void_p(stream or None)))
     return rep
+
+
+class RegimeRules(C.Structure):
+    """Mirror of ``cbf_regime_rules`` (include/cbf.h)."""
+    _fields_ = [
+        ("regimeTime", C.c_double),
+        ("maxAmountOfPeaks", C.c_int32),
+        ("dbscanEps", C.c_double),
+        ("regimeMinAmp", C.c_double),
+        ("regimeChaosLle", C.c_double),
+        ("flags", C.c_uint32),
+    ]
+
+
+def regime_rules(**kw) -> RegimeRules:
+    """Defaults of cbf_regime_rules_init, overridden by keyword."""
+    r = RegimeRules()
+    L = lib()
+    L.cbf_regime_rules_init.argtypes = [C.POINTER(RegimeRules)]
+    L.cbf_regime_rules_init.restype = None
+    L.cbf_regime_rules_init(C.byref(r))
+    for k, v in kw.items():
+        if not hasattr(r, k):
+            raise AttributeError(k)
+        setattr(r, k, v)
+    return r
+
+
+def LLE2D_surrogate(tMax, NT, nPts, h, eps, initialConditions, amountOfInitialConditions, ranges,
+                    indicesOfMutVars, writableVar, maxValue, transientTime, values, amountOfValues, *,
+                    system="memristive5", seedChunk=None, rules=None, config=None, out_lle=None,
+                    out_cls=None):
+    """LLE2D's arguments, surrogate-refined (cbf_lle2d_surrogate): returns (lle[nPts, nPts],
+    class[nPts, nPts], report).  seedChunk defaults to LLE2D's min(points, 200000);
+    out_lle / out_cls (optional, float64 / int32 with nPts^2 elements) receive the maps."""
+    ic, icp = _d(initialConditions)
+    r, rp = _d(ranges)
+    ix, ixp = _i(indicesOfMutVars)
+    v, vp = _d(values)
+    n = nPts * nPts
+    lle = out_lle if out_lle is not None else np.empty(n, np.float64)
+    cls = out_cls if out_cls is not None else np.empty(n, np.int32)
+    assert lle.dtype == np.float64 and lle.size == n and lle.flags.c_contiguous
+    assert cls.dtype == np.int32 and cls.size == n and cls.flags.c_contiguous
+    chunk = min(n, 200000) if seedChunk is None else seedChunk
+    rep = SurrogateReport()
+    L = lib()
+    L.cbf_lle2d_surrogate.restype = C.c_int32
+    L.cbf_lle2d_surrogate.argtypes = [C.c_int32, C.c_double, C.c_double, C.c_int32, C.c_double, C.c_double,
+                                      _dp, C.c_int32, _dp, _ip, C.c_int32, C.c_double, C.c_double, _dp,
+                                      C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p]
+    check(L.cbf_lle2d_surrogate(_sys(system), tMax, NT, nPts, h, eps, icp, amountOfInitialConditions, rp,
+                                ixp, writableVar, maxValue, transientTime, vp, amountOfValues, chunk,
+                                C.byref(rules) if rules is not None else None,
+                                C.byref(config) if config is not None else None,
+                                lle.ctypes.data, cls.ctypes.data, C.byref(rep)))
+    return lle.reshape(nPts, nPts), cls.reshape(nPts, nPts), rep
 
 
 def set_lle_variant(system, variant: int) -> None:

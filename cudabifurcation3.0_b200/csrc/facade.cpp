@@ -60,6 +60,17 @@ int current_system()
     return s;
 }
 
+// Surrogate-refined LLE2D: -1 = the environment's CBF_SURROGATE decides.
+std::atomic<int> g_surrogate{-1};
+
+bool surrogate_enabled()
+{
+    const int v = g_surrogate.load();
+    if (v >= 0) return v != 0;
+    const char* e = getenv("CBF_SURROGATE");
+    return e && *e && strcmp(e, "0") != 0;
+}
+
 std::string current_path()
 {
     std::lock_guard<std::mutex> lk(g_path_mu);
@@ -363,6 +374,17 @@ void lle_common(int variant, double tMax, double NT, int nPts, double h, double 
     const long long total = dims == 2 ? (long long)nPts * nPts : nPts;
     std::vector<double> res((size_t)(total > 0 ? total : 0));
     const long long seedChunk = reference_seed_chunk(variant, tMax, NT, nPts);
+    if (variant == 2 && surrogate_enabled()) {
+        // the opt-in surrogate-refined map (same grid, seeds and layout) plus its classes
+        std::vector<int32_t> cls((size_t)(total > 0 ? total : 0));
+        CBF_CHECK(cbf_lle2d_surrogate(current_system(), tMax, NT, nPts, h, eps, icv, nIC, ranges, idx, wv,
+                                      maxValue, transientTime, values, nV, seedChunk, nullptr, nullptr,
+                                      res.data(), cls.data(), nullptr));
+        const std::string path = current_path();
+        io_check(cbf_csv_write_map(path.c_str(), res.data(), 1, total, nPts, ranges, 6));
+        io_check(cbf_csv_write_map((path + ".regime.csv").c_str(), cls.data(), 0, total, nPts, ranges, 6));
+        return;
+    }
     cbf_status st;
     if (dims == 1)
         st = (ic ? cbf_lle1d_ic : cbf_lle1d)(current_system(), tMax, NT, nPts, h, eps, icv, nIC, ranges,
@@ -615,6 +637,8 @@ void LS2D(const double tMax, const double NT, const int nPts, const double h, co
 
 void cbfSetSystem(int system) { g_system.store(system); }
 int cbfGetSystem() { return current_system(); }
+void cbfSetSurrogate(int enable) { g_surrogate.store(enable < 0 ? -1 : (enable ? 1 : 0)); }
+int cbfGetSurrogate() { return surrogate_enabled() ? 1 : 0; }
 
 void cbfSetOutputPath(const char* path)
 {
@@ -758,6 +782,7 @@ extern "C" cbf_status cbf_csv_write_rows(const char* path, int32_t nPts, const d
 // C-callable access to the facade for bindings without C++ name mangling
 // (ctypes, cgo): same arguments as the C++ functions above.
 extern "C" {
-void cbf_facade_set_system(int32_t system) { cbfSetSystem(system); }
+void cbf_facade_set_system(int system) { cbfSetSystem(system); }
 void cbf_facade_set_output_path(const char* path) { cbfSetOutputPath(path); }
+void cbf_facade_set_surrogate(int enable) { cbfSetSurrogate(enable); }
 }

@@ -324,6 +324,24 @@ constexpr int kMaxDevices = 64;
 Workspace g_ws[kMaxDevices];
 std::mutex g_ws_mu[kMaxDevices];
 
+// Device copies of the refined map for the host-buffer entry point, kept per
+// device between calls like the workspace.
+struct HostMapBuffers {
+    double* lle = nullptr;
+    int* cls = nullptr;
+    long long n = 0;
+    void release()
+    {
+        if (lle) cudaFree(lle);
+        if (cls) cudaFree(cls);
+        lle = nullptr;
+        cls = nullptr;
+        n = 0;
+    }
+};
+HostMapBuffers g_hostMap[kMaxDevices];
+std::mutex g_hostMap_mu[kMaxDevices];
+
 }  // namespace
 }  // namespace cbf
 
@@ -637,10 +655,106 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
     return CBF_OK;
 }
 
+void cbf_regime_rules_init(cbf_regime_rules* r)
+{
+    if (!r) return;
+    memset(r, 0, sizeof(*r));
+    r->regimeTime = 50.0;
+    r->maxAmountOfPeaks = 512;
+    r->dbscanEps = 0.02;
+    r->regimeMinAmp = 1e-6;
+    r->regimeChaosLle = 0.05;
+    r->flags = 0;
+}
+
+// LLE2D's arguments (hostLibrary.cu:1524-1663) plus the regime rules and the
+// surrogate configuration; the refined map is computed into cached device
+// buffers on the library's stream and copied into the caller's host arrays.
+cbf_status cbf_lle2d_surrogate(int32_t system, double tMax, double NT, int32_t nPts, double h, double eps,
+                               const double* initialConditions, int32_t amountOfInitialConditions,
+                               const double* ranges, const int32_t* indicesOfMutVars, int32_t writableVar,
+                               double maxValue, double transientTime, const double* values,
+                               int32_t amountOfValues, int64_t seedChunk, const cbf_regime_rules* rules,
+                               const cbf_surrogate_config* cfg, double* outLle, int32_t* outCls,
+                               cbf_surrogate_report* report)
+{
+    if (!initialConditions || !ranges || !indicesOfMutVars || !values || !outLle)
+        return report_error(CBF_ERR_INVALID_ARG, "null argument");
+    if (amountOfInitialConditions < 1 || amountOfInitialConditions > CBF_MAX_DIM || amountOfValues < 1 ||
+        amountOfValues > CBF_MAX_VALUES)
+        return report_error(CBF_ERR_INVALID_ARG, "amountOfInitialConditions/amountOfValues out of range");
+    cbf_regime_rules r;
+    if (rules) r = *rules;
+    else cbf_regime_rules_init(&r);
+    cbf_surrogate_config c;
+    if (cfg) c = *cfg;
+    else cbf_surrogate_config_init(&c);
+    cbf_job j;
+    cbf_job_init(&j);
+    j.task = CBF_TASK_LLE_REGIME;
+    j.system = system;
+    j.dims = 2;
+    j.nPts = nPts;
+    j.h = h;
+    j.tMax = tMax;
+    j.NT = NT;
+    j.lleEps = eps;
+    j.transientTime = transientTime;
+    j.maxValue = maxValue;
+    j.writableVar = writableVar;
+    j.seedChunk = seedChunk;
+    j.nIC = amountOfInitialConditions;
+    j.nV = amountOfValues;
+    for (int i = 0; i < j.nIC; ++i) j.ic[i] = initialConditions[i];
+    for (int i = 0; i < j.nV; ++i) j.values[i] = values[i];
+    for (int i = 0; i < 4; ++i) j.ranges[i] = ranges[i];
+    j.idxMut[0] = indicesOfMutVars[0];
+    j.idxMut[1] = indicesOfMutVars[1];
+    j.regimeTime = r.regimeTime;
+    j.maxAmountOfPeaks = r.maxAmountOfPeaks;
+    j.dbscanEps = r.dbscanEps;
+    j.regimeMinAmp = r.regimeMinAmp;
+    j.regimeChaosLle = r.regimeChaosLle;
+    j.flags = r.flags;
+    cbf_status st = cbf_validate(&j);
+    if (st != CBF_OK) return st;
+
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+        return report_error(CBF_ERR_INVALID_ARG, "no usable current device");
+    cudaStream_t s = nullptr;
+    if ((st = library_default_stream(&s)) != CBF_OK) return st;
+    const long long n = (long long)nPts * nPts;
+    std::lock_guard<std::mutex> lk(g_hostMap_mu[dev]);
+    HostMapBuffers& hm = g_hostMap[dev];
+    if (hm.n < n) {
+        hm.release();
+        cudaError_t e = cudaMalloc((void**)&hm.lle, (size_t)n * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&hm.cls, (size_t)n * sizeof(int));
+        if (e != cudaSuccess) {
+            hm.release();
+            return report_cuda_error(e, "refined map buffers");
+        }
+        hm.n = n;
+    }
+    if ((st = cbf_lle_map_surrogate(&j, &c, hm.lle, hm.cls, nullptr, nullptr, nullptr, report, s)) != CBF_OK)
+        return st;
+    cudaError_t e = cudaMemcpyAsync(outLle, hm.lle, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && outCls)
+        e = cudaMemcpyAsync(outCls, hm.cls, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return report_cuda_error(e, "refined map readback");
+    return CBF_OK;
+}
+
 void cbf_surrogate_release(void)
 {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return;
+    {
+        std::lock_guard<std::mutex> lk(g_hostMap_mu[dev]);
+        g_hostMap[dev].release();
+    }
     std::lock_guard<std::mutex> lk(g_ws_mu[dev]);
     g_ws[dev].release();
 }

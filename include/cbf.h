@@ -282,6 +282,40 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
  * this frees them for the current device. */
 void cbf_surrogate_release(void);
 
+/* The plain method's regime-class rules (CBF_TASK_LLE_REGIME fields): the class
+ * of a point comes from the peaks of x[writableVar] during the first
+ * regimeTime time units after the transient. */
+typedef struct cbf_regime_rules {
+    double regimeTime;         /* window after the transient (50) */
+    int32_t maxAmountOfPeaks;  /* more peaks than this -> class 15 (512) */
+    double dbscanEps;          /* DBSCAN radius on (peak, interval) (0.02) */
+    double regimeMinAmp;       /* window range below this -> class 0 (1e-6) */
+    double regimeChaosLle;     /* LLE above this -> class 15 (0.05) */
+    uint32_t flags;            /* 0: the grid of LLE2D, getValueByIdx's FP32 index
+                                  (cudaLibrary.cu:210-216); CBF_FLAG_EXACT_GRID:
+                                  integer grid cells (differ from LLE2D's above 2^24
+                                  points, i.e. at 8192^2) (0) */
+} cbf_regime_rules;
+void cbf_regime_rules_init(cbf_regime_rules* rules);
+
+/* Host-buffer form of the surrogate-refined map: LLE2D's arguments
+ * (hostLibrary.cu:1524-1663; seedChunk as for cbf_lle2d), the regime rules
+ * (NULL: the defaults above) and the surrogate configuration (NULL: the
+ * defaults of cbf_surrogate_config_init).  outLle double[nPts^2] and outCls
+ * int32[nPts^2] (optional) are host arrays.  Labelled and recomputed points
+ * carry plain FP64 values; the others carry the network's prediction, whose
+ * error the report's audit fields estimate.  Runs on the library's stream and
+ * returns when the map is in the host arrays; device buffers are cached per
+ * device between calls (cbf_surrogate_release frees them).  The C++ facade's
+ * LLE2D writes this map when cbfSetSurrogate(1) or CBF_SURROGATE=1 is set. */
+cbf_status cbf_lle2d_surrogate(int32_t system, double tMax, double NT, int32_t nPts, double h, double eps,
+                               const double* initialConditions, int32_t amountOfInitialConditions,
+                               const double* ranges, const int32_t* indicesOfMutVars, int32_t writableVar,
+                               double maxValue, double transientTime, const double* values,
+                               int32_t amountOfValues, int64_t seedChunk, const cbf_regime_rules* rules,
+                               const cbf_surrogate_config* cfg, double* outLle, int32_t* outCls,
+                               cbf_surrogate_report* report);
+
 /* ---- host-buffer entry points (drop-in for hostLibrary.cuh) ---------- */
 /* bifurcation1D, hostLibrary.cuh:29-42 / hostLibrary.cu:7-158.
  * outPeaks[k*peakCapacity + j], outCounts[k]; peakCapacity >= record/2. */

@@ -134,4 +134,19 @@ int cbfGetSystem();
 void cbfSetOutputPath(const char* path);  // nullptr restores the default
 const char* cbfGetOutputPath();
 
+// Opt-in, no counterpart in the reference: with cbfSetSurrogate(1) (or the
+// environment variable CBF_SURROGATE=1; cbfSetSurrogate(-1) returns to the
+// environment's choice) LLE2D writes the surrogate-refined LLE map of
+// cbf_lle2d_surrogate (cbf.h) -- same grid, seeds, header and layout -- and the
+// regime classes beside it in "<path>.regime.csv" (same layout, integers).
+void cbfSetSurrogate(int enable);
+int cbfGetSurrogate();
+
+// The same settings for bindings without C++ name mangling (ctypes, cgo).
+extern "C" {
+void cbf_facade_set_system(int system);
+void cbf_facade_set_output_path(const char* path);
+void cbf_facade_set_surrogate(int enable);
+}
+
 #endif  // CBF_HOST_LIBRARY_H

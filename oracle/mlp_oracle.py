@@ -140,3 +140,46 @@ def init_params(seed):
         cnt = int(np.prod(shape))
         p[o:o + cnt] = [np.float32(rnd() * bound) for _ in range(cnt)]
     return p
+
+
+# ---------------------------------------------------------------------------
+# Grid prediction (the surrogate map's prediction step), restated.
+
+SYSTEM_FEATURE = {1: -1.0, 2: 0.0, 3: 1.0}  # Rossler, Lorenz, Chen
+
+
+def grid_features(system, nPts, ranges, idxMut, values, grid_values):
+    """The network's 4 FP32 inputs of grid points whose two swept parameters are
+    grid_values[:, 0] and grid_values[:, 1] (doubles): the system code, each
+    swept parameter mapped to [-1, 1] as ((float)p - lo) * (2 / (hi - lo)) - 1 in
+    FP32, and the first unswept parameter of values[1..3] divided by 10."""
+    f32 = np.float32
+    lo0, lo1 = f32(ranges[0]), f32(ranges[2])
+    inv0 = f32(2.0 / (ranges[1] - ranges[0])) if ranges[1] != ranges[0] else f32(0)
+    inv1 = f32(2.0 / (ranges[3] - ranges[2])) if ranges[3] != ranges[2] else f32(0)
+    third = 1
+    while third in idxMut:
+        third += 1
+    t = f32(values[third] * 0.1) if third < 4 else f32(0)
+    g = np.asarray(grid_values, np.float64)
+    x = np.empty((len(g), K_IN), np.float32)
+    x[:, 0] = f32(SYSTEM_FEATURE[system])
+    x[:, 1] = (g[:, 0].astype(np.float32) - lo0) * inv0 - f32(1)
+    x[:, 2] = (g[:, 1].astype(np.float32) - lo1) * inv1 - f32(1)
+    x[:, 3] = t
+    return x
+
+
+def predict(params, x, lle_mean, lle_std):
+    """Forward pass with the kernels' BF16 rounding points (exact accumulation):
+    (LLE = out0 * std + mean, class = argmax of out1..16, softmax maximum,
+    the raw outputs (n, 17), the gap between the two largest logits)."""
+    n = len(x)
+    _, _, out = forward_backward(params, x, np.zeros(n), np.zeros(n, np.int64), 1.0, bf16_round=True)
+    logits = out[:, 1:]
+    cls = logits.argmax(axis=1)
+    srt = np.sort(logits, axis=1)
+    margin = srt[:, -1] - srt[:, -2]
+    pm = np.exp(logits - logits.max(axis=1, keepdims=True))
+    conf = 1.0 / pm.sum(axis=1)
+    return out[:, 0] * lle_std + lle_mean, cls, conf, out, margin

@@ -28,6 +28,16 @@ double orc_get_value_by_idx(int idx, int nPts, double startRange, double finishR
     return startRange + (double)cell * ((double)(finishRange - startRange) / (double)(nPts - 1));
 }
 
+/* The library's exact-grid option: the cell is the integer quotient, the value
+ * formula is getValueByIdx's. */
+static double exact_value_by_idx(int64_t idx, int nPts, double startRange, double finishRange,
+                                 int valueNumber)
+{
+    const int64_t d = valueNumber == 0 ? 1 : (int64_t)nPts;
+    const int cell = (int)((idx / d) % nPts);
+    return startRange + (double)cell * ((double)(finishRange - startRange) / (double)(nPts - 1));
+}
+
 /* ------------------------------------------------------------------------- */
 /* Model steps.  One fixed-step CD (semi-implicit composition) step: an explicit
  * half with k = h*s in reverse variable order, then a linearly implicit half with
@@ -393,8 +403,10 @@ static void setup_point(const orc_job* job, int64_t g, double* x, double* v)
     for (int i = 0; i < job->nV; ++i)
         v[i] = job->values[i];
     for (int i = 0; i < job->dims; ++i) {
-        double p = orc_get_value_by_idx((int)g, job->nPts, job->ranges[i * 2],
-                                        job->ranges[i * 2 + 1], i);
+        double p = job->exactGrid
+                       ? exact_value_by_idx(g, job->nPts, job->ranges[i * 2], job->ranges[i * 2 + 1], i)
+                       : orc_get_value_by_idx((int)g, job->nPts, job->ranges[i * 2],
+                                              job->ranges[i * 2 + 1], i);
         if (job->sweepIC)
             x[job->idxMut[i]] = p;
         else
@@ -959,5 +971,16 @@ int orc_map_lle_list(const orc_job* job, const int64_t* idx, int64_t count, doub
 #pragma omp parallel for schedule(dynamic, 1) num_threads(threads_or_default(nThreads))
     for (int64_t k = 0; k < count; ++k)
         out[k] = orc_lle_point(job, idx[k]);
+    return 0;
+}
+
+int orc_map_lle_list_seeded(const orc_job* job, const int64_t* idx, int64_t count, const double* z,
+                            double* out, int nThreads)
+{
+    if ((int)(job->tMax / job->NT) <= 0 || job->nIC <= 0)
+        return -1;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads_or_default(nThreads))
+    for (int64_t k = 0; k < count; ++k)
+        out[k] = orc_lle_point_seeded(job, idx[k], z ? z + k * job->nIC : NULL);
     return 0;
 }

@@ -65,6 +65,8 @@ typedef struct orc_job {
     double regimeMinAmp; /* LLE + regime: window range below this -> class 0 */
     double regimeChaosLle; /* LLE + regime: > 0 and LLE above it -> class 15 */
     double ostrovskyThreshold; /* periodicity classifier threshold */
+    int32_t exactGrid; /* 1: grid cell by integer division (the library's CBF_FLAG_EXACT_GRID)
+                          instead of getValueByIdx's FP32 index */
 } orc_job;
 
 /* cudaLibrary.cu:210-216 */
@@ -125,6 +127,9 @@ int orc_map_lle_seeded(const orc_job* job, int64_t first, int64_t count, const d
                        double* out, int nThreads);
 /* Same, over an explicit list of global indices (strided samples for the CPU baseline). */
 int orc_map_lle_list(const orc_job* job, const int64_t* idx, int64_t count, double* out, int nThreads);
+/* The list form with per-point seeds z[k*nIC + i] (NULL: the oracle's own seeds). */
+int orc_map_lle_list_seeded(const orc_job* job, const int64_t* idx, int64_t count, const double* z,
+                            double* out, int nThreads);
 
 /* LLE plus peak-count regime class (the library's plain labelling method): the
  * LLE of orc_lle_point_seeded; x[writableVar] recorded before every step of the

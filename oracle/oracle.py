@@ -52,6 +52,7 @@ class OrcJob(C.Structure):
         ("regimeMinAmp", C.c_double),
         ("regimeChaosLle", C.c_double),
         ("ostrovskyThreshold", C.c_double),
+        ("exactGrid", C.c_int32),
     ]
 
 
@@ -59,7 +60,9 @@ def make_job(*, system, nPts, ranges, idxMut, ic, values, h, tMax=0.0, transient
              maxValue=0.0, writableVar=0, preScaller=1, sweepIC=False, maxAmountOfPeaks=0,
              kdeSampling=0, kdeI1=0.0, kdeI2=0.0, kdeH=0.0, dbscanEps=0.0, NT=0.0,
              lleEps=0.0, seedChunk=0, regimeTime=0.0, regimeMinAmp=0.0,
-             regimeChaosLle=0.0, ostrovskyThreshold=0.0) -> OrcJob:
+             regimeChaosLle=0.0, ostrovskyThreshold=0.0, flags=0, exactGrid=False) -> OrcJob:
+    """flags: the library's job flags; bit 0 (exact grid) selects integer grid
+    cells, the other bits do not concern the per-point code."""
     j = OrcJob()
     dims = len(idxMut)
     j.system = SYSTEMS[system] if isinstance(system, str) else int(system)
@@ -86,6 +89,7 @@ def make_job(*, system, nPts, ranges, idxMut, ic, values, h, tMax=0.0, transient
     j.regimeMinAmp = regimeMinAmp
     j.regimeChaosLle = regimeChaosLle
     j.ostrovskyThreshold = ostrovskyThreshold
+    j.exactGrid = 1 if (exactGrid or (int(flags) & 1)) else 0
     return j
 
 
@@ -189,6 +193,8 @@ def lib():
                                               _ip, C.c_int]
         L.orc_map_lle_list.restype = C.c_int
         L.orc_map_lle_list.argtypes = [C.POINTER(OrcJob), _lp, C.c_int64, _dp, C.c_int]
+        L.orc_map_lle_list_seeded.restype = C.c_int
+        L.orc_map_lle_list_seeded.argtypes = [C.POINTER(OrcJob), _lp, C.c_int64, C.c_void_p, _dp, C.c_int]
         _lib = L
     return _lib
 
@@ -412,10 +418,16 @@ def map_lle_regime(job: OrcJob, idx, z=None, threads: int = 0):
     return lle, cls
 
 
-def map_lle_list(job: OrcJob, idx, threads: int = 0):
+def map_lle_list(job: OrcJob, idx, threads: int = 0, z=None):
+    """LLE at grid indices idx; z (optional, nIC per point) replaces the seeds."""
     idx = np.ascontiguousarray(idx, dtype=np.int64)
     out = np.zeros(len(idx), np.float64)
-    rc = lib().orc_map_lle_list(C.byref(job), idx, len(idx), out, threads)
+    if z is not None:
+        z = np.ascontiguousarray(z, dtype=np.float64)
+        rc = lib().orc_map_lle_list_seeded(C.byref(job), idx, len(idx), z.ctypes.data_as(C.c_void_p),
+                                           out, threads)
+    else:
+        rc = lib().orc_map_lle_list(C.byref(job), idx, len(idx), out, threads)
     if rc != 0:
         raise RuntimeError(f"orc_map_lle_list failed: {rc}")
     return out

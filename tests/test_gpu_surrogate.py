@@ -210,3 +210,69 @@ def test_surrogate_rejects_bad_jobs(cbf, gpu_ok):
                        regimeTime=1.0, **dict(CHEN_REGIME, system="memristive5"))
     with pytest.raises(cbf.CbfError):
         cbf.lle_map_surrogate(job, cfg, 1, 1)
+
+
+def test_host_entry_point_returns_the_device_map(cbf, gpu_ok):
+    """cbf_lle2d_surrogate (LLE2D's arguments, host arrays) gives the map of the
+    device entry point cbf_lle_map_surrogate for the same job and configuration."""
+    torch = pytest.importorskip("torch")
+    side = 384
+    kw = dict(CHEN_REGIME, **SMALL)
+    job = cbf.make_job(task=cbf.TASK_LLE_REGIME, nPts=side, **kw)
+    cfg = cbf.surrogate_config(**SMALL_CFG)
+    n = side * side
+    d_lle = torch.empty(n, dtype=torch.float64, device="cuda")
+    d_cls = torch.empty(n, dtype=torch.int32, device="cuda")
+    rep = cbf.lle_map_surrogate(job, cfg, d_lle.data_ptr(), d_cls.data_ptr())
+    torch.cuda.synchronize()
+    rules = cbf.regime_rules(regimeTime=kw["regimeTime"], maxAmountOfPeaks=kw["maxAmountOfPeaks"],
+                             dbscanEps=kw["dbscanEps"], regimeMinAmp=kw["regimeMinAmp"],
+                             regimeChaosLle=kw["regimeChaosLle"], flags=cbf.FLAG_EXACT_GRID)
+    hl, hc, hrep = cbf.LLE2D_surrogate(kw["tMax"], kw["NT"], side, kw["h"], kw["lleEps"], kw["ic"], 3, kw["ranges"],
+                                       kw["idxMut"], 0, kw["maxValue"], kw["transientTime"], kw["values"], 4,
+                                       system="chen", seedChunk=kw["seedChunk"], rules=rules, config=cfg)
+    assert np.array_equal(hl.ravel(), d_lle.cpu().numpy(), equal_nan=True)
+    assert np.array_equal(hc.ravel(), d_cls.cpu().numpy())
+    assert (hrep.refined, hrep.labelled, hrep.waves) == (rep.refined, rep.labelled, rep.waves)
+
+
+def test_facade_lle2d_writes_the_refined_map_when_opted_in(cbf, gpu_ok, tmp_path, monkeypatch):
+    """The reference-named LLE2D (mangled C++ symbol) with CBF_SURROGATE=1 writes
+    the surrogate-refined map of cbf_lle2d_surrogate with the default rules and
+    configuration -- LLE2D's grid (FP32 index), seed chunk (200000), header and
+    precision -- and the classes in <path>.regime.csv; without it, the plain map."""
+    import ctypes as C
+
+    from test_abi import _ref_map_csv
+    side, tMax, NT, h, eps, tr = 1024, 20.0, 0.5, 0.002, 1e-8, 10.0
+    ic = np.array([0.1, 0.1, 0.1])
+    ranges = np.array([30.0, 45.0, 20.0, 30.0])
+    idx = np.array([1, 3], np.int32)
+    vals = np.array([0.5, 35.0, 3.0, 28.0])
+    L = cbf.lib()
+    f = L._Z5LLE2DddiddPKdiS0_PKiiddS0_i
+    f.restype = None
+    f.argtypes = [C.c_double, C.c_double, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_int, C.c_void_p,
+                  C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_int]
+    path = tmp_path / "lle.csv"
+    monkeypatch.setenv("CBF_OUT_FILE_PATH", str(path))
+    monkeypatch.setenv("CBF_SURROGATE", "1")
+    L.cbf_facade_set_output_path(None)
+    L.cbf_facade_set_system(cbf.SYS_CHEN)
+    try:
+        f(tMax, NT, side, h, eps, ic.ctypes.data, 3, ranges.ctypes.data, idx.ctypes.data, 0, 1e4, tr,
+          vals.ctypes.data, 4)
+        got = path.read_bytes()
+        got_cls = (tmp_path / "lle.csv.regime.csv").read_bytes()
+        lle, cls, rep = cbf.LLE2D_surrogate(tMax, NT, side, h, eps, ic, 3, ranges, idx, 0, 1e4, tr, vals, 4,
+                                            system="chen")
+        assert 0 < rep.refined and rep.labelled < side * side  # the network predicted part of the map
+        assert got == _ref_map_csv(lle.ravel().tolist(), side, list(ranges), 6, True)
+        assert got_cls == _ref_map_csv(cls.ravel().tolist(), side, list(ranges), 6, False)
+        monkeypatch.setenv("CBF_SURROGATE", "0")
+        f(tMax, NT, side, h, eps, ic.ctypes.data, 3, ranges.ctypes.data, idx.ctypes.data, 0, 1e4, tr,
+          vals.ctypes.data, 4)
+        plain = cbf.LLE2D(tMax, NT, side, h, eps, ic, 3, ranges, idx, 0, 1e4, tr, vals, 4, system="chen")
+        assert path.read_bytes() == _ref_map_csv(plain.ravel().tolist(), side, list(ranges), 6, True)
+    finally:
+        L.cbf_facade_set_system(-1)
