@@ -1,5 +1,6 @@
 """C-ABI library checks that need no GPU: load, exports, validation, host logic."""
 import ctypes as C
+import math
 import re
 import subprocess
 from pathlib import Path
@@ -139,8 +140,14 @@ def test_divergence_threshold_is_exact(cbf, orc):
 
 
 def _ref_map_csv(values, nPts, header, precision, is_double):
-    """The reference's ostream output (hostLibrary.cu:474-546), restated in Python."""
-    fmt = (lambda v: "%.*g" % (precision, v)) if is_double else (lambda v: "%d" % v)
+    """The reference's ostream output (hostLibrary.cu:474-546), restated in Python.
+    glibc prints a NaN with its sign bit set as "-nan"; Python's %g drops the sign."""
+    def fmt_double(v):
+        if math.isnan(v):
+            return "-nan" if math.copysign(1.0, v) < 0 else "nan"
+        return "%.*g" % (precision, v)
+
+    fmt = fmt_double if is_double else (lambda v: "%d" % v)
     s = []
     if header is not None:
         g = lambda v: "%.*g" % (precision, v)  # noqa: E731
