@@ -51,7 +51,7 @@ EXPORTS = [
     "cbf_mlp_predict_grid", "cbf_mlp_grid_features",
     "cbf_surrogate_config_init", "cbf_lle_map_surrogate", "cbf_surrogate_release", "cbf_ls1d", "cbf_ls2d",
     "cbf_regime_rules_init", "cbf_lle2d_surrogate", "cbf_facade_set_system", "cbf_facade_set_output_path",
-    "cbf_facade_set_surrogate",
+    "cbf_facade_set_surrogate", "cbf_job_scaled_step",
     "cbf_csv_write_rows", "cbf_npy_write", "cbf_ostrovsky2d", "cbf_modeling_one_system",
 ]
 

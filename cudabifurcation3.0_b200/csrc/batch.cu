@@ -156,8 +156,18 @@ __global__ void __launch_bounds__(kBatchThreads, 6) batch_kernel(
                 if (WITH_M5) run_tile<Memristive5, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err);
                 break;
             case CBF_SYS_ROSSLER: run_tile<Rossler, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err); break;
-            case CBF_SYS_LORENZ: run_tile<Lorenz, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err); break;
-            case CBF_SYS_CHEN: run_tile<Chen, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err); break;
+            case CBF_SYS_LORENZ:
+                if (J.scaledStep)
+                    run_tile<LorenzScaled, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err);
+                else
+                    run_tile<Lorenz, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err);
+                break;
+            case CBF_SYS_CHEN:
+                if (J.scaledStep)
+                    run_tile<ChenScaled, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err);
+                else
+                    run_tile<Chen, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err);
+                break;
             default: break;
             }
         };

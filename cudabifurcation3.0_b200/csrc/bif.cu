@@ -326,8 +326,8 @@ cudaError_t launch_bif_prealloc(const DevJob& J, void* d_out, double* scratch, s
     switch (J.system) {
     case CBF_SYS_MEMRISTIVE5: return launch_bif_prealloc_s<Memristive5>(J, d_out, scratch, scratchBytes, err, s);
     case CBF_SYS_ROSSLER: return launch_bif_prealloc_s<Rossler>(J, d_out, scratch, scratchBytes, err, s);
-    case CBF_SYS_LORENZ: return launch_bif_prealloc_s<Lorenz>(J, d_out, scratch, scratchBytes, err, s);
-    case CBF_SYS_CHEN: return launch_bif_prealloc_s<Chen>(J, d_out, scratch, scratchBytes, err, s);
+    case CBF_SYS_LORENZ: return J.scaledStep ? launch_bif_prealloc_s<LorenzScaled>(J, d_out, scratch, scratchBytes, err, s) : launch_bif_prealloc_s<Lorenz>(J, d_out, scratch, scratchBytes, err, s);
+    case CBF_SYS_CHEN: return J.scaledStep ? launch_bif_prealloc_s<ChenScaled>(J, d_out, scratch, scratchBytes, err, s) : launch_bif_prealloc_s<Chen>(J, d_out, scratch, scratchBytes, err, s);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -337,8 +337,8 @@ cudaError_t launch_bif(const DevJob& J, void* d_out, int* d_aux, cudaStream_t s)
     switch (J.system) {
     case CBF_SYS_MEMRISTIVE5: return launch_bif_s<Memristive5>(J, d_out, d_aux, s);
     case CBF_SYS_ROSSLER: return launch_bif_s<Rossler>(J, d_out, d_aux, s);
-    case CBF_SYS_LORENZ: return launch_bif_s<Lorenz>(J, d_out, d_aux, s);
-    case CBF_SYS_CHEN: return launch_bif_s<Chen>(J, d_out, d_aux, s);
+    case CBF_SYS_LORENZ: return J.scaledStep ? launch_bif_s<LorenzScaled>(J, d_out, d_aux, s) : launch_bif_s<Lorenz>(J, d_out, d_aux, s);
+    case CBF_SYS_CHEN: return J.scaledStep ? launch_bif_s<ChenScaled>(J, d_out, d_aux, s) : launch_bif_s<Chen>(J, d_out, d_aux, s);
     default: return cudaErrorInvalidValue;
     }
 }

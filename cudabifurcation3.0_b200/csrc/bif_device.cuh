@@ -170,6 +170,7 @@ __device__ int integrate_point(const DevJob& J, long long g, double* pk, double*
     double x[D], v[CBF_MAX_VALUES];
     setup_point<D>(J, g, x, v);
     const typename S::Coef c = S::prep(v, J.h);
+    to_stored<S>(x, c);
 
 #pragma unroll 4
     for (int i = 0; i < J.nSkip; ++i) S::step(x, c);
@@ -180,7 +181,7 @@ __device__ int integrate_point(const DevJob& J, long long g, double* pk, double*
     bool div = false;
     int t = 0;
     for (; t < J.nRecord; ++t) {
-        const double val = pick<D>(x, wv);
+        const double val = phys_comp<S>(pick<D>(x, wv), wv, c);
         if (TASK == CBF_TASK_TRAJECTORY) {
             traj[t] = val;
         } else if (TASK == CBF_TASK_OSTROVSKY) {
@@ -191,7 +192,7 @@ __device__ int integrate_point(const DevJob& J, long long g, double* pk, double*
         }
         for (int j = 0; j < J.preScaller - 1; ++j) S::step(x, c);
         S::step(x, c);
-        if (J.checkDiv && diverged(pick<D>(x, wv), J.divThresh)) {
+        if (J.checkDiv && diverged(phys_comp<S>(pick<D>(x, wv), wv, c), J.divThresh)) {
             div = true;
             ++t;
             break;

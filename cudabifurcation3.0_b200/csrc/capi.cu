@@ -172,6 +172,52 @@ void divergence_threshold(double M, int* active, double* T)
 
 namespace {
 
+// Whether every point of a Chen or Lorenz job can run the rescaled 10-instruction
+// step (systems.cuh, QuadScaled): s = values[0] not swept, and every value each
+// other parameter takes (the fixed value, or all nPts values of its swept axis,
+// whatever points the job selects) finite and within 2^64 in magnitude, with
+// A = values[1] (a or sigma) and the step's denominators 1 + h1 A, 1 - k B,
+// 1 + h1 B and the y-equation factors (Chen 1 + k c, 1 - h1 c; Lorenz 1 - k,
+// 1 + h1) at least 2^-64 in magnitude.  Every derived coefficient then lies far
+// inside the double range and sy is nonzero.  The oracle applies the same rule.
+bool scaled_step_ok(const cbf_job* j)
+{
+    const bool chen = j->system == CBF_SYS_CHEN, lorenz = j->system == CBF_SYS_LORENZ;
+    if (!chen && !lorenz) return false;
+    const double big = 0x1p64, small = 0x1p-64;
+    auto fin = [&](double v) { return isfinite(v) && fabs(v) <= big; };
+    auto away = [&](double v) { return isfinite(v) && fabs(v) >= small; };
+    int sweptAxis[CBF_MAX_VALUES];
+    for (int i = 0; i < CBF_MAX_VALUES; ++i) sweptAxis[i] = -1;
+    if (!j->sweepIC)
+        for (int a = 0; a < j->dims && a < 2; ++a)
+            if (j->idxMut[a] >= 0 && j->idxMut[a] < CBF_MAX_VALUES) sweptAxis[j->idxMut[a]] = a;
+    if (sweptAxis[0] >= 0) return false;
+    const double h = j->h, s = j->values[0];
+    if (!(fin(h) && away(h) && fin(s))) return false;
+    const double k = h * s, h1 = h * (1.0 - s);
+    if (lorenz && !(away(1.0 - k) && away(1.0 + h1))) return false;
+    for (int slot = 1; slot <= 3; ++slot) {
+        const int ax = sweptAxis[slot];
+        const int count = ax < 0 ? 1 : j->nPts;
+        for (int cell = 0; cell < count; ++cell) {
+            // the values grid_value produces for this axis (engine.cuh)
+            const double v = ax < 0 ? j->values[slot]
+                                    : j->ranges[2 * ax] + (double)cell * ((double)(j->ranges[2 * ax + 1] -
+                                                                                    j->ranges[2 * ax]) /
+                                                                          (double)(j->nPts - 1));
+            if (!fin(v)) return false;
+            bool ok = true;
+            if (slot == 1) ok = away(v) && away(1.0 + h1 * v);                      // a / sigma
+            else if (chen && slot == 2) ok = away(1.0 - k * v) && away(1.0 + h1 * v);  // b
+            else if (chen && slot == 3) ok = away(1.0 + k * v) && away(1.0 - h1 * v);  // c
+            else if (lorenz && slot == 3) ok = away(1.0 - k * v) && away(1.0 + h1 * v);  // beta
+            if (!ok) return false;
+        }
+    }
+    return true;
+}
+
 cbf_status lower_job(const cbf_job* j, DevJob* d)
 {
     if (!j || !d) return fail(CBF_ERR_INVALID_ARG, "null job");
@@ -213,6 +259,7 @@ cbf_status lower_job(const cbf_job* j, DevJob* d)
     d->task = j->task;
     d->system = j->system;
     d->sweepIC = j->sweepIC ? 1 : 0;
+    d->scaledStep = scaled_step_ok(j) ? 1 : 0;
     d->dims = j->dims;
     d->nPts = j->nPts;
     d->nIC = j->nIC;
@@ -613,6 +660,13 @@ cbf_status cbf_validate(const cbf_job* job)
 {
     DevJob d;
     return lower_job(job, &d);
+}
+
+int32_t cbf_job_scaled_step(const cbf_job* job)
+{
+    DevJob d;
+    if (lower_job(job, &d) != CBF_OK) return -1;
+    return d.scaledStep;
 }
 
 cbf_status cbf_run(const cbf_job* job, void* d_out, void* d_aux, void* stream)

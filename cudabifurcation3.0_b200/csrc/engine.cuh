@@ -50,6 +50,7 @@ struct DevJob {
     int task;
     int system;
     int sweepIC;
+    int scaledStep;     // Chen/Lorenz: the 10-instruction rescaled step (systems.cuh) for this job
 };
 
 // Grid index of the job's k-th point: an explicit list, or a contiguous range.

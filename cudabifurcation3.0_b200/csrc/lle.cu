@@ -40,6 +40,7 @@ __global__ void __launch_bounds__(THREADS, MINB) lle_kernel(const DevJob J, doub
             double v[CBF_MAX_VALUES];
             setup_point<D>(J, grid_index(J, p), x[j], v);
             c[j] = S::prep(v, J.h);
+            to_stored<S>(x[j], c[j]);
         }
 
         run_checked<S, PPT>(x, c, J.nSkip, J);
@@ -51,7 +52,7 @@ __global__ void __launch_bounds__(THREADS, MINB) lle_kernel(const DevJob J, doub
             double z[D];
             lle_seed<D, IC>(grid_index(J, p), J.seedChunk, z);
 #pragma unroll
-            for (int i = 0; i < D; ++i) y[j][i] = z[i] * J.lleEps + x[j][i];
+            for (int i = 0; i < D; ++i) y[j][i] = stored_comp<S>(z[i] * J.lleEps, i, c[j]) + x[j][i];
         }
 
         double result[PPT];
@@ -63,7 +64,10 @@ __global__ void __launch_bounds__(THREADS, MINB) lle_kernel(const DevJob J, doub
             for (int j = 0; j < PPT; ++j) {
                 double t = 0;
 #pragma unroll
-                for (int l = 0; l < D; ++l) t += (x[j][l] - y[j][l]) * (x[j][l] - y[j][l]);
+                for (int l = 0; l < D; ++l) {
+                    const double d = phys_comp<S>(x[j][l] - y[j][l], l, c[j]);
+                    t += d * d;
+                }
                 t = sqrt(t) / J.lleEps;
                 result[j] += log(t);
                 if (t != 0) t = (1 / t);
@@ -148,8 +152,8 @@ cudaError_t launch_lle_variant(const DevJob& J, double* d_out, cudaStream_t s, i
     switch (J.system) {
     case CBF_SYS_MEMRISTIVE5: return launch_lle_s<Memristive5>(J, d_out, s, variant);
     case CBF_SYS_ROSSLER: return launch_lle_s<Rossler>(J, d_out, s, variant);
-    case CBF_SYS_LORENZ: return launch_lle_s<Lorenz>(J, d_out, s, variant);
-    case CBF_SYS_CHEN: return launch_lle_s<Chen>(J, d_out, s, variant);
+    case CBF_SYS_LORENZ: return J.scaledStep ? launch_lle_s<LorenzScaled>(J, d_out, s, variant) : launch_lle_s<Lorenz>(J, d_out, s, variant);
+    case CBF_SYS_CHEN: return J.scaledStep ? launch_lle_s<ChenScaled>(J, d_out, s, variant) : launch_lle_s<Chen>(J, d_out, s, variant);
     default: return cudaErrorInvalidValue;
     }
 }

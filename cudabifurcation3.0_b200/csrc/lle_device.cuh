@@ -137,18 +137,22 @@ __device__ __forceinline__ double lle_point(const DevJob& J, long long g)
         double v[CBF_MAX_VALUES];
         setup_point<D>(J, g, x[0], v);
         c[0] = S::prep(v, J.h);
+        to_stored<S>(x[0], c[0]);
     }
     run_checked<S, 1>(x, c, J.nSkip, J);
     double z[D];
     lle_seed<D, IC>(g, J.seedChunk, z);
 #pragma unroll
-    for (int i = 0; i < D; ++i) y[0][i] = z[i] * J.lleEps + x[0][i];
+    for (int i = 0; i < D; ++i) y[0][i] = stored_comp<S>(z[i] * J.lleEps, i, c[0]) + x[0][i];
     double result = 0;
     for (int b = 0; b < J.nRecord; ++b) {
         run_pair<S, 1>(x, y, c, J.nNT, J);
         double t = 0;
 #pragma unroll
-        for (int l = 0; l < D; ++l) t += (x[0][l] - y[0][l]) * (x[0][l] - y[0][l]);
+        for (int l = 0; l < D; ++l) {
+            const double d = phys_comp<S>(x[0][l] - y[0][l], l, c[0]);
+            t += d * d;
+        }
         t = sqrt(t) / J.lleEps;
         result += log(t);
         if (t != 0) t = (1 / t);

@@ -37,20 +37,24 @@ __device__ double lle_regime_point(const DevJob& J, long long g, double* pk, dou
         double v[CBF_MAX_VALUES];
         setup_point<D>(J, g, x[0], v);
         c[0] = S::prep(v, J.h);
+        to_stored<S>(x[0], c[0]);
     }
     run_checked<S, 1>(x, c, J.nSkip, J);
     {
         double z[D];
         lle_seed<D, IC>(g, J.seedChunk, z);
 #pragma unroll
-        for (int i = 0; i < D; ++i) y[0][i] = z[i] * J.lleEps + x[0][i];
+        for (int i = 0; i < D; ++i) y[0][i] = stored_comp<S>(z[i] * J.lleEps, i, c[0]) + x[0][i];
     }
     double result = 0;
     // Renormalisation (cudaLibrary.cu:757-776) after each interval.
     auto renorm = [&]() {
         double tt = 0;
 #pragma unroll
-        for (int l = 0; l < D; ++l) tt += (x[0][l] - y[0][l]) * (x[0][l] - y[0][l]);
+        for (int l = 0; l < D; ++l) {
+            const double d = phys_comp<S>(x[0][l] - y[0][l], l, c[0]);
+            tt += d * d;
+        }
         tt = sqrt(tt) / J.lleEps;
         result += log(tt);
         if (tt != 0) tt = (1 / tt);
@@ -78,7 +82,7 @@ __device__ double lle_regime_point(const DevJob& J, long long g, double* pk, dou
             for (int i = 0; i < J.nNT; ++i, ++t) {
                 if (ax) {
                     if (t < J.regimeSteps) {
-                        const double v = pick<D>(x[0], J.writableVar);
+                        const double v = phys_comp<S>(pick<D>(x[0], J.writableVar), J.writableVar, c[0]);
                         lo = fmin(lo, v);
                         hi = fmax(hi, v);
                         ps.push<true>(v, t, pk, iv, cap);
@@ -239,8 +243,8 @@ long long lle_regime_resident_points(const DevJob& J)
     switch (J.system) {
     case CBF_SYS_MEMRISTIVE5: return resident_s<Memristive5>(J);
     case CBF_SYS_ROSSLER: return resident_s<Rossler>(J);
-    case CBF_SYS_LORENZ: return resident_s<Lorenz>(J);
-    case CBF_SYS_CHEN: return resident_s<Chen>(J);
+    case CBF_SYS_LORENZ: return J.scaledStep ? resident_s<LorenzScaled>(J) : resident_s<Lorenz>(J);
+    case CBF_SYS_CHEN: return J.scaledStep ? resident_s<ChenScaled>(J) : resident_s<Chen>(J);
     default: return 0;
     }
 }
@@ -250,8 +254,8 @@ cudaError_t launch_lle_regime(const DevJob& J, double* d_lle, int* d_cls, cudaSt
     switch (J.system) {
     case CBF_SYS_MEMRISTIVE5: return launch_s<Memristive5>(J, d_lle, d_cls, s);
     case CBF_SYS_ROSSLER: return launch_s<Rossler>(J, d_lle, d_cls, s);
-    case CBF_SYS_LORENZ: return launch_s<Lorenz>(J, d_lle, d_cls, s);
-    case CBF_SYS_CHEN: return launch_s<Chen>(J, d_lle, d_cls, s);
+    case CBF_SYS_LORENZ: return J.scaledStep ? launch_s<LorenzScaled>(J, d_lle, d_cls, s) : launch_s<Lorenz>(J, d_lle, d_cls, s);
+    case CBF_SYS_CHEN: return J.scaledStep ? launch_s<ChenScaled>(J, d_lle, d_cls, s) : launch_s<Chen>(J, d_lle, d_cls, s);
     default: return cudaErrorInvalidValue;
     }
 }

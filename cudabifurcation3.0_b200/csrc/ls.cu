@@ -108,6 +108,7 @@ __device__ void ls_point(const DevJob& J, long long g, double* __restrict__ out)
         double v[CBF_MAX_VALUES];
         setup_point<D>(J, g, t[0], v);
         c = S::prep(v, J.h);
+        to_stored<S>(t[0], c);
     }
     {
         double x1[1][D];
@@ -123,20 +124,20 @@ __device__ void ls_point(const DevJob& J, long long g, double* __restrict__ out)
     for (int j = 0; j < D; ++j) {
         res[j] = 0;
 #pragma unroll
-        for (int i = 0; i < D; ++i) t[1 + j][i] = w[j][i] * J.lleEps + t[0][i];
+        for (int i = 0; i < D; ++i) t[1 + j][i] = stored_comp<S>(w[j][i] * J.lleEps, i, c) + t[0][i];
     }
     for (int b = 0; b < J.nRecord; ++b) {
         run_multi<S, D + 1>(t, c, J.nNT, J);
 #pragma unroll
         for (int k = 0; k < D; ++k)
 #pragma unroll
-            for (int l = 0; l < D; ++l) w[k][l] = t[1 + k][l] - t[0][l];
+            for (int l = 0; l < D; ++l) w[k][l] = phys_comp<S>(t[1 + k][l] - t[0][l], l, c);
         gram_schmidt<D, true>(w, z, den);
 #pragma unroll
         for (int k = 0; k < D; ++k) {
             res[k] += log(den[k] / J.lleEps);
 #pragma unroll
-            for (int j = 0; j < D; ++j) t[1 + k][j] = t[0][j] + z[k][j] * J.lleEps;
+            for (int j = 0; j < D; ++j) t[1 + k][j] = t[0][j] + stored_comp<S>(z[k][j] * J.lleEps, j, c);
         }
     }
 #pragma unroll
@@ -181,8 +182,8 @@ cudaError_t launch_ls(const DevJob& J, double* d_out, cudaStream_t s)
     switch (J.system) {
     case CBF_SYS_MEMRISTIVE5: return launch_s<Memristive5>(J, d_out, s);
     case CBF_SYS_ROSSLER: return launch_s<Rossler>(J, d_out, s);
-    case CBF_SYS_LORENZ: return launch_s<Lorenz>(J, d_out, s);
-    case CBF_SYS_CHEN: return launch_s<Chen>(J, d_out, s);
+    case CBF_SYS_LORENZ: return J.scaledStep ? launch_s<LorenzScaled>(J, d_out, s) : launch_s<Lorenz>(J, d_out, s);
+    case CBF_SYS_CHEN: return J.scaledStep ? launch_s<ChenScaled>(J, d_out, s) : launch_s<Chen>(J, d_out, s);
     default: return cudaErrorInvalidValue;
     }
 }

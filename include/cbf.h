@@ -135,6 +135,12 @@ int32_t cbf_record_length(const cbf_job* job);   /* (int)(tMax/h/preScaller) or 
 int32_t cbf_peak_capacity(const cbf_job* job);   /* peaks a PEAKS row can hold = record/2 */
 int64_t cbf_job_points(const cbf_job* job);      /* nPoints, or nPts^dims when 0 */
 cbf_status cbf_validate(const cbf_job* job);
+/* 1 when the job's Chen or Lorenz steps use the rescaled 10-instruction form (y
+ * stored in units of a per-point constant, 4 MUL + 6 FMA per step), 0 for the
+ * 14-instruction form (other systems, s swept, A = 0, or factors near 0 or
+ * beyond 2^64), -1 for an invalid job.  Both are the same CD step; each has its
+ * own rounding, and the CPU oracle follows the one the job uses. */
+int32_t cbf_job_scaled_step(const cbf_job* job);
 
 /* ---- device-resident interface --------------------------------------- */
 /* Run one job on `stream` (a cudaStream_t, NULL = legacy default stream).

@@ -158,9 +158,68 @@ static void step_lorenz(double* X, const double* v, double h)
     X[0] = x2; X[1] = y2; X[2] = z2;
 }
 
+/* The library's rescaled Chen / Lorenz step (10 FP64 operations), for the jobs
+ * orc_scaled_step admits.  The state's y is stored as Y = sy * y; x and z are
+ * physical.  With A = a or sigma, B = b or beta, om = 1 - k B, ups = r1 A h,
+ * sy = ups cy, th = ups sy om, the CD step becomes
+ *   p = k1 x;  Z1 = fma(p, Y, z);  W = fma(al, Z1, be);  Y1 = fma(p, W, Y);
+ *   x2 = fma(rho, x, Y1);  q = k2 x2;  Y2 = ly fma(q, W, Y1);  z2 = lz fma(q, Y2, Z1)
+ * (coefficients below, in the kernels' operation order). */
+typedef struct {
+    double k1, al, be, rho, k2, ly, lz, sy, iy;
+} scaled_coef;
+
+static void scaled_coef_of(int lorenz, const double* v, double h, scaled_coef* q)
+{
+    const double s = v[0];
+    const double k = h * s;
+    const double h1 = h * (1.0 - s);
+    const double A = v[1];
+    const double B = lorenz ? v[3] : v[2];
+    const double W0 = lorenz ? v[2] : v[3] - v[1];
+    const double cy = lorenz ? 1.0 - k : 1.0 + k * v[3];
+    const double r2 = lorenz ? 1.0 / (1.0 + h1) : 1.0 / (1.0 - h1 * v[3]);
+    const double r1 = 1.0 / (1.0 + h1 * A);
+    const double r3 = 1.0 / (1.0 + h1 * B);
+    const double ups = (r1 * A) * h;
+    const double om = 1.0 - k * B;
+    q->sy = ups * cy;
+    const double th = (ups * q->sy) * om;
+    const double osy = om * q->sy;
+    q->k1 = k / osy;
+    q->k2 = h1 / osy;
+    q->al = -(th * om);
+    q->be = th * W0;
+    q->rho = r1 * (1.0 - k * A);
+    q->ly = cy * r2;
+    q->lz = om * r3;
+    q->iy = 1.0 / q->sy;
+}
+
+static void step_quad_scaled(int lorenz, double* X, const double* v, double h)
+{
+    scaled_coef q;
+    scaled_coef_of(lorenz, v, h, &q);
+    const double x = X[0], y = X[1], z = X[2];
+    const double p = q.k1 * x;
+    const double z1 = fma(p, y, z);
+    const double w = fma(q.al, z1, q.be);
+    const double y1 = fma(p, w, y);
+    const double x2 = fma(q.rho, x, y1);
+    const double qq = q.k2 * x2;
+    const double y2 = q.ly * fma(qq, w, y1);
+    const double z2 = q.lz * fma(qq, y2, z1);
+    X[0] = x2; X[1] = y2; X[2] = z2;
+}
+
+/* Internal ids of the rescaled forms (never in a job; setup_point returns them). */
+enum { ORC_SCALED = 0x100 };
+
+static int is_scaled(int system) { return (system & ORC_SCALED) != 0; }
+
 int orc_system_dim(int system)
 {
-    switch (system) {
+    switch (system & ~ORC_SCALED) {
     case ORC_SYS_MEMRISTIVE5: return 5;
     case ORC_SYS_ROSSLER:
     case ORC_SYS_LORENZ:
@@ -176,8 +235,81 @@ void orc_model_step(int system, double* x, const double* a, double h)
     case ORC_SYS_ROSSLER: step_rossler(x, a, h); break;
     case ORC_SYS_LORENZ: step_lorenz(x, a, h); break;
     case ORC_SYS_CHEN: step_chen(x, a, h); break;
+    case ORC_SYS_LORENZ | ORC_SCALED: step_quad_scaled(1, x, a, h); break;
+    case ORC_SYS_CHEN | ORC_SCALED: step_quad_scaled(0, x, a, h); break;
     default: break;
     }
+}
+
+/* 1/sy of a rescaled system (the factor that turns a stored y into a physical
+ * one), 1 for the others. */
+static double y_phys_factor(int system, const double* v, double h)
+{
+    if (!is_scaled(system))
+        return 1.0;
+    scaled_coef q;
+    scaled_coef_of((system & ~ORC_SCALED) == ORC_SYS_LORENZ, v, h, &q);
+    return q.iy;
+}
+
+/* Stored component i -> physical (multiplied by 1/sy for y of a rescaled system). */
+static double to_phys(int system, double value, int i, double iy)
+{
+    return (is_scaled(system) && i == 1) ? value * iy : value;
+}
+
+/* Whether a Chen / Lorenz job runs the rescaled step (the library's
+ * scaled_step_ok, capi.cu): s not swept; every value of a, b, c (sigma, rho,
+ * beta) the job's grid holds finite and within 2^64; A = values[1] and the
+ * factors 1 + h1 A, 1 - k B, 1 + h1 B, Chen 1 + k c, 1 - h1 c, Lorenz 1 - k,
+ * 1 + h1 at least 2^-64 in magnitude. */
+static int fin64(double v) { return isfinite(v) && fabs(v) <= 0x1p64; }
+static int away64(double v) { return isfinite(v) && fabs(v) >= 0x1p-64; }
+
+int orc_scaled_step(const orc_job* job)
+{
+    const int chen = job->system == ORC_SYS_CHEN, lorenz = job->system == ORC_SYS_LORENZ;
+    if (!chen && !lorenz)
+        return 0;
+    int sweptAxis[16];
+    for (int i = 0; i < 16; ++i)
+        sweptAxis[i] = -1;
+    if (!job->sweepIC)
+        for (int a = 0; a < job->dims && a < 2; ++a)
+            if (job->idxMut[a] >= 0 && job->idxMut[a] < 16)
+                sweptAxis[job->idxMut[a]] = a;
+    if (sweptAxis[0] >= 0)
+        return 0;
+    const double h = job->h, s = job->values[0];
+    if (!(fin64(h) && away64(h) && fin64(s)))
+        return 0;
+    const double k = h * s, h1 = h * (1.0 - s);
+    if (lorenz && !(away64(1.0 - k) && away64(1.0 + h1)))
+        return 0;
+    for (int slot = 1; slot <= 3; ++slot) {
+        const int ax = sweptAxis[slot];
+        const int count = ax < 0 ? 1 : job->nPts;
+        for (int cell = 0; cell < count; ++cell) {
+            const double v = ax < 0 ? job->values[slot]
+                                    : job->ranges[2 * ax] + (double)cell * ((double)(job->ranges[2 * ax + 1] -
+                                                                                      job->ranges[2 * ax]) /
+                                                                            (double)(job->nPts - 1));
+            if (!fin64(v))
+                return 0;
+            int ok = 1;
+            if (slot == 1)
+                ok = away64(v) && away64(1.0 + h1 * v);
+            else if (chen && slot == 2)
+                ok = away64(1.0 - k * v) && away64(1.0 + h1 * v);
+            else if (chen && slot == 3)
+                ok = away64(1.0 + k * v) && away64(1.0 - h1 * v);
+            else if (lorenz && slot == 3)
+                ok = away64(1.0 - k * v) && away64(1.0 + h1 * v);
+            if (!ok)
+                return 0;
+        }
+    }
+    return 1;
 }
 
 /* `if (maxValue != 0) if (fabsf(x[writableVar]) > maxValue)`: fabsf rounds the
@@ -193,14 +325,16 @@ int orc_loop(int system, double* x, const double* values, double h, int amountOf
              int preScaller, int writableVar, double maxValue, double* data,
              int64_t startDataIndex, int writeStep)
 {
+    /* x[writableVar] in physical units (a rescaled system stores y times sy) */
+    const double iy = y_phys_factor(system, values, h);
     for (int i = 0; i < amountOfIterations; ++i) {
         if (data != NULL)
-            data[startDataIndex + (int64_t)i * writeStep] = x[writableVar];
+            data[startDataIndex + (int64_t)i * writeStep] = to_phys(system, x[writableVar], writableVar, iy);
         for (int j = 0; j < preScaller - 1; ++j)
             orc_model_step(system, x, values, h);
         orc_model_step(system, x, values, h);
         if (maxValue != 0)
-            if ((double)fabsf((float)x[writableVar]) > maxValue)
+            if ((double)fabsf((float)to_phys(system, x[writableVar], writableVar, iy)) > maxValue)
                 return 0;
     }
     return 1;
@@ -414,14 +548,36 @@ static void setup_point(const orc_job* job, int64_t g, double* x, double* v)
     }
 }
 
+/* setup_point, then the state converted to the units the job's step uses; returns
+ * the system id the loops integrate (a rescaled form where the job admits it) and
+ * sets *sy (1 for unscaled systems). */
+static int setup_state(const orc_job* job, int64_t g, double* x, double* v, double* sy)
+{
+    setup_point(job, g, x, v);
+    *sy = 1.0;
+    if (!orc_scaled_step(job))
+        return job->system;
+    scaled_coef q;
+    scaled_coef_of(job->system == ORC_SYS_LORENZ, v, job->h, &q);
+    x[1] = x[1] * q.sy;
+    *sy = q.sy;
+    return job->system | ORC_SCALED;
+}
+
+/* A physical perturbation component in stored units. */
+static double to_stored(int system, double value, int i, double sy)
+{
+    return (is_scaled(system) && i == 1) ? value * sy : value;
+}
+
 /* cudaLibrary.cu:107-114 (and :194-201): unchecked transient, then the recorded
  * loop with the divergence check on x[writableVar]. */
 int orc_trajectory_point(const orc_job* job, int64_t g, double* data)
 {
-    double x[8], v[16];
-    setup_point(job, g, x, v);
-    orc_loop(job->system, x, v, job->h, orc_skip_len(job), 1, 0, 0, NULL, 0, 1);
-    int ok = orc_loop(job->system, x, v, job->h, orc_record_len(job), job->preScaller,
+    double x[8], v[16], sy;
+    const int sys = setup_state(job, g, x, v, &sy);
+    orc_loop(sys, x, v, job->h, orc_skip_len(job), 1, 0, 0, NULL, 0, 1);
+    int ok = orc_loop(sys, x, v, job->h, orc_record_len(job), job->preScaller,
                       job->writableVar, job->maxValue, data, 0, 1);
     return !ok;
 }
@@ -460,8 +616,8 @@ double orc_lle_point(const orc_job* job, int64_t g)
 /* zIn: the normalised perturbation to start from (NULL: orc_lle_seed). */
 double orc_lle_point_seeded(const orc_job* job, int64_t g, const double* zIn)
 {
-    double x[8], y[8], z[8], v[16];
-    setup_point(job, g, x, v);
+    double x[8], y[8], z[8], v[16], sy;
+    const int sys = setup_state(job, g, x, v, &sy);
 
     const int nIC = job->nIC;
     if (zIn) {
@@ -471,17 +627,18 @@ double orc_lle_point_seeded(const orc_job* job, int64_t g, const double* zIn)
         orc_lle_seed(job, g, z);
     }
 
-    const int sys = job->system;
     const double h = job->h;
     const int skip = orc_skip_len(job);
     const int nNT = (int)(size_t)(job->NT / h);
     const int sizeOfBlock = (int)(job->tMax / job->NT);
     const double eps = job->lleEps;
+    const double iy = y_phys_factor(sys, v, h);
 
     orc_loop(sys, x, v, h, skip, 1, 0, job->maxValue, NULL, 0, 1);
 
+    /* the perturbation in physical units; distances measured in physical units */
     for (int i = 0; i < nIC; ++i)
-        y[i] = z[i] * eps + x[i];
+        y[i] = to_stored(sys, z[i] * eps, i, sy) + x[i];
 
     double result = 0;
     for (int i = 0; i < sizeOfBlock; ++i) {
@@ -489,8 +646,10 @@ double orc_lle_point_seeded(const orc_job* job, int64_t g, const double* zIn)
         orc_loop(sys, y, v, h, nNT, 1, 0, job->maxValue, NULL, 0, 1);
 
         double tempData = 0;
-        for (int l = 0; l < nIC; ++l)
-            tempData += (x[l] - y[l]) * (x[l] - y[l]);
+        for (int l = 0; l < nIC; ++l) {
+            const double d = to_phys(sys, x[l] - y[l], l, iy);
+            tempData += d * d;
+        }
         tempData = sqrt(tempData) / eps;
 
         result += log(tempData);
@@ -506,8 +665,8 @@ double orc_lle_point_seeded(const orc_job* job, int64_t g, const double* zIn)
 
 double orc_lle_regime_point(const orc_job* job, int64_t g, const double* zIn, int32_t* cls)
 {
-    double x[8], y[8], z[8], v[16];
-    setup_point(job, g, x, v);
+    double x[8], y[8], z[8], v[16], sy;
+    const int sys = setup_state(job, g, x, v, &sy);
     const int nIC = job->nIC;
     if (zIn) {
         for (int i = 0; i < nIC; ++i)
@@ -515,8 +674,8 @@ double orc_lle_regime_point(const orc_job* job, int64_t g, const double* zIn, in
     } else {
         orc_lle_seed(job, g, z);
     }
-    const int sys = job->system;
     const double h = job->h;
+    const double iy = y_phys_factor(sys, v, h);
     const int nNT = (int)(size_t)(job->NT / h);
     const int sizeOfBlock = (int)(job->tMax / job->NT);
     const double eps = job->lleEps;
@@ -528,7 +687,7 @@ double orc_lle_regime_point(const orc_job* job, int64_t g, const double* zIn, in
 
     orc_loop(sys, x, v, h, orc_skip_len(job), 1, 0, job->maxValue, NULL, 0, 1);
     for (int i = 0; i < nIC; ++i)
-        y[i] = z[i] * eps + x[i];
+        y[i] = to_stored(sys, z[i] * eps, i, sy) + x[i];
 
     double result = 0;
     int t = 0;
@@ -549,8 +708,10 @@ double orc_lle_regime_point(const orc_job* job, int64_t g, const double* zIn, in
         t += nNT;
 
         double tempData = 0;
-        for (int l = 0; l < nIC; ++l)
-            tempData += (x[l] - y[l]) * (x[l] - y[l]);
+        for (int l = 0; l < nIC; ++l) {
+            const double d = to_phys(sys, x[l] - y[l], l, iy);
+            tempData += d * d;
+        }
         tempData = sqrt(tempData) / eps;
         result += log(tempData);
         if (tempData != 0)
@@ -910,28 +1071,29 @@ void orc_ls_seed(const orc_job* job, int64_t g, double* z)
  * optional) replaces the seed rows. */
 void orc_ls_point(const orc_job* job, int64_t g, const double* zIn, double* out)
 {
-    double x[8], y[64], z[64], v[16], den[8], result[8];
+    double x[8], y[64], z[64], v[16], den[8], result[8], sy;
     const int n = job->nIC;
-    setup_point(job, g, x, v);
+    const int sys = setup_state(job, g, x, v, &sy);
     if (zIn) {
         for (int i = 0; i < n * n; ++i)
             z[i] = zIn[i];
     } else {
         orc_ls_seed(job, g, z);
     }
-    const int sys = job->system;
     const double h = job->h;
     const int nNT = (int)(size_t)(job->NT / h);
     const int sizeOfBlock = (int)(job->tMax / job->NT);
     const double eps = job->lleEps;
+    const double iy = y_phys_factor(sys, v, h);
     for (int i = 0; i < n; ++i)
         result[i] = 0;
 
     orc_loop(sys, x, v, h, orc_skip_len(job), 1, 0, job->maxValue, NULL, 0, 1);
     orc_gram_schmidt(z, y, n, NULL);
+    /* perturbations placed, and deviations orthonormalised, in physical units */
     for (int j = 0; j < n; ++j)
         for (int i = 0; i < n; ++i)
-            y[j * n + i] = y[j * n + i] * eps + x[i];
+            y[j * n + i] = to_stored(sys, y[j * n + i] * eps, i, sy) + x[i];
 
     for (int b = 0; b < sizeOfBlock; ++b) {
         /* every trajectory stops at its own first violation (cudaLibrary.cu:1049-1060) */
@@ -940,12 +1102,12 @@ void orc_ls_point(const orc_job* job, int64_t g, const double* zIn, double* out)
             orc_loop(sys, y + j * n, v, h, nNT, 1, 0, job->maxValue, NULL, 0, 1);
         for (int k = 0; k < n; ++k)
             for (int l = 0; l < n; ++l)
-                y[k * n + l] = y[k * n + l] - x[l];
+                y[k * n + l] = to_phys(sys, y[k * n + l] - x[l], l, iy);
         orc_gram_schmidt(y, z, n, den);
         for (int k = 0; k < n; ++k) {
             result[k] += log(den[k] / eps);
             for (int j = 0; j < n; ++j)
-                y[k * n + j] = (double)(x[j] + z[k * n + j] * eps);
+                y[k * n + j] = (double)(x[j] + to_stored(sys, z[k * n + j] * eps, j, sy));
         }
     }
     for (int i = 0; i < n; ++i)

@@ -156,6 +156,12 @@ int orc_map_ls_list(const orc_job* job, const int64_t* idx, int64_t count, const
 int orc_map_lle_regime_list(const orc_job* job, const int64_t* idx, int64_t count,
                             const double* z, double* outLle, int32_t* outCls, int nThreads);
 
+/* 1 when a Chen / Lorenz job runs the rescaled 10-operation step (y stored times
+ * a per-point constant sy; the library's cbf_job_scaled_step), else 0.  Every
+ * per-point routine above follows the form the job runs, and reports, records and
+ * checks states in physical units. */
+int orc_scaled_step(const orc_job* job);
+
 /* Divergence test of loopCalculateDiscreteModel (cudaLibrary.cu:69-71), exposed for tests. */
 int orc_diverged(double v, double maxValue);
 

@@ -285,3 +285,33 @@ def test_surrogate_config_defaults(cbf):
     assert (c.boundaryRadius, c.expandRadius, c.maxWaves, c.refine) == (1, -1, 20, 1)
     with pytest.raises(AttributeError):
         cbf.surrogate_config(noSuchField=1)
+
+
+@pytest.mark.parametrize("kw,want", [
+    (dict(), 1),                                              # Chen a in [30, 45]: rescaled step
+    (dict(system="lorenz", values=[0.5, 10, 28, 8 / 3], ranges=[5, 20, 20, 200], idxMut=[1, 2]), 1),
+    (dict(ranges=[-5, 5, 20, 30], nPts=11), 0),               # a = 0 on the grid: 14-instruction form
+    (dict(ranges=[-5, 5, 20, 30], nPts=10), 1),               # a never exactly 0
+    (dict(idxMut=[0, 3], ranges=[0.2, 0.8, 20, 30]), 0),      # s swept
+    (dict(system="rossler", values=[0.5, 0.2, 0.2, 5.7], ranges=[0.05, 0.35, 0.05, 0.35], idxMut=[1, 2]), 0),
+    (dict(sweepIC=True, idxMut=[0, 2], ranges=[-5, 5, -5, 5]), 1),
+    (dict(values=[0.5, 0.0, 3, 28], sweepIC=True, idxMut=[0, 2], ranges=[-5, 5, -5, 5]), 0),
+    (dict(values=[0.5, 35, 3, 1e30], idxMut=[1, 2], ranges=[30, 45, 1, 5]), 0),  # c beyond 2^64
+])
+def test_step_form_choice_matches_oracle(cbf, orc, kw, want):
+    """The rescaled Chen/Lorenz step is chosen per job by the same rule in the
+    library and the oracle (every value the grid holds is checked)."""
+    base = dict(system="chen", nPts=16, ranges=[30, 45, 20, 30], idxMut=[1, 3], ic=[0.1, 0.1, 0.1],
+                values=[0.5, 35, 3, 28], h=0.002, tMax=10, NT=0.5, lleEps=1e-8, transientTime=1, maxValue=1e4)
+    base.update(kw)
+    j = cbf.make_job(task=cbf.TASK_LLE, **base)
+    L = cbf.lib()
+    L.cbf_job_scaled_step.restype = C.c_int32
+    L.cbf_job_scaled_step.argtypes = [C.c_void_p]
+    got = L.cbf_job_scaled_step(C.addressof(j))
+    O = orc.lib()
+    O.orc_scaled_step.restype = C.c_int
+    O.orc_scaled_step.argtypes = [C.c_void_p]
+    o = orc.make_job(**base)
+    assert got == want
+    assert O.orc_scaled_step(C.addressof(o)) == want

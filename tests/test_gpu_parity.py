@@ -388,3 +388,28 @@ def test_exact_grid_flag(cbf, orc, gpu_ok):
     g = np.arange(16777216, 16777216 + 2048)
     assert np.array_equal(got[:, 0], (g % 8192).astype(float))
     assert np.array_equal(got[:, 1], (g // 8192).astype(float))
+
+
+@pytest.mark.parametrize("task", ["lle", "traj"])
+def test_fourteen_instruction_form_when_the_grid_holds_a_zero(cbf, orc, gpu_ok, task):
+    """A Chen grid whose a-axis holds a = 0 runs the 14-instruction step (the
+    rescaled form needs a != 0); results still equal the oracle's, which makes the
+    same choice.  y (writableVar 1) is recorded in physical units either way."""
+    kw = dict(CHEN, nPts=11, ranges=[-5.0, 5.0, 20.0, 30.0], idxMut=[1, 3], h=0.002, maxValue=1e4)
+    j0 = cbf.make_job(task=cbf.TASK_LLE, NT=0.5, tMax=10.0, transientTime=2.0, lleEps=1e-8, **kw)
+    import ctypes as C2
+    cbf.lib().cbf_job_scaled_step.restype = C2.c_int32
+    assert cbf.lib().cbf_job_scaled_step(C2.byref(j0)) == 0
+    if task == "lle":
+        j, o = both(cbf, orc, task=cbf.TASK_LLE, NT=0.5, tMax=10.0, transientTime=2.0, lleEps=1e-8, **kw)
+        got, _ = cbf.run_host(j)
+        assert_lle_close(got, orc.map_lle_seeded(o, 0, 121, cbf.lle_seeds(j)))
+    else:
+        j, o = both(cbf, orc, task=cbf.TASK_TRAJECTORY, tMax=2.0, transientTime=1.0, preScaller=1,
+                    writableVar=1, **kw)
+        traj, div = cbf.run_host(j)
+        rec = cbf.record_length(j)
+        for g in range(0, 121, 7):
+            want, wdiv = orc.trajectory(o, g)
+            assert bool(div[g]) == wdiv
+            assert np.array_equal(traj[g, :rec], want), g
