@@ -564,6 +564,23 @@ static int setup_state(const orc_job* job, int64_t g, double* x, double* v, doub
     return job->system | ORC_SCALED;
 }
 
+/* The regime window of the LLE + regime point: x[recVar] (physical) recorded
+ * before every step, the LLE's divergence test on x[0] after it (the LLE kernels
+ * test x[0] whatever writableVar is, cudaLibrary.cu:735-753); returns 0 at the
+ * first violation, like orc_loop. */
+static int loop_window(int system, double* x, const double* values, double h, int n, int recVar,
+                       double maxValue, double* data)
+{
+    const double iy = y_phys_factor(system, values, h);
+    for (int i = 0; i < n; ++i) {
+        data[i] = to_phys(system, x[recVar], recVar, iy);
+        orc_model_step(system, x, values, h);
+        if (maxValue != 0 && (double)fabsf((float)x[0]) > maxValue)
+            return 0;
+    }
+    return 1;
+}
+
 /* A physical perturbation component in stored units. */
 static double to_stored(int system, double value, int i, double sy)
 {
@@ -699,7 +716,7 @@ double orc_lle_regime_point(const orc_job* job, int64_t g, const double* zIn, in
         if (inWin < 0) inWin = 0;
         int ok = 1;
         if (inWin > 0) {
-            ok = orc_loop(sys, x, v, h, inWin, 1, job->writableVar, job->maxValue, data, t, 1);
+            ok = loop_window(sys, x, v, h, inWin, job->writableVar, job->maxValue, data + t);
             if (!ok) regimeDiv = 1;
         }
         if (ok && nNT - inWin > 0)
