@@ -120,6 +120,7 @@ class SurrogateConfig(C.Structure):
         ("seed", C.c_uint64),
         ("expandRadius", C.c_int32),
         ("maxWaves", C.c_int32),
+        ("predictor", C.c_int32),
     ]
 
 

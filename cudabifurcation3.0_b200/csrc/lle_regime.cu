@@ -110,6 +110,41 @@ __device__ double lle_regime_point(const DevJob& J, long long g, double* pk, dou
     return result / J.tMax;
 }
 
+// LLE and regime class of the lane's grid point g (`valid` false: the lane idles
+// through the integration), the warp cooperating on the DBSCAN epilogues of
+// lanes 0..live-1; *lleOut = the lane's LLE.
+template <class S, bool IC>
+__device__ __forceinline__ int regime_tile(const DevJob& J, long long g, bool valid, int live, int lane,
+                                           double* scrPk, double* scrIv, long long slot0, unsigned* L,
+                                           unsigned* Sb, const DbscanSort& so, int* err, double* lleOut)
+{
+    const int cap = J.peakCap;
+    double* myPk = scrPk + (slot0 + lane) * (long long)cap;
+    double* myIv = scrIv + (slot0 + lane) * (long long)cap;
+    int n = 0;
+    double lv = 0, amp = 0;
+    if (valid) lv = lle_regime_point<S, IC>(J, g, myPk, myIv, cap, &n, &amp);
+    if (amp < J.regimeMinAmp) n = 0;  // no oscillation
+    __syncwarp();
+    int res = 0;
+    for (int j = 0; j < live; ++j) {
+        const int nj = __shfl_sync(kFull, n, j);
+        const double lj = __shfl_sync(kFull, lv, j);
+        int r;
+        if (nj <= 0) r = 0;
+        else if (J.regimeChaosLle > 0 && lj > J.regimeChaosLle) r = kNumClasses - 1;
+        else if (nj > J.maxPeaks) r = kNumClasses - 1;
+        else {
+            const double* pk = scrPk + (slot0 + j) * (long long)cap;
+            const double* iv = scrIv + (slot0 + j) * (long long)cap;
+            r = min(dbscan_warp(J, pk, iv, nj, lane, L, Sb, err, so), kNumClasses - 1);
+        }
+        if (lane == j) res = r;
+    }
+    *lleOut = lv;
+    return res;
+}
+
 // Six blocks per SM, like the autotuned LLE map kernel: 80 registers, no spill.
 template <class S, bool IC>
 __global__ void __launch_bounds__(kRegThreads, 6) lle_regime_kernel(const DevJob J, double* __restrict__ lle,
@@ -132,35 +167,279 @@ __global__ void __launch_bounds__(kRegThreads, 6) lle_regime_kernel(const DevJob
     for (long long tile = warpId; tile < nTiles; tile += nWarps) {
         const long long p = tile * 32 + lane;
         const bool valid = p < J.nPoints;
-        double* myPk = scrPk + (slot0 + lane) * (long long)cap;
-        double* myIv = scrIv + (slot0 + lane) * (long long)cap;
-        int n = 0;
-        double lv = 0, amp = 0;
-        if (valid) lv = lle_regime_point<S, IC>(J, grid_index(J, p), myPk, myIv, cap, &n, &amp);
-        if (amp < J.regimeMinAmp) n = 0;  // no oscillation
-        __syncwarp();
-        int res = 0;
         const int live = (int)min(32ll, J.nPoints - tile * 32);
-        for (int j = 0; j < live; ++j) {
-            const int nj = __shfl_sync(kFull, n, j);
-            const double lj = __shfl_sync(kFull, lv, j);
-            int r;
-            if (nj <= 0) r = 0;
-            else if (J.regimeChaosLle > 0 && lj > J.regimeChaosLle) r = kNumClasses - 1;
-            else if (nj > J.maxPeaks) r = kNumClasses - 1;
-            else {
-                const double* pk = scrPk + (slot0 + j) * (long long)cap;
-                const double* iv = scrIv + (slot0 + j) * (long long)cap;
-                r = min(dbscan_warp(J, pk, iv, nj, lane, L, Sb, err, so), kNumClasses - 1);
-            }
-            if (lane == j) res = r;
-        }
+        double lv = 0;
+        const int res = regime_tile<S, IC>(J, valid ? grid_index(J, p) : 0, valid, live, lane, scrPk, scrIv,
+                                           slot0, L, Sb, so, err, &lv);
         if (valid) {
             lle[p] = lv;
             cls[p] = res;
         }
         __syncwarp();
     }
+}
+
+// ---------------------------------------------------------------------------
+// Plain recompute of a surrogate-refined map in one persistent launch (RefineCtx,
+// engine.cuh).
+
+template <class S>
+long long resident_s(const DevJob& J);
+
+constexpr int kExpandOnly = 1 << 30;  // queue item: re-expand a computed point (its depth dropped)
+constexpr int kQueueEmpty = -1;
+
+__device__ __forceinline__ unsigned long long vload(const unsigned long long* p)
+{
+    return *(const volatile unsigned long long*)p;
+}
+
+// Make item v visible to the consumers; the pending count rises first, so that
+// no warp sees the work finished while v is on its way.
+__device__ __forceinline__ void refine_push(const RefineCtx& R, int v)
+{
+    atomicAdd(&R.counters[3], 1ull);
+    const unsigned long long pos = atomicAdd(&R.counters[1], 1ull);
+    if (pos < R.qCap) {
+        *(volatile int*)&R.queue[pos] = v;
+    } else {  // cannot happen for a queue of the planned size; reported, never waited for
+        atomicExch(R.err, 3);
+        atomicAdd(&R.counters[3], ~0ull);
+    }
+}
+
+// The neighbours of g (Chebyshev radius) get depth <= d + 1; a neighbour reached
+// for the first time is queued for computation, one computed earlier whose depth
+// dropped is queued for another expansion if its class surprised.  The fences
+// pair with the computing lane's: either that lane reads the lowered depth, or
+// this one sees its done/surprised bits.
+__device__ void refine_expand(const RefineCtx& R, long long g, int d)
+{
+    const int row = (int)(g / R.nPts), col = (int)(g % R.nPts);
+    const int nd = d + 1;
+    atomicMax(&R.stats->deepest, nd);
+    for (int dr = -R.radius; dr <= R.radius; ++dr) {
+        const int r = row + dr;
+        if (r < 0 || r >= R.nPts) continue;
+        for (int dc = -R.radius; dc <= R.radius; ++dc) {
+            const int q = col + dc;
+            if (q < 0 || q >= R.nPts) continue;
+            const long long nb = (long long)r * R.nPts + q;
+            const int old = atomicMin(&R.depth[nb], nd);
+            if (old == kRefUnreached) {
+                refine_push(R, (int)nb);
+            } else if (nd < old && nd < R.maxDepth) {
+                __threadfence();
+                const unsigned char f = *(const volatile unsigned char*)&R.flag[nb];
+                if ((f & kRefDone) && (f & kRefSurprised)) refine_push(R, (int)nb | kExpandOnly);
+            }
+        }
+    }
+}
+
+// Surprised training labels (depth 0) seed the expansion.
+__global__ void refine_seed_kernel(const RefineCtx R)
+{
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= R.nLabel || !R.labelSurprise[k] || R.maxDepth < 1) return;
+    refine_expand(R, R.labelIdx[k], 0);
+}
+
+// Depth 0 for rule points and labels, unreached elsewhere; pending = rule count.
+__global__ void refine_init_kernel(const RefineCtx R, long long n)
+{
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g == 0) R.counters[3] = (unsigned long long)*R.nRule;
+    if (g >= n) return;
+    R.depth[g] = (R.flag[g] & (kRefLabel | kRefReasons)) ? 0 : kRefUnreached;
+}
+
+template <class S>
+__global__ void __launch_bounds__(kRegThreads, 6) regime_refine_kernel(const DevJob J, const RefineCtx R,
+                                                                       double* scrIv, int bitWords, int sortCap)
+{
+    extern __shared__ unsigned smem[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const long long warpId = (long long)blockIdx.x * kRegWarps + wib;
+    unsigned* L = smem + (size_t)wib * dbscan_warp_words(bitWords, sortCap);
+    unsigned* Sb = L + bitWords;
+    const DbscanSort so = dbscan_sort_area(L, bitWords, sortCap);
+    const long long slot0 = warpId * 32;
+    const unsigned long long nRule = (unsigned long long)*R.nRule;
+
+    for (;;) {
+        // lane 0 takes up to 32 items: expansion points first, then rule points
+        unsigned long long base = 0;
+        int cnt = 0, fromQueue = 0;
+        if (lane == 0) {
+            unsigned long long idleSince = 0;
+            for (;;) {
+                const unsigned long long t = vload(&R.counters[1]);
+                const unsigned long long tt = t < R.qCap ? t : R.qCap;
+                const unsigned long long h = vload(&R.counters[0]);
+                if (h < tt) {
+                    const unsigned long long k = tt - h < 32 ? tt - h : 32;
+                    if (atomicCAS(&R.counters[0], h, h + k) == h) {
+                        base = h;
+                        cnt = (int)k;
+                        fromQueue = 1;
+                        break;
+                    }
+                    continue;
+                }
+                if (vload(&R.counters[2]) < nRule) {
+                    const unsigned long long r = atomicAdd(&R.counters[2], 32ull);
+                    if (r < nRule) {
+                        base = r;
+                        cnt = (int)(nRule - r < 32 ? nRule - r : 32);
+                        break;
+                    }
+                }
+                if (vload(&R.counters[3]) == 0) break;  // nothing queued and nothing in flight
+                unsigned long long now;
+                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+                if (!idleSince) idleSince = now;
+                if (now - idleSince > R.maxIdleNs) {
+                    atomicExch(R.err, 2);
+                    break;
+                }
+                __nanosleep(2000);
+            }
+        }
+        cnt = __shfl_sync(kFull, cnt, 0);
+        if (cnt == 0) break;
+        base = __shfl_sync(kFull, base, 0);
+        fromQueue = __shfl_sync(kFull, fromQueue, 0);
+
+        int item = -1;
+        if (lane < cnt) {
+            if (fromQueue) {
+                // the slot was reserved before this warp took it; its value follows shortly
+                for (int spin = 0; spin < (1 << 22); ++spin) {
+                    item = *(const volatile int*)&R.queue[base + lane];
+                    if (item != kQueueEmpty) break;
+                    __nanosleep(200);
+                }
+                if (item == kQueueEmpty) atomicExch(R.err, 4);
+            } else {
+                item = (int)R.rule[base + lane];
+            }
+        }
+        const bool expandOnly = item >= 0 && (item & kExpandOnly);
+        const bool compute = item >= 0 && !expandOnly;
+        const long long g = item >= 0 ? (long long)(item & ~kExpandOnly) : 0;
+
+        double lv = 0;
+        const int res = regime_tile<S, false>(J, g, compute, cnt, lane, R.scrPk, scrIv, slot0, L, Sb, so, R.err, &lv);
+
+        // merge into the map; statistics of the predictions replaced
+        unsigned long long b = 0, lc = 0, au = 0, ao = 0, aa = 0, ch = 0, ex = 0, cp = 0;
+        double es = 0, em = 0;
+        int d = kRefUnreached;
+        bool expand = false;
+        if (compute) {
+            const unsigned char f = R.flag[g];
+            const int pc = R.mapCls[g];
+            const double pl = R.mapLle[g];
+            const bool sur = pc != res;
+            cp = 1;
+            b = (f & kRefBoundary) != 0;
+            lc = (f & kRefLowConf) != 0;
+            au = (f & kRefAudit) != 0;
+            ex = (f & kRefReasons) == 0;
+            ch = sur;
+            if ((f & kRefReasons) == kRefAudit) {
+                ao = 1;
+                aa = !sur;
+                const double e = fabs(pl - lv);
+                if (isfinite(e)) es = em = e;
+            }
+            R.mapLle[g] = lv;
+            R.mapCls[g] = res;
+            R.src[g] = 2;
+            *(volatile unsigned char*)&R.flag[g] = f | kRefDone | (sur ? kRefSurprised : 0);
+            __threadfence();
+            d = *(const volatile int*)&R.depth[g];
+            expand = sur;
+        } else if (expandOnly) {
+            d = *(const volatile int*)&R.depth[g];
+            expand = true;
+        }
+        if (expand && d < R.maxDepth) refine_expand(R, g, d);
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            b += __shfl_down_sync(kFull, b, o);
+            lc += __shfl_down_sync(kFull, lc, o);
+            au += __shfl_down_sync(kFull, au, o);
+            ao += __shfl_down_sync(kFull, ao, o);
+            aa += __shfl_down_sync(kFull, aa, o);
+            ch += __shfl_down_sync(kFull, ch, o);
+            ex += __shfl_down_sync(kFull, ex, o);
+            cp += __shfl_down_sync(kFull, cp, o);
+            es += __shfl_down_sync(kFull, es, o);
+            em = fmax(em, __shfl_down_sync(kFull, em, o));
+        }
+        __syncwarp();
+        __threadfence();
+        if (lane == 0) {
+            RefineStats* st = R.stats;
+            if (b) atomicAdd(&st->boundary, b);
+            if (lc) atomicAdd(&st->lowConf, lc);
+            if (au) atomicAdd(&st->audit, au);
+            if (ao) atomicAdd(&st->auditOnly, ao);
+            if (aa) atomicAdd(&st->auditOnlyAgree, aa);
+            if (ch) atomicAdd(&st->changed, ch);
+            if (ex) atomicAdd(&st->expanded, ex);
+            if (cp) atomicAdd(&st->computed, cp);
+            if (es != 0) atomicAdd(&st->errSum, es);
+            if (em > 0) atomicMax(&st->errMaxBits, (unsigned long long)__double_as_longlong(em));
+            atomicAdd(&R.counters[3], (unsigned long long)(-(long long)cnt));  // this tile is finished
+        }
+    }
+}
+
+template <class S>
+size_t refine_scratch_bytes_s(const DevJob& J)
+{
+    const long long resident = resident_s<S>(J);
+    return (size_t)resident * J.peakCap * sizeof(double) * 2;
+}
+
+template <class S>
+cudaError_t launch_refine_s(const DevJob& J, const RefineCtx& R, cudaStream_t s)
+{
+    const long long n = (long long)R.nPts * R.nPts;
+    const int bitWords = (J.peakCap + 31) / 32;
+    const int sortCap = dbscan_sort_cap(J.peakCap);
+    const size_t smemBytes = (size_t)kRegWarps * dbscan_warp_words(bitWords, sortCap) * sizeof(unsigned);
+    auto kern = regime_refine_kernel<S>;
+    cudaError_t e;
+    if (smemBytes > 48 * 1024) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBytes);
+        if (e != cudaSuccess) return e;
+    }
+    int dev = 0, sms = 0, perSm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, kRegThreads, smemBytes)) != cudaSuccess)
+        return e;
+    if (perSm < 1) return cudaErrorInvalidConfiguration;
+    // one block per resident slot (idle warps wait, bounded, for the expansion items of busy ones)
+    long long blocks = (long long)sms * perSm;
+    const size_t perBlock = (size_t)kRegThreads * J.peakCap * sizeof(double) * 2;
+    if ((size_t)blocks * perBlock > R.scrBytes) blocks = (long long)(R.scrBytes / perBlock);
+    if (blocks < 1) return cudaErrorInvalidValue;
+    refine_init_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(R, n);
+    note_launch();
+    if (R.nLabel > 0 && R.maxDepth > 0) {
+        refine_seed_kernel<<<(unsigned)((R.nLabel + 255) / 256), 256, 0, s>>>(R);
+        note_launch();
+    }
+    double* scrIv = R.scrPk + (size_t)blocks * kRegThreads * J.peakCap;
+    kern<<<(unsigned)blocks, kRegThreads, smemBytes, s>>>(J, R, scrIv, bitWords, sortCap);
+    note_launch();
+    return cudaGetLastError();
 }
 
 template <class S, bool IC>
@@ -246,6 +525,27 @@ long long lle_regime_resident_points(const DevJob& J)
     case CBF_SYS_LORENZ: return J.scaledStep ? resident_s<LorenzScaled>(J) : resident_s<Lorenz>(J);
     case CBF_SYS_CHEN: return J.scaledStep ? resident_s<ChenScaled>(J) : resident_s<Chen>(J);
     default: return 0;
+    }
+}
+
+size_t refine_scratch_bytes(const DevJob& J)
+{
+    switch (J.system) {
+    case CBF_SYS_ROSSLER: return refine_scratch_bytes_s<Rossler>(J);
+    case CBF_SYS_LORENZ:
+        return J.scaledStep ? refine_scratch_bytes_s<LorenzScaled>(J) : refine_scratch_bytes_s<Lorenz>(J);
+    case CBF_SYS_CHEN: return J.scaledStep ? refine_scratch_bytes_s<ChenScaled>(J) : refine_scratch_bytes_s<Chen>(J);
+    default: return 0;
+    }
+}
+
+cudaError_t launch_regime_refine(const DevJob& J, const RefineCtx& R, cudaStream_t s)
+{
+    switch (J.system) {
+    case CBF_SYS_ROSSLER: return launch_refine_s<Rossler>(J, R, s);
+    case CBF_SYS_LORENZ: return J.scaledStep ? launch_refine_s<LorenzScaled>(J, R, s) : launch_refine_s<Lorenz>(J, R, s);
+    case CBF_SYS_CHEN: return J.scaledStep ? launch_refine_s<ChenScaled>(J, R, s) : launch_refine_s<Chen>(J, R, s);
+    default: return cudaErrorInvalidValue;
     }
 }
 

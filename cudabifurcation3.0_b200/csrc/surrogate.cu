@@ -11,13 +11,17 @@
 //   * whose softmax confidence is below confThreshold,
 //   * in a seeded random audit sample (auditFraction of the grid).
 // Wherever the plain class of a label or a recomputed point differs from the
-// network's, its neighbours (expandRadius) are recomputed in a further wave, until
-// a wave finds no new disagreement: thin structures the network cannot resolve
-// (periodic windows inside chaos) are traced from any point that hits them.
-// Labelled and recomputed points carry plain values; the rest carry the
-// network's prediction.  The audit points that no other rule selected measure
+// network's, its neighbours (expandRadius) are recomputed too, and so on up to
+// an expansion depth of maxWaves steps from a rule point or label: thin
+// structures the network cannot resolve (periodic windows inside chaos) are
+// traced from any point that hits them.  The recompute is one persistent launch
+// whose warps pull work from a device queue (lle_regime.cu, RefineCtx); the set
+// of computed points, and so the map, does not depend on the order in which the
+// warps run.  Labelled and recomputed points carry plain values; the rest carry
+// the network's prediction.  The audit points that no other rule selected measure
 // the error of the kept predictions.  Everything runs on one stream; the host
-// only sizes the recompute list and normalises the LLE targets.
+// reads the labels back once (to normalise the LLE targets) and waits once at
+// the end.
 #include <math.h>
 #include <string.h>
 
@@ -32,9 +36,8 @@ namespace {
 constexpr int kChunk = 4096;          // points per compaction block
 constexpr int kChunkThreads = 256;
 // flag bits: reasons to recompute, then the point's state
-constexpr unsigned char kBoundary = 1, kLowConf = 2, kAudit = 4, kExpand = 8;
-constexpr unsigned char kReasons = kBoundary | kLowConf | kAudit | kExpand;
-constexpr unsigned char kDone = 0x40, kLabel = 0x80;
+constexpr unsigned char kBoundary = kRefBoundary, kLowConf = kRefLowConf, kAudit = kRefAudit;
+constexpr unsigned char kDone = kRefDone, kLabel = kRefLabel;
 
 __device__ __forceinline__ unsigned long long mix64(unsigned long long z)
 {
@@ -76,6 +79,24 @@ __global__ void label_scatter_kernel(const long long* __restrict__ idx, long lon
     mapCls[g] = cls[k];
     flag[g] = kLabel;
     src[g] = 1;
+}
+
+// The prediction without a network: each grid point takes the LLE and class of
+// the nearest point of the coarse label grid (labels 0..cs*cs-1, the point
+// (r*stride, c*stride) at index r*cs + c), confidence 1.
+__global__ void nearest_label_kernel(const double* __restrict__ labLle, const int* __restrict__ labCls, int cs,
+                                     int stride, int nPts, long long nPoints, double* __restrict__ lle,
+                                     int* __restrict__ cls, float* __restrict__ conf)
+{
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= nPoints) return;
+    const int row = (int)(g / nPts), col = (int)(g % nPts);
+    const int cr = min(cs - 1, (row + stride / 2) / stride);
+    const int cc = min(cs - 1, (col + stride / 2) / stride);
+    const long long k = (long long)cr * cs + cc;
+    lle[g] = labLle[k];
+    cls[g] = labCls[k];
+    conf[g] = 1.0f;
 }
 
 // Refinement reasons of every grid point from the predicted classes/confidences.
@@ -177,94 +198,6 @@ __global__ void __launch_bounds__(kChunkThreads) compact_kernel(const unsigned c
     }
 }
 
-struct Stats {
-    unsigned long long boundary, lowConf, audit, auditOnly, auditOnlyAgree, changed, expanded;
-    double errSum;
-    unsigned long long errMaxBits;
-};
-
-// Plain results into the map; statistics of the predictions they replace;
-// surprise[k] = the plain class differs from the predicted one.
-__global__ void merge_kernel(const long long* __restrict__ list, long long n, const double* __restrict__ rl,
-                             const int* __restrict__ rc, unsigned char* __restrict__ flag,
-                             double* __restrict__ mapLle, int* __restrict__ mapCls,
-                             unsigned char* __restrict__ src, unsigned char* __restrict__ surprise, Stats* st)
-{
-    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    unsigned long long b = 0, lc = 0, au = 0, ao = 0, aa = 0, ch = 0, ex = 0;
-    double es = 0, em = 0;
-    if (k < n) {
-        const long long g = list[k];
-        const unsigned char f = flag[g];
-        const int pc = mapCls[g];
-        const double pl = mapLle[g];
-        b = (f & kBoundary) != 0;
-        lc = (f & kLowConf) != 0;
-        au = (f & kAudit) != 0;
-        ex = (f & kReasons) == kExpand;
-        ch = pc != rc[k];
-        surprise[k] = (unsigned char)ch;
-        if (f == kAudit) {
-            ao = 1;
-            aa = pc == rc[k];
-            const double err = fabs(pl - rl[k]);
-            if (isfinite(err)) {
-                es = err;
-                em = err;
-            }
-        }
-        mapLle[g] = rl[k];
-        mapCls[g] = rc[k];
-        src[g] = 2;
-        flag[g] = f | kDone;
-    }
-#pragma unroll
-    for (int o = 16; o; o >>= 1) {
-        b += __shfl_down_sync(0xffffffffu, b, o);
-        lc += __shfl_down_sync(0xffffffffu, lc, o);
-        au += __shfl_down_sync(0xffffffffu, au, o);
-        ao += __shfl_down_sync(0xffffffffu, ao, o);
-        aa += __shfl_down_sync(0xffffffffu, aa, o);
-        ch += __shfl_down_sync(0xffffffffu, ch, o);
-        ex += __shfl_down_sync(0xffffffffu, ex, o);
-        es += __shfl_down_sync(0xffffffffu, es, o);
-        em = fmax(em, __shfl_down_sync(0xffffffffu, em, o));
-    }
-    if ((threadIdx.x & 31) == 0) {
-        if (b) atomicAdd(&st->boundary, b);
-        if (lc) atomicAdd(&st->lowConf, lc);
-        if (au) atomicAdd(&st->audit, au);
-        if (ao) atomicAdd(&st->auditOnly, ao);
-        if (aa) atomicAdd(&st->auditOnlyAgree, aa);
-        if (ch) atomicAdd(&st->changed, ch);
-        if (ex) atomicAdd(&st->expanded, ex);
-        if (es != 0) atomicAdd(&st->errSum, es);
-        if (em > 0) atomicMax(&st->errMaxBits, (unsigned long long)__double_as_longlong(em));
-    }
-}
-
-// Neighbours (Chebyshev radius) of every surprised point that no rule selected
-// and the plain method has not computed are marked for the next wave (rule-
-// selected points are computed in their own chunk and expand from there).
-__global__ void expand_kernel(const long long* __restrict__ list, const unsigned char* __restrict__ surprise,
-                              long long n, int nPts, int radius, unsigned char* __restrict__ flag)
-{
-    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n || !surprise[k]) return;
-    const long long g = list[k];
-    const int row = (int)(g / nPts), col = (int)(g % nPts);
-    for (int dr = -radius; dr <= radius; ++dr) {
-        const int r = row + dr;
-        if (r < 0 || r >= nPts) continue;
-        for (int dc = -radius; dc <= radius; ++dc) {
-            const int q = col + dc;
-            if (q < 0 || q >= nPts) continue;
-            const long long nb = (long long)r * nPts + q;
-            if (flag[nb] == 0) flag[nb] = kExpand;
-        }
-    }
-}
-
 template <class F>
 cudaError_t launch1d(long long n, cudaStream_t s, F f)
 {
@@ -279,7 +212,8 @@ cudaError_t launch1d(long long n, cudaStream_t s, F f)
 // map allocates nothing.  cbf_surrogate_release frees them.
 enum Slot {
     kSlotIdx, kSlotLabLle, kSlotLabCls, kSlotX, kSlotYl, kSlotConf, kSlotFlag, kSlotSrc, kSlotBlock,
-    kSlotOffsets, kSlotStats, kSlotLsur, kSlotRule, kSlotList, kSlotRl, kSlotRc, kSlotSur, kNumSlots
+    kSlotOffsets, kSlotStats, kSlotLsur, kSlotRule, kSlotDepth, kSlotQueue, kSlotCounters, kSlotErr,
+    kSlotScratch, kNumSlots
 };
 
 struct Workspace {
@@ -382,8 +316,8 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
         return report_error(CBF_ERR_INVALID_ARG, "the surrogate map covers the whole grid");
     if (job->nPts < 3 || cfg->coarseSide < 2 || cfg->randomPoints < 0 || cfg->batch < 1 ||
         cfg->trainSteps < 0 || !(cfg->lr > 0) || cfg->boundaryRadius < 0 || cfg->boundaryRadius > 8 ||
-        cfg->expandRadius < -1 || cfg->expandRadius > 16 || cfg->maxWaves < 0 ||
-        !(cfg->auditFraction >= 0 && cfg->auditFraction <= 1))
+        cfg->expandRadius < -1 || cfg->expandRadius > 16 || cfg->maxWaves < 0 || cfg->maxWaves > 1000000 ||
+        cfg->predictor < 0 || cfg->predictor > 1 || !(cfg->auditFraction >= 0 && cfg->auditFraction <= 1))
         return report_error(CBF_ERR_INVALID_ARG, "bad surrogate configuration");
     DevJob dj;
     cbf_status st = lower_job_for(job, &dj);
@@ -433,7 +367,7 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
     unsigned char *flag = nullptr, *src = dSource;
     int* blockCount = nullptr;
     long long* offsets = nullptr;
-    Stats* stats = nullptr;
+    RefineStats* stats = nullptr;
     const int nb = (int)((n + kChunk - 1) / kChunk);
     cudaError_t e = buf.get(kSlotIdx, &dIdx, nLab);
     if (e == cudaSuccess) e = buf.get(kSlotLabLle, &labLle, nLab);
@@ -500,17 +434,26 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
         return report_cuda_error(e, "network reset");
     }
     cbf_mlp* net = buf.net;
-    const int tail = cfg->trainSteps < 100 ? cfg->trainSteps : 100;
+    const bool learned = cfg->predictor == 0;
+    const int tail = !learned ? 0 : (cfg->trainSteps < 100 ? cfg->trainSteps : 100);
     std::vector<float> losses(tail > 0 ? tail : 1, 0.f);
-    st = cbf_mlp_train(net, X, yl, labCls, nLab, cfg->trainSteps - tail, cfg->lr, cfg->trainSteps, cfg->wLle,
-                       nullptr, s);
-    if (st == CBF_OK && tail > 0)
-        st = cbf_mlp_train(net, X, yl, labCls, nLab, tail, cfg->lr, cfg->trainSteps, cfg->wLle, losses.data(), s);
-    if (st != CBF_OK) return st;
+    if (learned) {
+        st = cbf_mlp_train(net, X, yl, labCls, nLab, cfg->trainSteps - tail, cfg->lr, cfg->trainSteps, cfg->wLle,
+                           nullptr, s);
+        if (st == CBF_OK && tail > 0)
+            st = cbf_mlp_train(net, X, yl, labCls, nLab, tail, cfg->lr, cfg->trainSteps, cfg->wLle, losses.data(),
+                               s);
+        if (st != CBF_OK) return st;
+    }
     cudaEventRecord(ev[2], s);
 
-    // 3. prediction on every grid point
-    e = mlp_predict_grid(net, fs, n, (float)mean, (float)sd, dLle, dCls, conf, s);
+    // 3. prediction on every grid point (the ablation: the nearest coarse label)
+    if (learned)
+        e = mlp_predict_grid(net, fs, n, (float)mean, (float)sd, dLle, dCls, conf, s);
+    else
+        e = launch1d(n, s, [&](unsigned b, int t) {
+            nearest_label_kernel<<<b, t, 0, s>>>(labLle, labCls, cs, stride, nPts, n, dLle, dCls, conf);
+        });
     if (e == cudaSuccess && dPred) e = cudaMemcpyAsync(dPred, dCls, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
     if (e != cudaSuccess) return report_cuda_error(e, "prediction");
     cudaEventRecord(ev[3], s);
@@ -535,97 +478,88 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
         e = launch1d(nLab, s, [&](unsigned b, int t) {
             label_scatter_kernel<<<b, t, 0, s>>>(dIdx, nLab, labLle, labCls, dLle, dCls, flag, src, lsur);
         });
-    if (e == cudaSuccess && er > 0)
-        e = launch1d(nLab, s, [&](unsigned b, int t) {
-            expand_kernel<<<b, t, 0, s>>>(dIdx, lsur, nLab, nPts, er, flag);
-        });
-    if (e == cudaSuccess) e = cudaMemsetAsync(stats, 0, sizeof(Stats), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(stats, 0, sizeof(RefineStats), s);
     if (e != cudaSuccess) return report_cuda_error(e, "refinement mask");
     cudaEventRecord(ev[4], s);
 
-    // 5. plain recompute in rounds.  The rule-selected points (ascending grid
-    // index) are fed in chunks; every round also takes all points the expansion
-    // marked in the previous rounds, so the chain of expansion waves overlaps
-    // the bulk of the recompute.  A round is sized to about two waves of
-    // resident threads of the LLE_REGIME kernel.
-    auto select = [&](unsigned char want, long long* out, long long* count) -> cudaError_t {
-        count_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, want, blockCount);
-        scan_kernel<<<1, 1024, 0, s>>>(blockCount, nb, offsets);
-        note_launch(2);
-        cudaError_t ce = cudaGetLastError();
-        if (ce == cudaSuccess) ce = cudaMemcpyAsync(count, offsets + nb, sizeof(long long), cudaMemcpyDeviceToHost, s);
-        if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
-        if (ce == cudaSuccess && out && *count > 0) {
-            compact_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, want, offsets, out);
-            note_launch();
-            ce = cudaGetLastError();
-        }
-        return ce;
-    };
-    long long n0 = 0;
-    if ((e = select(kBoundary | kLowConf | kAudit, nullptr, &n0)) != cudaSuccess)
-        return report_cuda_error(e, "recompute list");
+    // 5. plain recompute in one persistent launch: the rule-selected points
+    // (ascending grid index) and, from every label or computed point whose plain
+    // class differs from the prediction, its neighbours within the expansion
+    // radius, up to expansion depth maxWaves (RefineCtx, engine.cuh).  The host
+    // waits once, at the end.
+    const unsigned char want = kBoundary | kLowConf | kAudit;
     long long* rule = nullptr;
-    if ((e = buf.get(kSlotRule, &rule, n0)) != cudaSuccess) return report_cuda_error(e, "recompute list");
-    if (n0 > 0 && (e = select(kBoundary | kLowConf | kAudit, rule, &n0)) != cudaSuccess)
-        return report_cuda_error(e, "recompute list");
-    long long resident = lle_regime_resident_points(dj);
-    if (resident < 4096) resident = 4096;
-    const long long target = 2 * resident;
-    long long* list = nullptr;
-    double* rl = nullptr;
-    int* rc = nullptr;
-    unsigned char* sur = nullptr;
-    long long refined = 0, pos = 0;
-    int waves = 0;
-    for (int w = 0;; ++w) {
-        // the expansion marks of the previous rounds (counted first: sizes the chunk)
-        long long nA = 0;
-        if ((e = select(kExpand, nullptr, &nA)) != cudaSuccess) return report_cuda_error(e, "expansion list");
-        long long nB = target - nA > target / 4 ? target - nA : target / 4;
-        if (nB > n0 - pos) nB = n0 - pos;
-        const long long nSel = nA + nB;
-        if (nSel == 0) break;
-        e = buf.get(kSlotList, &list, nSel);
-        if (e == cudaSuccess) e = buf.get(kSlotRl, &rl, nSel);
-        if (e == cudaSuccess) e = buf.get(kSlotRc, &rc, nSel);
-        if (e == cudaSuccess) e = buf.get(kSlotSur, &sur, nSel);
-        if (e != cudaSuccess) return report_cuda_error(e, "recompute buffers");
-        if (nA > 0 && (e = select(kExpand, list, &nA)) != cudaSuccess) return report_cuda_error(e, "expansion list");
-        if (nB > 0 && (e = cudaMemcpyAsync(list + nA, rule + pos, nB * sizeof(long long), cudaMemcpyDeviceToDevice,
-                                           s)) != cudaSuccess)
-            return report_cuda_error(e, "recompute list");
-        cbf_job rj = *job;
-        rj.pointIndex = (const int64_t*)list;
-        rj.nPoints = nSel;
-        rj.firstPoint = 0;
-        if ((st = cbf_run(&rj, rl, rc, s)) != CBF_OK) return st;
-        e = launch1d(nSel, s, [&](unsigned b, int t) {
-            merge_kernel<<<b, t, 0, s>>>(list, nSel, rl, rc, flag, dLle, dCls, src, sur, stats);
-        });
-        if (e == cudaSuccess && er > 0 && w < cfg->maxWaves)
-            e = launch1d(nSel, s, [&](unsigned b, int t) {
-                expand_kernel<<<b, t, 0, s>>>(list, sur, nSel, nPts, er, flag);
-            });
-        if (e != cudaSuccess) return report_cuda_error(e, "merge");
-        pos += nB;
-        refined += nSel;
-        waves = w + 1;
-    }
-    Stats hs;
+    int* depth = nullptr;
+    int* queue = nullptr;
+    unsigned long long* counters = nullptr;
+    int* rerr = nullptr;
+    double* scr = nullptr;
+    const size_t scrBytes = refine_scratch_bytes(dj);
+    // each point enters the queue once for computation, and again only when its
+    // depth drops after it was expanded (rare): room for all points and half again
+    const unsigned long long qCap = (unsigned long long)n + (unsigned long long)n / 2 + 1024;
+    e = buf.get(kSlotRule, &rule, n);
+    if (e == cudaSuccess) e = buf.get(kSlotDepth, &depth, n);
+    if (e == cudaSuccess) e = buf.get(kSlotQueue, &queue, (long long)qCap);
+    if (e == cudaSuccess) e = buf.get(kSlotCounters, &counters, 4);
+    if (e == cudaSuccess) e = buf.get(kSlotErr, &rerr, 1);
+    if (e == cudaSuccess) e = buf.get(kSlotScratch, &scr, (long long)(scrBytes / sizeof(double)) + 1);
+    if (e != cudaSuccess) return report_cuda_error(e, "recompute buffers");
+    count_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, want, blockCount);
+    scan_kernel<<<1, 1024, 0, s>>>(blockCount, nb, offsets);
+    compact_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, want, offsets, rule);
+    note_launch(3);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemsetAsync(queue, 0xff, qCap * sizeof(int), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned long long), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(rerr, 0, sizeof(int), s);
+    if (e != cudaSuccess) return report_cuda_error(e, "recompute list");
+    RefineCtx R;
+    memset(&R, 0, sizeof(R));
+    R.rule = rule;
+    R.nRule = offsets + nb;
+    R.queue = queue;
+    R.qCap = qCap;
+    R.counters = counters;
+    R.depth = depth;
+    R.flag = flag;
+    R.mapLle = dLle;
+    R.mapCls = dCls;
+    R.src = src;
+    R.stats = stats;
+    R.err = rerr;
+    R.labelIdx = dIdx;
+    R.labelSurprise = lsur;
+    R.nLabel = nLab;
+    R.scrPk = scr;
+    R.scrBytes = scrBytes;
+    R.nPts = nPts;
+    R.radius = er;
+    R.maxDepth = er > 0 ? cfg->maxWaves : 0;
+    // an idle warp waits while others finish their tiles: allow far more than the
+    // integration of one point (~1e-7 s per step at most) before calling it stuck
+    const double stepsPerPoint = (double)dj.nSkip + 2.0 * (double)dj.nRecord * (double)dj.nNT;
+    R.maxIdleNs = (unsigned long long)(60e9 + stepsPerPoint * 1000.0);
+    if ((e = launch_regime_refine(dj, R, s)) != cudaSuccess) return report_cuda_error(e, "recompute");
+    RefineStats hs;
     memset(&hs, 0, sizeof(hs));
-    e = cudaMemcpyAsync(&hs, stats, sizeof(Stats), cudaMemcpyDeviceToHost, s);
+    int hostErr = 0;
+    e = cudaMemcpyAsync(&hs, stats, sizeof(RefineStats), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&hostErr, rerr, sizeof(int), cudaMemcpyDeviceToHost, s);
     cudaEventRecord(ev[5], s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return report_cuda_error(e, "recompute");
+    if (hostErr == 2 || hostErr == 4)
+        return report_error(CBF_ERR_TIMEOUT, "surrogate recompute: a bounded device-side wait gave up");
+    if (hostErr) return report_error(CBF_ERR_INTERNAL, "surrogate recompute: a device-side check failed");
 
     if (rep) {
         memset(rep, 0, sizeof(*rep));
         rep->points = n;
         rep->labelled = nLab;
-        rep->refined = refined;
+        rep->refined = (int64_t)hs.computed;
         rep->expanded = (int64_t)hs.expanded;
-        rep->waves = waves;
+        rep->waves = hs.deepest;
         rep->boundary = (int64_t)hs.boundary;
         rep->lowConfidence = (int64_t)hs.lowConf;
         rep->audit = (int64_t)hs.audit;

@@ -253,7 +253,13 @@ typedef struct cbf_surrogate_config {
     int32_t expandRadius;    /* neighbours within this radius of a point whose plain class
                                 differs from the prediction are recomputed next; -1 (default):
                                 ceil(nPts / 8192); 0: no expansion */
-    int32_t maxWaves;        /* recompute rounds that may mark expansions (20) */
+    int32_t maxWaves;        /* expansion depth: a point is recomputed through the expansion
+                                only within this many expansion steps of a rule point or
+                                label (20) */
+    int32_t predictor;       /* 0: the trained network (default); 1: no network -- every
+                                point takes the class and LLE of its nearest coarse-grid
+                                label, confidence 1 (the ablation that measures what the
+                                learning adds; same mask, audit and expansion rules) */
 } cbf_surrogate_config;
 void cbf_surrogate_config_init(cbf_surrogate_config* cfg);
 

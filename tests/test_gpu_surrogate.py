@@ -276,3 +276,24 @@ def test_facade_lle2d_writes_the_refined_map_when_opted_in(cbf, gpu_ok, tmp_path
         assert path.read_bytes() == _ref_map_csv(plain.ravel().tolist(), side, list(ranges), 6, True)
     finally:
         L.cbf_facade_set_system(-1)
+
+
+def test_trained_network_beats_the_nearest_label_predictor(cbf, gpu_ok):
+    """What the learning adds: the same pipeline (labels, mask, audit, expansion)
+    with the network replaced by the nearest coarse-grid label (predictor 1).
+    The network's map must agree with the plain map at least as well while the
+    plain method recomputes fewer points."""
+    torch = pytest.importorskip("torch")
+    side = 384
+    net = _plain_and_surrogate(cbf, torch, side, SMALL_CFG, **SMALL)
+    abl = _plain_and_surrogate(cbf, torch, side, dict(SMALL_CFG, predictor=1), **SMALL)
+    res = {}
+    for name, (pl, pc, sl, sc, src, rep) in (("network", net), ("nearest label", abl)):
+        computed = src > 0
+        assert np.array_equal(sc[computed], pc[computed])
+        res[name] = (float(np.mean(sc == pc)), float(np.mean(computed)))
+    print(res)
+    (a_net, f_net), (a_abl, f_abl) = res["network"], res["nearest label"]
+    assert a_net >= 0.995
+    assert f_net < f_abl
+    assert a_net >= a_abl - 1e-3
