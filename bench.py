@@ -63,6 +63,8 @@ SUR_WORKLOAD = dict(WORKLOAD, nPts=8192, seedChunk=200000, maxAmountOfPeaks=512,
 # FP64 work of one CD step of each system (csrc/systems.cuh; FMA = 2 flops)
 FLOPS_PER_STEP = {"chen": 19, "lorenz": 19, "rossler": 17, "memristive5": 66}
 FP64_INSTR_PER_STEP = {"chen": 14, "lorenz": 14, "rossler": 10, "memristive5": 52}
+# the rescaled Chen/Lorenz step (systems.cuh QuadScaled: 4 MUL + 6 FMA)
+SCALED_FLOPS_PER_STEP, SCALED_INSTR_PER_STEP = 16, 10
 FP64_LANES_PER_SM = 64
 
 # The other measured configurations (printed as their own JSON lines with
@@ -300,25 +302,38 @@ class ClockSampler:
                 "reasons": sorted(reasons)}
 
 
-def fp64_roofline(torch, device: int, system: str, n_points: int, spp: int, mean_ms: float,
+def step_cost(cbf, job, system: str):
+    """(flops, FP64 instructions, form) of one CD step of the job: the rescaled
+    Chen/Lorenz form (4 MUL + 6 FMA) where the job's grid admits it
+    (cbf_job_scaled_step), the 14-instruction forms otherwise."""
+    L = cbf.lib()
+    L.cbf_job_scaled_step.restype = C.c_int32
+    L.cbf_job_scaled_step.argtypes = [C.c_void_p]
+    if L.cbf_job_scaled_step(C.addressof(job)) == 1:
+        return SCALED_FLOPS_PER_STEP, SCALED_INSTR_PER_STEP, "rescaled 10-instruction CD step"
+    return FLOPS_PER_STEP[system], FP64_INSTR_PER_STEP[system], "reference-order CD step"
+
+
+def fp64_roofline(torch, device: int, cost, n_points: int, spp: int, mean_ms: float,
                   clocks: dict, probe_tflops: float) -> dict:
-    """FP64 roofline of one map: algorithmic flops and FP64-pipe instructions."""
+    """FP64 roofline of one map: algorithmic flops and FP64-pipe instructions;
+    cost = step_cost(...)."""
+    flops_step, instr_step, form = cost
     props = torch.cuda.get_device_properties(device)
     max_mhz = clocks.get("sm_max_mhz") or 1965.0
     nominal = props.multi_processor_count * FP64_LANES_PER_SM * 2 * max_mhz * 1e6 / 1e12
     peak = max(nominal, probe_tflops)
-    flops = float(n_points) * spp * FLOPS_PER_STEP[system]
+    flops = float(n_points) * spp * flops_step
     achieved = flops / (mean_ms / 1e3) / 1e12
     sm_mhz = clocks.get("sm_mhz") or max_mhz
-    instr = float(n_points) * spp * FP64_INSTR_PER_STEP[system]
+    instr = float(n_points) * spp * instr_step
     pipe = instr / (mean_ms / 1e3) / (props.multi_processor_count * FP64_LANES_PER_SM * sm_mhz * 1e6)
     return {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak,
             "peak_source": "max(nominal SMs x 64 FP64 lanes x 2 flops x max SM clock, FP64 FMA "
                            "probe measured in this run); MEASURED_PEAKS.json has no FP64 figure",
             "peak_nominal": nominal, "peak_probe": probe_tflops, "flops_per_launch": flops,
-            "flops_per_step": FLOPS_PER_STEP[system],
-            "fp64_instr_per_step": FP64_INSTR_PER_STEP[system],
+            "flops_per_step": flops_step, "fp64_instr_per_step": instr_step, "step_form": form,
             "fp64_pipe_frac": pipe}
 
 
@@ -490,7 +505,7 @@ def run_secondary(args, name: str) -> int:
     clocks = sampler.stop()
     t = statistics.mean(ms)
     probe = cbf.probe_fp64_peak(300.0)
-    roof = fp64_roofline(torch, 0, w["system"], n, spp, t, clocks, probe)
+    roof = fp64_roofline(torch, 0, step_cost(cbf, job, w["system"]), n, spp, t, clocks, probe)
     roof["traffic"] = None
     roof["note"] = ("integration flops only (base + perturbed trajectories); Gram-Schmidt and log "
                     "per interval on top") if task == cbf.TASK_LS else \
@@ -679,6 +694,24 @@ def run_surrogate(args) -> int:
                     np.array_equal(h_lle, s_lle.cpu().numpy(), equal_nan=True))
     e2e_h2d = int(sum(a.nbytes for a in e2e_in) + C.sizeof(rules) + C.sizeof(cfg))
 
+    # What the learning adds: one map with the network replaced by the nearest
+    # coarse-grid label (same labels, mask, audit and expansion rules).
+    abl_cfg = cbf.surrogate_config(predictor=1)
+    with torch.cuda.stream(stream):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+    abl_rep = cbf.lle_map_surrogate(job, abl_cfg, s_lle.data_ptr(), s_cls.data_ptr(), s_src.data_ptr(),
+                                    stream=stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        e1.record(stream)
+    stream.synchronize()
+    ablation = {"predictor": "nearest coarse-grid label, no network", "ms": e0.elapsed_time(e1),
+                "regime_agreement": float((s_cls == p_cls).double().mean().item()),
+                "computed_fraction": float((s_src > 0).double().mean().item()),
+                "refined": int(abl_rep.refined), "waves": int(abl_rep.waves)}
+
     r = reps[-1].as_dict()
     plain_points = r["labelled"] + r["refined"]
     plain_phase_ms = r["msLabel"] + r["msRefine"]
@@ -686,16 +719,21 @@ def run_surrogate(args) -> int:
     max_mhz = clocks.get("sm_max_mhz") or 1965.0
     nominal = props.multi_processor_count * FP64_LANES_PER_SM * 2 * max_mhz * 1e6 / 1e12
     peak = max(nominal, probe)
-    flops = float(plain_points) * spp * FLOPS_PER_STEP["chen"]
+    flops_step, instr_step, form = step_cost(cbf, job, "chen")
+    flops = float(plain_points) * spp * flops_step
     achieved = flops / (plain_phase_ms / 1e3) / 1e12
-    plain_achieved = float(n) * spp * FLOPS_PER_STEP["chen"] / (plain_ms / 1e3) / 1e12
+    plain_achieved = float(n) * spp * flops_step / (plain_ms / 1e3) / 1e12
+    pipe_den = props.multi_processor_count * FP64_LANES_PER_SM * (clocks.get("sm_mhz") or max_mhz) * 1e6
     roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak,
             "kernel": "lle_regime_kernel (plain FP64 labels + recompute rounds of the refined map)",
             "peak_source": "max(nominal SMs x 64 FP64 lanes x 2 flops x max SM clock, FP64 FMA "
                            "probe measured in this run); MEASURED_PEAKS.json has no FP64 figure",
             "peak_nominal": nominal, "peak_probe": probe,
-            "flops_per_step": FLOPS_PER_STEP["chen"], "steps_per_point": spp,
+            "flops_per_step": flops_step, "fp64_instr_per_step": instr_step, "step_form": form,
+            "fp64_pipe_frac": float(plain_points) * spp * instr_step / (plain_phase_ms / 1e3) / pipe_den,
+            "plain_map_fp64_pipe_frac": float(n) * spp * instr_step / (plain_ms / 1e3) / pipe_den,
+            "steps_per_point": spp,
             "plain_points_in_step": plain_points, "plain_phase_ms": plain_phase_ms,
             "plain_map_achieved": plain_achieved, "plain_map_frac": plain_achieved / peak,
             "traffic": regime_traffic(plain_points)}
@@ -732,6 +770,7 @@ def run_surrogate(args) -> int:
                           "kept_lle_p99_abs_err": float(torch.quantile(kept_err[:1 << 24].float(), 0.99).item())
                           if kept_err.numel() else None},
             "report": r,
+            "ablation_no_network": ablation,
             "e2e": {"value": e2e_value, "unit": "points/s", "h2d_bytes_per_step": e2e_h2d,
                     "d2h_bytes_per_step": n * 12, "matches_device_api": e2e_same,
                     "call": "cbf_lle2d_surrogate (LLE2D's arguments, host arrays in and out)"},
@@ -864,7 +903,7 @@ def main(argv=None) -> int:
     e2e_value = world * n * len(e2e_times) / float(e2e_total.item())
     same = np.array_equal(res, out.cpu().numpy(), equal_nan=True)
 
-    roof = fp64_roofline(torch, local, w["system"], n, spp, statistics.mean(kernel_ms),
+    roof = fp64_roofline(torch, local, step_cost(cbf, job, w["system"]), n, spp, statistics.mean(kernel_ms),
                          clocks, probe)
     roof["traffic"] = traffic_from_profiles()
 
