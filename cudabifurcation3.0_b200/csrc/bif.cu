@@ -265,9 +265,11 @@ cudaError_t launch_bif_s(const DevJob& J, void* d_out, int* d_aux, cudaStream_t 
     }
 }
 
+// One pass of the fused kernel with caller-provided scratch (no allocation);
+// synchronises `s` to read the error flag.
 template <class S, int TASK>
-cudaError_t launch_bif_prealloc_t(const DevJob& J, void* d_out, double* scratch, size_t scratchBytes,
-                                  int* err, cudaStream_t s)
+cudaError_t prealloc_pass(const DevJob& J, void* d_out, double* scratch, size_t scratchBytes, int* err,
+                          const Overflow& ov, cudaStream_t s)
 {
     const long long nTiles = (J.nPoints + 31) / 32;
     if (nTiles == 0) return cudaSuccess;
@@ -296,13 +298,79 @@ cudaError_t launch_bif_prealloc_t(const DevJob& J, void* d_out, double* scratch,
     if (blocks > fit) blocks = fit;
     double* scrInt = (TASK == CBF_TASK_DBSCAN) ? scratch + (size_t)blocks * kBifThreads * J.peakCap : nullptr;
     kern<<<(unsigned)blocks, kBifThreads, smemBytes, s>>>(J, d_out, nullptr, scratch, scrInt, bitWords, sortCap,
-                                                          err, Overflow{nullptr, nullptr, nullptr});
+                                                          err, ov);
     note_launch();
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     int hostErr = 0;
     if ((e = cudaMemcpyAsync(&hostErr, err, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
     return hostErr ? cudaErrorAssert : cudaSuccess;
+}
+
+// KDE / DBSCAN map with caller-provided scratch, in the regular entry point's two
+// passes: when the peak capacity exceeds kFirstPassPeaks, a first pass at that
+// capacity (many more blocks fit the scratch) lists the points whose peaks did
+// not fit, a second pass recomputes them at full capacity and their results are
+// scattered into place -- the same per-point code, the same map.  The scratch
+// holds the overflow list (grid index and slot, 16 B per point) and the second
+// pass's results (4 B per point) of a chunk of points in front of the peak
+// buffers; the chunk is sized so that the list takes at most a quarter of the
+// scratch and one block still fits at full capacity.  Without room for that,
+// every point runs once at full capacity.
+template <class S, int TASK>
+cudaError_t launch_bif_prealloc_t(const DevJob& J, void* d_out, double* scratch, size_t scratchBytes,
+                                  int* err, cudaStream_t s)
+{
+    const Overflow none{nullptr, nullptr, nullptr};
+    if (J.nPoints == 0) return cudaSuccess;
+    const size_t perBlockFull = (size_t)kBifThreads * J.peakCap * sizeof(double) * (task_with_intervals(TASK) ? 2 : 1);
+    const size_t perPoint = 2 * sizeof(long long) + sizeof(int);
+    size_t listBytes = scratchBytes / 4;
+    if (scratchBytes < perBlockFull + 1024) listBytes = 0;
+    else if (listBytes > scratchBytes - perBlockFull - 1024) listBytes = scratchBytes - perBlockFull - 1024;
+    long long chunk = (long long)(listBytes / perPoint);
+    if (J.peakCap <= kFirstPassPeaks || chunk < 32)
+        return prealloc_pass<S, TASK>(J, d_out, scratch, scratchBytes, err, none, s);
+    if (chunk > J.nPoints) chunk = J.nPoints;
+    char* base = (char*)scratch;
+    long long* listG = (long long*)base;
+    long long* listP = listG + chunk;
+    int* tmp = (int*)(listP + chunk);
+    const size_t countOff = ((size_t)((char*)(tmp + chunk) - base) + 255) / 256 * 256;
+    unsigned long long* count = (unsigned long long*)(base + countOff);
+    const size_t peakOff = countOff + 256;
+    double* peaks = (double*)(base + peakOff);
+    const size_t peakBytes = scratchBytes - peakOff;
+    cudaError_t e = cudaSuccess;
+    for (long long first = 0; first < J.nPoints && e == cudaSuccess; first += chunk) {
+        const long long m = (J.nPoints - first < chunk) ? J.nPoints - first : chunk;
+        DevJob J1 = J;
+        if (J.pointIndex) J1.pointIndex = J.pointIndex + first;
+        else J1.firstPoint = J.firstPoint + first;
+        J1.nPoints = m;
+        J1.peakCap = kFirstPassPeaks;
+        int* out = (int*)d_out + first;
+        unsigned long long n2 = 0;
+        e = cudaMemsetAsync(count, 0, sizeof(unsigned long long), s);
+        if (e == cudaSuccess) e = prealloc_pass<S, TASK>(J1, out, peaks, peakBytes, err, Overflow{listG, listP, count}, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&n2, count, sizeof(n2), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e == cudaSuccess && n2 > 0) {
+            DevJob J2 = J;
+            J2.pointIndex = listG;
+            J2.firstPoint = 0;
+            J2.nPoints = (long long)n2;
+            e = prealloc_pass<S, TASK>(J2, tmp, peaks, peakBytes, err, none, s);
+            if (e == cudaSuccess) {
+                scatter_kernel<int><<<(unsigned)(((long long)n2 + 255) / 256), 256, 0, s>>>(tmp, listP, (long long)n2,
+                                                                                         out);
+                note_launch();
+                e = cudaGetLastError();
+            }
+        }
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e;
 }
 
 template <class S>

@@ -13,6 +13,10 @@
 // memory and belongs at start-up.  A device keeps the array until the process
 // exits.  Each call waits for its stream to finish, to read the error flag.
 //
+// Maps with long peak lists run the regular entry point's two passes inside the
+// array (a first pass with 1024 peak slots per point, the overflow points again
+// at full capacity), so that many more blocks fit than at full capacity.
+//
 // The array is shared by every call: calls that overlap on the GPU (from several
 // host threads, or on several streams) race on it and must be serialised by the
 // caller.  Its first 256 bytes hold the kernel's error flag, which every call
