@@ -123,3 +123,47 @@ def test_batch_rejects_bad_jobs(cbf, gpu_ok):
         job = cbf.make_job(task=task, system="chen", nPts=4, h=0.01, tMax=1.0, **extra, **SYS["chen"])
         with pytest.raises(cbf.CbfError, match="batched"):
             cbf.Batch([job], [outs[0].data_ptr()], [outs[0].data_ptr()])
+
+
+def test_seeded_64_job_mix_matches_the_oracle(cbf, orc, gpu_ok):
+    """The benchmark's seeded 64-job batch (bench.batch_specs: systems, tasks, grid
+    sides, record lengths and step sizes drawn from seed 20240101), with every grid
+    cut to a few points per axis and every record and transient cut 100x / 20x so
+    that the oracle finishes in seconds, in one persistent launch: each job
+    against the CPU oracle directly -- KDE and DBSCAN counts bit-exact, LLE within
+    1e-9 from the device's seeds."""
+    torch = pytest.importorskip("torch")
+    import sys
+    from pathlib import Path
+    root = str(Path(__file__).resolve().parents[1])
+    if root not in sys.path:
+        sys.path.insert(0, root)
+    import bench
+    from test_gpu_parity import assert_lle_close
+    specs = bench.batch_specs()
+    assert len(specs) == 64
+    jobs, kinds, okw = [], [], []
+    for sp in specs:
+        sp = dict(sp)
+        task = sp.pop("task")
+        sp.update(nPts=max(3, sp["nPts"] // 128), tMax=sp["tMax"] / 100.0, transientTime=sp["transientTime"] / 20.0)
+        jobs.append(cbf.make_job(task=task, **sp))
+        kinds.append(task)
+        okw.append(sp)
+    outs, auxs = _buffers(cbf, torch, jobs, kinds)
+    b = cbf.Batch(jobs, [o.data_ptr() for o in outs])
+    b.run()
+    torch.cuda.synchronize()
+    b.check()
+    assert {cbf.TASK_LLE, cbf.TASK_KDE, cbf.TASK_DBSCAN} <= set(kinds)
+    for j, t, kw, o in zip(jobs, kinds, okw, outs):
+        got = o.cpu().numpy()
+        oj = orc.make_job(**kw)
+        n = kw["nPts"] ** 2
+        if t == cbf.TASK_LLE:
+            assert_lle_close(got, orc.map_lle_seeded(oj, 0, n, cbf.lle_seeds(j)))
+        elif t == cbf.TASK_KDE:
+            assert np.array_equal(got, orc.map_kde(oj, 0, n)), kw
+        else:
+            assert np.array_equal(got, orc.map_dbscan(oj, 0, n)), kw
+    b.close()
