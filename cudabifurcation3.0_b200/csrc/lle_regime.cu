@@ -188,6 +188,9 @@ long long resident_s(const DevJob& J);
 
 constexpr int kExpandOnly = 1 << 30;  // queue item: re-expand a computed point (its depth dropped)
 constexpr int kQueueEmpty = -1;
+// A queue holding fewer than 32 points waits this long for more before a warp
+// takes them as a partial tile (one point's integration takes tens of ms).
+constexpr unsigned long long kPartialWaitNs = 2000000ull;
 
 __device__ __forceinline__ unsigned long long vload(const unsigned long long* p)
 {
@@ -269,7 +272,11 @@ __global__ void __launch_bounds__(kRegThreads, 6) regime_refine_kernel(const Dev
     const unsigned long long nRule = (unsigned long long)*R.nRule;
 
     for (;;) {
-        // lane 0 takes up to 32 items: expansion points first, then rule points
+        // Lane 0 takes a tile: 32 queued expansion points if there are that many,
+        // else 32 rule points, else -- once the rule list is spent -- a partial
+        // tile of the queue, but only when no tile in flight can still add to it
+        // or the queue has waited kPartialWaitNs: a warp busy for a whole point
+        // integration on a few lanes would waste the rest of its lanes.
         unsigned long long base = 0;
         int cnt = 0, fromQueue = 0;
         if (lane == 0) {
@@ -278,8 +285,18 @@ __global__ void __launch_bounds__(kRegThreads, 6) regime_refine_kernel(const Dev
                 const unsigned long long t = vload(&R.counters[1]);
                 const unsigned long long tt = t < R.qCap ? t : R.qCap;
                 const unsigned long long h = vload(&R.counters[0]);
-                if (h < tt) {
-                    const unsigned long long k = tt - h < 32 ? tt - h : 32;
+                const unsigned long long avail = h < tt ? tt - h : 0;
+                const bool ruleLeft = vload(&R.counters[2]) < nRule;
+                unsigned long long now;
+                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+                if (avail > 0 && !idleSince) idleSince = now;
+                bool takeQueue = avail >= 32;
+                if (!takeQueue && avail > 0 && !ruleLeft) {
+                    const unsigned long long pending = vload(&R.counters[3]);
+                    takeQueue = pending <= avail || now - idleSince > kPartialWaitNs;  // nothing else in flight
+                }
+                if (takeQueue) {
+                    const unsigned long long k = avail < 32 ? avail : 32;
                     if (atomicCAS(&R.counters[0], h, h + k) == h) {
                         base = h;
                         cnt = (int)k;
@@ -288,17 +305,16 @@ __global__ void __launch_bounds__(kRegThreads, 6) regime_refine_kernel(const Dev
                     }
                     continue;
                 }
-                if (vload(&R.counters[2]) < nRule) {
+                if (ruleLeft) {
                     const unsigned long long r = atomicAdd(&R.counters[2], 32ull);
                     if (r < nRule) {
                         base = r;
                         cnt = (int)(nRule - r < 32 ? nRule - r : 32);
                         break;
                     }
+                    continue;
                 }
                 if (vload(&R.counters[3]) == 0) break;  // nothing queued and nothing in flight
-                unsigned long long now;
-                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
                 if (!idleSince) idleSince = now;
                 if (now - idleSince > R.maxIdleNs) {
                     atomicExch(R.err, 2);
