@@ -707,9 +707,12 @@ def run_surrogate(args) -> int:
     with torch.cuda.stream(stream):
         e1.record(stream)
     stream.synchronize()
+    abl_err = (s_lle - p_lle).abs()
+    abl_kept = (s_src == 0) & torch.isfinite(abl_err)
     ablation = {"predictor": "nearest coarse-grid label, no network", "ms": e0.elapsed_time(e1),
                 "regime_agreement": float((s_cls == p_cls).double().mean().item()),
                 "computed_fraction": float((s_src > 0).double().mean().item()),
+                "kept_lle_mean_abs_err": float(abl_err[abl_kept].mean().item()) if abl_kept.any() else None,
                 "refined": int(abl_rep.refined), "waves": int(abl_rep.waves)}
 
     r = reps[-1].as_dict()
