@@ -149,6 +149,7 @@ class SurrogateReport(C.Structure):
         ("msTotal", C.c_double),
         ("expanded", C.c_int64),
         ("waves", C.c_int32),
+        ("refineTiles", C.c_int64),
     ]
 
     def as_dict(self):

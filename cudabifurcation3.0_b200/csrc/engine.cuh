@@ -205,6 +205,7 @@ struct RefineStats {
     unsigned long long errMaxBits;
     int deepest;  // largest expansion depth reached
     int pad;
+    unsigned long long tiles;  // warp tiles run (lane use = computed / (32 tiles))
 };
 
 // One persistent launch that computes every rule-selected point (rule[0..*nRule),

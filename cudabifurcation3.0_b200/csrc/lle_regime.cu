@@ -408,6 +408,7 @@ __global__ void __launch_bounds__(kRegThreads, 6) regime_refine_kernel(const Dev
             if (ch) atomicAdd(&st->changed, ch);
             if (ex) atomicAdd(&st->expanded, ex);
             if (cp) atomicAdd(&st->computed, cp);
+            atomicAdd(&st->tiles, 1ull);
             if (es != 0) atomicAdd(&st->errSum, es);
             if (em > 0) atomicMax(&st->errMaxBits, (unsigned long long)__double_as_longlong(em));
             atomicAdd(&R.counters[3], (unsigned long long)(-(long long)cnt));  // this tile is finished

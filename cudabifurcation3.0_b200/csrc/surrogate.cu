@@ -560,6 +560,7 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
         rep->refined = (int64_t)hs.computed;
         rep->expanded = (int64_t)hs.expanded;
         rep->waves = hs.deepest;
+        rep->refineTiles = (int64_t)hs.tiles;
         rep->boundary = (int64_t)hs.boundary;
         rep->lowConfidence = (int64_t)hs.lowConf;
         rep->audit = (int64_t)hs.audit;

@@ -278,7 +278,9 @@ typedef struct cbf_surrogate_report {
     float finalLoss;           /* mean training loss over the last 100 steps */
     double msLabel, msTrain, msPredict, msMask, msRefine, msTotal;  /* stream time */
     int64_t expanded;          /* recomputed points selected only by the expansion */
-    int32_t waves;             /* recompute rounds run */
+    int32_t waves;             /* largest expansion depth reached */
+    int64_t refineTiles;       /* 32-lane warp tiles the recompute ran (lane use =
+                                  refined / (32 * refineTiles)) */
 } cbf_surrogate_report;
 
 /* job: a whole-grid 2-D CBF_TASK_LLE_REGIME sweep of the Rossler, Lorenz or
