@@ -223,7 +223,8 @@ struct RefineCtx {
     const long long* nRule;        // device count of rule
     int* queue;                    // expansion queue, qCap slots, -1 = not yet written
     unsigned long long qCap;
-    unsigned long long* counters;  // [0] queue head, [1] queue tail, [2] rule head, [3] pending items
+    unsigned long long* counters;  // [0] queue head, [1] queue tail, [2] rule head, [3] pending items,
+                                   // [4] busy warps
     int* depth;                    // per grid point
     unsigned char* flag;           // per grid point (kRef* bits)
     double* mapLle;

@@ -188,9 +188,6 @@ long long resident_s(const DevJob& J);
 
 constexpr int kExpandOnly = 1 << 30;  // queue item: re-expand a computed point (its depth dropped)
 constexpr int kQueueEmpty = -1;
-// A queue holding fewer than 32 points waits this long for more before a warp
-// takes them as a partial tile (one point's integration takes tens of ms).
-constexpr unsigned long long kPartialWaitNs = 2000000ull;
 
 __device__ __forceinline__ unsigned long long vload(const unsigned long long* p)
 {
@@ -275,12 +272,14 @@ __global__ void __launch_bounds__(kRegThreads, 6) regime_refine_kernel(const Dev
         // Lane 0 takes a tile: 32 queued expansion points if there are that many,
         // else 32 rule points, else -- once the rule list is spent -- a partial
         // tile of the queue, but only when no tile in flight can still add to it
-        // or the queue has waited kPartialWaitNs: a warp busy for a whole point
-        // integration on a few lanes would waste the rest of its lanes.
+        // or fewer than a quarter of the warps are busy.  A warp's FP64
+        // instructions cost the pipe the same with 1 active lane as with 32, so
+        // partial tiles on a busy device would slow every other tile down.
         unsigned long long base = 0;
         int cnt = 0, fromQueue = 0;
         if (lane == 0) {
             unsigned long long idleSince = 0;
+            const unsigned long long quarter = (unsigned long long)gridDim.x * kRegWarps / 4;
             for (;;) {
                 const unsigned long long t = vload(&R.counters[1]);
                 const unsigned long long tt = t < R.qCap ? t : R.qCap;
@@ -289,11 +288,10 @@ __global__ void __launch_bounds__(kRegThreads, 6) regime_refine_kernel(const Dev
                 const bool ruleLeft = vload(&R.counters[2]) < nRule;
                 unsigned long long now;
                 asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
-                if (avail > 0 && !idleSince) idleSince = now;
                 bool takeQueue = avail >= 32;
                 if (!takeQueue && avail > 0 && !ruleLeft) {
                     const unsigned long long pending = vload(&R.counters[3]);
-                    takeQueue = pending <= avail || now - idleSince > kPartialWaitNs;  // nothing else in flight
+                    takeQueue = pending <= avail || vload(&R.counters[4]) < quarter;
                 }
                 if (takeQueue) {
                     const unsigned long long k = avail < 32 ? avail : 32;
@@ -322,6 +320,7 @@ __global__ void __launch_bounds__(kRegThreads, 6) regime_refine_kernel(const Dev
                 }
                 __nanosleep(2000);
             }
+            if (cnt > 0) atomicAdd(&R.counters[4], 1ull);  // busy warps
         }
         cnt = __shfl_sync(kFull, cnt, 0);
         if (cnt == 0) break;
@@ -412,6 +411,7 @@ __global__ void __launch_bounds__(kRegThreads, 6) regime_refine_kernel(const Dev
             if (es != 0) atomicAdd(&st->errSum, es);
             if (em > 0) atomicMax(&st->errMaxBits, (unsigned long long)__double_as_longlong(em));
             atomicAdd(&R.counters[3], (unsigned long long)(-(long long)cnt));  // this tile is finished
+            atomicAdd(&R.counters[4], ~0ull);
         }
     }
 }
