@@ -269,10 +269,10 @@ __global__ void __launch_bounds__(kRegThreads, 6) regime_refine_kernel(const Dev
     const unsigned long long nRule = (unsigned long long)*R.nRule;
 
     for (;;) {
-        // Lane 0 takes a tile: 32 queued expansion points if there are that many,
-        // else 32 rule points, else -- once the rule list is spent -- a partial
-        // tile of the queue, but only when no tile in flight can still add to it
-        // or fewer than a quarter of the warps are busy.  A warp's FP64
+        // Lane 0 takes a tile: 32 rule points while any are left, then 32 queued
+        // expansion points, and a partial tile of the queue only when no tile in
+        // flight can still add to it or fewer than a quarter of the warps are
+        // busy.  A warp's FP64
         // instructions cost the pipe the same with 1 active lane as with 32, so
         // partial tiles on a busy device would slow every other tile down.
         unsigned long long base = 0;
@@ -288,7 +288,9 @@ __global__ void __launch_bounds__(kRegThreads, 6) regime_refine_kernel(const Dev
                 const bool ruleLeft = vload(&R.counters[2]) < nRule;
                 unsigned long long now;
                 asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
-                bool takeQueue = avail >= 32;
+                // rule points first: every expansion chain starts from one of them
+                // or a label, so the chains get going as early as possible
+                bool takeQueue = !ruleLeft && avail >= 32;
                 if (!takeQueue && avail > 0 && !ruleLeft) {
                     const unsigned long long pending = vload(&R.counters[3]);
                     takeQueue = pending <= avail || vload(&R.counters[4]) < quarter;
