@@ -224,7 +224,7 @@ struct RefineCtx {
     int* queue;                    // expansion queue, qCap slots, -1 = not yet written
     unsigned long long qCap;
     unsigned long long* counters;  // [0] queue head, [1] queue tail, [2] rule head, [3] pending items,
-                                   // [4] busy warps
+                                   // [4] busy warps, [5] time a short queue started waiting
     int* depth;                    // per grid point
     unsigned char* flag;           // per grid point (kRef* bits)
     double* mapLle;

@@ -188,6 +188,9 @@ long long resident_s(const DevJob& J);
 
 constexpr int kExpandOnly = 1 << 30;  // queue item: re-expand a computed point (its depth dropped)
 constexpr int kQueueEmpty = -1;
+// A queue shorter than a tile is taken as a partial tile once it has waited this
+// long (a point's integration takes ~0.1 s on a busy device).
+constexpr unsigned long long kStarveNs = 20000000ull;
 
 __device__ __forceinline__ unsigned long long vload(const unsigned long long* p)
 {
@@ -245,13 +248,29 @@ __global__ void refine_seed_kernel(const RefineCtx R)
     refine_expand(R, R.labelIdx[k], 0);
 }
 
-// Depth 0 for rule points and labels, unreached elsewhere; pending = rule count.
+// Depth 0 for labels, unreached elsewhere (rule points get theirs below);
+// pending = rule count.
 __global__ void refine_init_kernel(const RefineCtx R, long long n)
 {
     const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (g == 0) R.counters[3] = (unsigned long long)*R.nRule;
     if (g >= n) return;
-    R.depth[g] = (R.flag[g] & (kRefLabel | kRefReasons)) ? 0 : kRefUnreached;
+    R.depth[g] = (R.flag[g] & kRefLabel) ? 0 : kRefUnreached;
+}
+
+// Rule point i (ascending grid index) starts at depth i * maxDepth / nRule: the
+// rule points enter the expansion spread over its depth levels, so that the
+// deepest chain -- and the whole recompute -- ends after about maxDepth tile
+// durations however many rule points there are; the rule points late in the
+// list get the fewer expansion steps.  Depths stay a pure function of the map
+// (the least start depth plus path length over all roots), whatever order the
+// warps run in.
+__global__ void refine_rule_depth_kernel(const RefineCtx R, long long cap)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nRule = *R.nRule;
+    if (i >= nRule || i >= cap) return;
+    R.depth[R.rule[i]] = (int)(((long long)R.maxDepth * i) / nRule);
 }
 
 template <class S>
@@ -288,16 +307,23 @@ __global__ void __launch_bounds__(kRegThreads, 6) regime_refine_kernel(const Dev
                 const bool ruleLeft = vload(&R.counters[2]) < nRule;
                 unsigned long long now;
                 asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
-                // rule points first: every expansion chain starts from one of them
-                // or a label, so the chains get going as early as possible
-                bool takeQueue = !ruleLeft && avail >= 32;
-                if (!takeQueue && avail > 0 && !ruleLeft) {
-                    const unsigned long long pending = vload(&R.counters[3]);
-                    takeQueue = pending <= avail || vload(&R.counters[4]) < quarter;
+                bool takeQueue = avail >= 32;
+                if (!takeQueue && avail > 0) {
+                    if (!ruleLeft && (vload(&R.counters[3]) <= avail || vload(&R.counters[4]) < quarter)) {
+                        takeQueue = true;
+                    } else {
+                        // a short queue may not wait for ever: an expansion chain
+                        // stalled here would finish alone at the end, one level
+                        // after the other
+                        const unsigned long long since = vload(&R.counters[5]);
+                        if (since == 0) atomicCAS(&R.counters[5], 0ull, now);
+                        else if (now - since > kStarveNs) takeQueue = true;
+                    }
                 }
                 if (takeQueue) {
                     const unsigned long long k = avail < 32 ? avail : 32;
                     if (atomicCAS(&R.counters[0], h, h + k) == h) {
+                        atomicExch(&R.counters[5], 0ull);
                         base = h;
                         cnt = (int)k;
                         fromQueue = 1;
@@ -450,7 +476,8 @@ cudaError_t launch_refine_s(const DevJob& J, const RefineCtx& R, cudaStream_t s)
     if ((size_t)blocks * perBlock > R.scrBytes) blocks = (long long)(R.scrBytes / perBlock);
     if (blocks < 1) return cudaErrorInvalidValue;
     refine_init_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(R, n);
-    note_launch();
+    refine_rule_depth_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(R, n);
+    note_launch(2);
     if (R.nLabel > 0 && R.maxDepth > 0) {
         refine_seed_kernel<<<(unsigned)((R.nLabel + 255) / 256), 256, 0, s>>>(R);
         note_launch();

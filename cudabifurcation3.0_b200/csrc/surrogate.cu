@@ -501,7 +501,7 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
     e = buf.get(kSlotRule, &rule, n);
     if (e == cudaSuccess) e = buf.get(kSlotDepth, &depth, n);
     if (e == cudaSuccess) e = buf.get(kSlotQueue, &queue, (long long)qCap);
-    if (e == cudaSuccess) e = buf.get(kSlotCounters, &counters, 5);
+    if (e == cudaSuccess) e = buf.get(kSlotCounters, &counters, 6);
     if (e == cudaSuccess) e = buf.get(kSlotErr, &rerr, 1);
     if (e == cudaSuccess) e = buf.get(kSlotScratch, &scr, (long long)(scrBytes / sizeof(double)) + 1);
     if (e != cudaSuccess) return report_cuda_error(e, "recompute buffers");
@@ -511,7 +511,7 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
     note_launch(3);
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemsetAsync(queue, 0xff, qCap * sizeof(int), s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(counters, 0, 5 * sizeof(unsigned long long), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(counters, 0, 6 * sizeof(unsigned long long), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(rerr, 0, sizeof(int), s);
     if (e != cudaSuccess) return report_cuda_error(e, "recompute list");
     RefineCtx R;
