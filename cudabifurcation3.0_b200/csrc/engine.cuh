@@ -188,63 +188,14 @@ cudaError_t launch_ls_seeds(const DevJob& J, double* d_out, cudaStream_t s);
 cudaError_t launch_lle_regime(const DevJob& J, double* d_lle, int* d_class, cudaStream_t s);
 // Points the LLE_REGIME kernel keeps in flight at once on the current device.
 long long lle_regime_resident_points(const DevJob& J);
+// The LLE_REGIME kernel over a device point list (J.pointIndex) whose length
+// *nDev (at most maxPoints) a previous kernel wrote, with caller-provided
+// scratch of lle_regime_scratch_bytes(J); no allocation, no host
+// synchronisation: a device-side check sets *err (zero on entry).
+size_t lle_regime_scratch_bytes(const DevJob& J);
+cudaError_t launch_lle_regime_list(const DevJob& J, const long long* nDev, long long maxPoints, double* d_lle,
+                                   int* d_cls, double* scratch, size_t scratchBytes, int* err, cudaStream_t s);
 
-// ---- plain recompute of a surrogate-refined map (lle_regime.cu) -----------
-// Per-point state bits of the refinement (one byte per grid point).
-constexpr unsigned char kRefBoundary = 1, kRefLowConf = 2, kRefAudit = 4;
-constexpr unsigned char kRefReasons = kRefBoundary | kRefLowConf | kRefAudit;
-constexpr unsigned char kRefSurprised = 0x20;  // plain class differs from the prediction
-constexpr unsigned char kRefDone = 0x40, kRefLabel = 0x80;
-constexpr int kRefUnreached = 0x7fffffff;     // expansion depth of a point nobody reached
-
-// Counters of the recompute (all points it computed; the audit-only fields
-// measure the predictions that no other rule replaced).
-struct RefineStats {
-    unsigned long long boundary, lowConf, audit, auditOnly, auditOnlyAgree, changed, expanded, computed;
-    double errSum;
-    unsigned long long errMaxBits;
-    int deepest;  // largest expansion depth reached
-    int pad;
-    unsigned long long tiles;  // warp tiles run (lane use = computed / (32 tiles))
-};
-
-// One persistent launch that computes every rule-selected point (rule[0..*nRule),
-// ascending grid indices) and, from every computed point or training label whose
-// plain class differs from the prediction, the neighbours within `radius` up to
-// expansion depth maxDepth.  Warps pull 32-point tiles from a device queue of
-// expansion points first and from the rule list otherwise; a point's depth is the
-// least number of expansion steps from a rule point or label (lowered atomically,
-// and re-propagated when it drops after the point was expanded), so the set of
-// computed points -- {depth <= maxDepth} -- and the map do not depend on the
-// order in which warps run.  Results go straight into the map; flags, depth and
-// the statistics are updated in place.
-struct RefineCtx {
-    const long long* rule;
-    const long long* nRule;        // device count of rule
-    int* queue;                    // expansion queue, qCap slots, -1 = not yet written
-    unsigned long long qCap;
-    unsigned long long* counters;  // [0] queue head, [1] queue tail, [2] rule head, [3] pending items,
-                                   // [4] busy warps, [5] time a short queue started waiting
-    int* depth;                    // per grid point
-    unsigned char* flag;           // per grid point (kRef* bits)
-    double* mapLle;
-    int* mapCls;
-    unsigned char* src;            // per grid point: 2 once recomputed
-    RefineStats* stats;
-    int* err;                      // 1 DBSCAN guard, 2 idle timeout, 3 queue overflow, 4 queue slot timeout
-    const long long* labelIdx;     // training labels (grid indices) and their surprise flags
-    const unsigned char* labelSurprise;
-    long long nLabel;
-    double* scrPk;                 // per-warp DBSCAN scratch, refine_scratch_bytes()
-    size_t scrBytes;
-    unsigned long long maxIdleNs;  // a warp that finds no work for this long gives up (err 2)
-    int nPts, radius, maxDepth;
-};
-// Scratch bytes the refine launch needs on the current device.
-size_t refine_scratch_bytes(const DevJob& J);
-// Depth initialisation, label seeding and the persistent kernel, on `s`; no host
-// synchronisation (the caller reads stats and err afterwards).
-cudaError_t launch_regime_refine(const DevJob& J, const RefineCtx& R, cudaStream_t s);
 // KDE/DBSCAN with caller-provided scratch (no allocation): `scratch` holds
 // `scratchBytes` of peak buffers, `err` one int that must be zero on entry.
 // Synchronises `s` to read `err`.

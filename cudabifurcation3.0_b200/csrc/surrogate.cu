@@ -11,17 +11,15 @@
 //   * whose softmax confidence is below confThreshold,
 //   * in a seeded random audit sample (auditFraction of the grid).
 // Wherever the plain class of a label or a recomputed point differs from the
-// network's, its neighbours (expandRadius) are recomputed too, and so on up to
-// an expansion depth of maxWaves steps from a rule point or label: thin
-// structures the network cannot resolve (periodic windows inside chaos) are
-// traced from any point that hits them.  The recompute is one persistent launch
-// whose warps pull work from a device queue (lle_regime.cu, RefineCtx); the set
-// of computed points, and so the map, does not depend on the order in which the
-// warps run.  Labelled and recomputed points carry plain values; the rest carry
-// the network's prediction.  The audit points that no other rule selected measure
-// the error of the kept predictions.  Everything runs on one stream; the host
-// reads the labels back once (to normalise the LLE targets) and waits once at
-// the end.
+// network's, its neighbours (expandRadius) are recomputed in a later round, for
+// maxWaves rounds: thin structures the network cannot resolve (periodic windows
+// inside chaos) are traced from any point that hits them.  Labelled and
+// recomputed points carry plain values; the rest carry the network's
+// prediction.  The audit points that no other rule selected measure the error of
+// the kept predictions.  Everything runs on one stream.  The rounds are planned
+// on the device (plan_kernel): the host reads the labels back once (to normalise
+// the LLE targets), the number of rule-selected points once (to bound the
+// rounds) and waits once at the end.
 #include <math.h>
 #include <string.h>
 
@@ -36,8 +34,9 @@ namespace {
 constexpr int kChunk = 4096;          // points per compaction block
 constexpr int kChunkThreads = 256;
 // flag bits: reasons to recompute, then the point's state
-constexpr unsigned char kBoundary = kRefBoundary, kLowConf = kRefLowConf, kAudit = kRefAudit;
-constexpr unsigned char kDone = kRefDone, kLabel = kRefLabel;
+constexpr unsigned char kBoundary = 1, kLowConf = 2, kAudit = 4, kExpand = 8;
+constexpr unsigned char kReasons = kBoundary | kLowConf | kAudit | kExpand;
+constexpr unsigned char kDone = 0x40, kLabel = 0x80;
 
 __device__ __forceinline__ unsigned long long mix64(unsigned long long z)
 {
@@ -133,9 +132,13 @@ __device__ __forceinline__ bool selected(unsigned char f, unsigned char want)
     return (f & want) && !(f & (kLabel | kDone));
 }
 
+// `stop` (optional): nonzero once the recompute rounds have ended; every round
+// kernel then returns at once.
 __global__ void __launch_bounds__(kChunkThreads) count_kernel(const unsigned char* __restrict__ flag, long long n,
-                                                              unsigned char want, int* __restrict__ blockCount)
+                                                              unsigned char want, int* __restrict__ blockCount,
+                                                              const int* stop)
 {
+    if (stop && *stop) return;
     const long long base = (long long)blockIdx.x * kChunk;
     int total = 0;
     for (int r = 0; r < kChunk; r += kChunkThreads) {
@@ -148,9 +151,10 @@ __global__ void __launch_bounds__(kChunkThreads) count_kernel(const unsigned cha
 // Exclusive prefix over nb block counts (one block of 1024 threads);
 // offsets[nb] = total.
 __global__ void __launch_bounds__(1024) scan_kernel(const int* __restrict__ blockCount, int nb,
-                                                    long long* __restrict__ offsets)
+                                                    long long* __restrict__ offsets, const int* stop)
 {
     __shared__ long long part[1024];
+    if (stop && *stop) return;
     const int per = (nb + 1023) / 1024;
     const int b0 = threadIdx.x * per;
     long long s = 0;
@@ -175,9 +179,10 @@ __global__ void __launch_bounds__(1024) scan_kernel(const int* __restrict__ bloc
 __global__ void __launch_bounds__(kChunkThreads) compact_kernel(const unsigned char* __restrict__ flag, long long n,
                                                                 unsigned char want,
                                                                 const long long* __restrict__ offsets,
-                                                                long long* __restrict__ list)
+                                                                long long* __restrict__ list, const int* stop)
 {
     __shared__ int warpTot[kChunkThreads / 32];
+    if (stop && *stop) return;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     long long out = offsets[blockIdx.x];
     const long long base = (long long)blockIdx.x * kChunk;
@@ -198,6 +203,145 @@ __global__ void __launch_bounds__(kChunkThreads) compact_kernel(const unsigned c
     }
 }
 
+// Device state of the recompute: statistics of the replaced predictions, then
+// the plan of the current round.
+struct Refine {
+    unsigned long long boundary, lowConf, audit, auditOnly, auditOnlyAgree, changed, expanded;
+    double errSum;
+    unsigned long long errMaxBits;
+    long long n0;       // rule-selected points (ascending grid index in `rule`)
+    long long pos;      // rule points taken by the rounds so far
+    long long nA, nB;   // this round: expansion marks, then rule points rule[from, from + nB)
+    long long from;
+    long long nSel;     // nA + nB: the round's list length
+    long long refined;  // points computed by all rounds
+    long long tiles;    // 32-point warp tiles of all rounds
+    int rounds;         // rounds that computed at least one point
+    int stop;           // a round found nothing to compute: the later rounds are empty
+};
+
+// One thread: the round's list is every expansion mark of the previous rounds
+// (nMarked, already compacted to the list's head) and the next chunk of rule
+// points, at least target/4 of them, so that the chain of expansion rounds
+// overlaps the bulk of the recompute; together about `target` points.
+__global__ void plan_kernel(const long long* __restrict__ nMarked, Refine* R, long long target, int round)
+{
+    if (R->stop) return;
+    const long long nA = *nMarked;
+    long long nB = target - nA > target / 4 ? target - nA : target / 4;
+    if (nB > R->n0 - R->pos) nB = R->n0 - R->pos;
+    const long long nSel = nA + nB;
+    R->nA = nA;
+    R->nB = nB;
+    R->from = R->pos;
+    R->pos += nB;
+    R->nSel = nSel;
+    R->refined += nSel;
+    R->tiles += (nSel + 31) / 32;
+    if (nSel > 0) R->rounds = round + 1;
+    else R->stop = 1;
+}
+
+// The round's rule chunk after its expansion marks.
+__global__ void copy_rule_kernel(const long long* __restrict__ rule, long long* __restrict__ list,
+                                 const Refine* R)
+{
+    const long long nA = R->nA, nB = R->nB, from = R->from;
+    const long long step = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nB; i += step)
+        list[nA + i] = rule[from + i];
+}
+
+// Plain results into the map; statistics of the predictions they replace;
+// surprise[k] = the plain class differs from the predicted one.
+__global__ void merge_kernel(const long long* __restrict__ list, const long long* __restrict__ nSel,
+                             const double* __restrict__ rl, const int* __restrict__ rc,
+                             unsigned char* __restrict__ flag, double* __restrict__ mapLle,
+                             int* __restrict__ mapCls, unsigned char* __restrict__ src,
+                             unsigned char* __restrict__ surprise, Refine* st)
+{
+    const long long n = *nSel;
+    const long long step = (long long)gridDim.x * blockDim.x;
+    unsigned long long b = 0, lc = 0, au = 0, ao = 0, aa = 0, ch = 0, ex = 0;
+    double es = 0, em = 0;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += step) {
+        const long long g = list[k];
+        const unsigned char f = flag[g];
+        const int pc = mapCls[g];
+        const double pl = mapLle[g];
+        b += (f & kBoundary) != 0;
+        lc += (f & kLowConf) != 0;
+        au += (f & kAudit) != 0;
+        ex += (f & kReasons) == kExpand;
+        const bool changed = pc != rc[k];
+        ch += changed;
+        surprise[k] = (unsigned char)changed;
+        if (f == kAudit) {
+            ++ao;
+            aa += pc == rc[k];
+            const double err = fabs(pl - rl[k]);
+            if (isfinite(err)) {
+                es += err;
+                em = fmax(em, err);
+            }
+        }
+        mapLle[g] = rl[k];
+        mapCls[g] = rc[k];
+        src[g] = 2;
+        flag[g] = f | kDone;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        b += __shfl_down_sync(0xffffffffu, b, o);
+        lc += __shfl_down_sync(0xffffffffu, lc, o);
+        au += __shfl_down_sync(0xffffffffu, au, o);
+        ao += __shfl_down_sync(0xffffffffu, ao, o);
+        aa += __shfl_down_sync(0xffffffffu, aa, o);
+        ch += __shfl_down_sync(0xffffffffu, ch, o);
+        ex += __shfl_down_sync(0xffffffffu, ex, o);
+        es += __shfl_down_sync(0xffffffffu, es, o);
+        em = fmax(em, __shfl_down_sync(0xffffffffu, em, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (b) atomicAdd(&st->boundary, b);
+        if (lc) atomicAdd(&st->lowConf, lc);
+        if (au) atomicAdd(&st->audit, au);
+        if (ao) atomicAdd(&st->auditOnly, ao);
+        if (aa) atomicAdd(&st->auditOnlyAgree, aa);
+        if (ch) atomicAdd(&st->changed, ch);
+        if (ex) atomicAdd(&st->expanded, ex);
+        if (es != 0) atomicAdd(&st->errSum, es);
+        if (em > 0) atomicMax(&st->errMaxBits, (unsigned long long)__double_as_longlong(em));
+    }
+}
+
+// Neighbours (Chebyshev radius) of every surprised point that no rule selected
+// and the plain method has not computed are marked for the next round (rule-
+// selected points are computed in their own chunk and expand from there).
+// The list length is *nDev when given, else nHost.
+__global__ void expand_kernel(const long long* __restrict__ list, const unsigned char* __restrict__ surprise,
+                              const long long* __restrict__ nDev, long long nHost, int nPts, int radius,
+                              unsigned char* __restrict__ flag)
+{
+    const long long n = nDev ? *nDev : nHost;
+    const long long step = (long long)gridDim.x * blockDim.x;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += step) {
+        if (!surprise[k]) continue;
+        const long long g = list[k];
+        const int row = (int)(g / nPts), col = (int)(g % nPts);
+        for (int dr = -radius; dr <= radius; ++dr) {
+            const int r = row + dr;
+            if (r < 0 || r >= nPts) continue;
+            for (int dc = -radius; dc <= radius; ++dc) {
+                const int q = col + dc;
+                if (q < 0 || q >= nPts) continue;
+                const long long nb = (long long)r * nPts + q;
+                if (flag[nb] == 0) flag[nb] = kExpand;
+            }
+        }
+    }
+}
+
 template <class F>
 cudaError_t launch1d(long long n, cudaStream_t s, F f)
 {
@@ -212,7 +356,7 @@ cudaError_t launch1d(long long n, cudaStream_t s, F f)
 // map allocates nothing.  cbf_surrogate_release frees them.
 enum Slot {
     kSlotIdx, kSlotLabLle, kSlotLabCls, kSlotX, kSlotYl, kSlotConf, kSlotFlag, kSlotSrc, kSlotBlock,
-    kSlotOffsets, kSlotStats, kSlotLsur, kSlotRule, kSlotDepth, kSlotQueue, kSlotCounters, kSlotErr,
+    kSlotOffsets, kSlotStats, kSlotLsur, kSlotRule, kSlotList, kSlotRl, kSlotRc, kSlotSur, kSlotErr,
     kSlotScratch, kNumSlots
 };
 
@@ -367,7 +511,7 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
     unsigned char *flag = nullptr, *src = dSource;
     int* blockCount = nullptr;
     long long* offsets = nullptr;
-    RefineStats* stats = nullptr;
+    Refine* stats = nullptr;
     const int nb = (int)((n + kChunk - 1) / kChunk);
     cudaError_t e = buf.get(kSlotIdx, &dIdx, nLab);
     if (e == cudaSuccess) e = buf.get(kSlotLabLle, &labLle, nLab);
@@ -478,88 +622,113 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
         e = launch1d(nLab, s, [&](unsigned b, int t) {
             label_scatter_kernel<<<b, t, 0, s>>>(dIdx, nLab, labLle, labCls, dLle, dCls, flag, src, lsur);
         });
-    if (e == cudaSuccess) e = cudaMemsetAsync(stats, 0, sizeof(RefineStats), s);
+    if (e == cudaSuccess && er > 0)
+        e = launch1d(nLab, s, [&](unsigned b, int t) {
+            expand_kernel<<<b, t, 0, s>>>(dIdx, lsur, nullptr, nLab, nPts, er, flag);
+        });
+    if (e == cudaSuccess) e = cudaMemsetAsync(stats, 0, sizeof(Refine), s);
     if (e != cudaSuccess) return report_cuda_error(e, "refinement mask");
     cudaEventRecord(ev[4], s);
 
-    // 5. plain recompute in one persistent launch: the rule-selected points
-    // (ascending grid index) and, from every label or computed point whose plain
-    // class differs from the prediction, its neighbours within the expansion
-    // radius, up to expansion depth maxWaves (RefineCtx, engine.cuh).  The host
-    // waits once, at the end.
+    // 5. plain recompute in rounds.  The rule-selected points (ascending grid
+    // index) are fed in chunks; every round also takes all points the expansion
+    // marked in the previous rounds, so the chain of expansion rounds overlaps
+    // the bulk of the recompute.  A round is sized to about two waves of
+    // resident threads of the LLE_REGIME kernel.  plan_kernel sizes each round
+    // on the device; the host launches a fixed number of rounds, enough for
+    // every rule chunk and every expansion round, and the rounds after the last
+    // one with work return at once.
     const unsigned char want = kBoundary | kLowConf | kAudit;
     long long* rule = nullptr;
-    int* depth = nullptr;
-    int* queue = nullptr;
-    unsigned long long* counters = nullptr;
+    long long* list = nullptr;
+    double* rl = nullptr;
+    int* rc = nullptr;
+    unsigned char* sur = nullptr;
     int* rerr = nullptr;
     double* scr = nullptr;
-    const size_t scrBytes = refine_scratch_bytes(dj);
-    // each point enters the queue once for computation, and again only when its
-    // depth drops after it was expanded (rare): room for all points and half again
-    const unsigned long long qCap = (unsigned long long)n + (unsigned long long)n / 2 + 1024;
+    const size_t scrBytes = lle_regime_scratch_bytes(dj);
     e = buf.get(kSlotRule, &rule, n);
-    if (e == cudaSuccess) e = buf.get(kSlotDepth, &depth, n);
-    if (e == cudaSuccess) e = buf.get(kSlotQueue, &queue, (long long)qCap);
-    if (e == cudaSuccess) e = buf.get(kSlotCounters, &counters, 6);
+    if (e == cudaSuccess) e = buf.get(kSlotList, &list, n);
+    if (e == cudaSuccess) e = buf.get(kSlotRl, &rl, n);
+    if (e == cudaSuccess) e = buf.get(kSlotRc, &rc, n);
+    if (e == cudaSuccess) e = buf.get(kSlotSur, &sur, n);
     if (e == cudaSuccess) e = buf.get(kSlotErr, &rerr, 1);
     if (e == cudaSuccess) e = buf.get(kSlotScratch, &scr, (long long)(scrBytes / sizeof(double)) + 1);
     if (e != cudaSuccess) return report_cuda_error(e, "recompute buffers");
-    count_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, want, blockCount);
-    scan_kernel<<<1, 1024, 0, s>>>(blockCount, nb, offsets);
-    compact_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, want, offsets, rule);
+    if (scrBytes == 0) return report_error(CBF_ERR_INTERNAL, "recompute: no resident LLE_REGIME blocks");
+    count_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, want, blockCount, nullptr);
+    scan_kernel<<<1, 1024, 0, s>>>(blockCount, nb, offsets, nullptr);
+    compact_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, want, offsets, rule, nullptr);
     note_launch(3);
+    long long n0 = 0;
     e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemsetAsync(queue, 0xff, qCap * sizeof(int), s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(counters, 0, 6 * sizeof(unsigned long long), s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&stats->n0, offsets + nb, sizeof(long long), cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&n0, offsets + nb, sizeof(long long), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(rerr, 0, sizeof(int), s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return report_cuda_error(e, "recompute list");
-    RefineCtx R;
-    memset(&R, 0, sizeof(R));
-    R.rule = rule;
-    R.nRule = offsets + nb;
-    R.queue = queue;
-    R.qCap = qCap;
-    R.counters = counters;
-    R.depth = depth;
-    R.flag = flag;
-    R.mapLle = dLle;
-    R.mapCls = dCls;
-    R.src = src;
-    R.stats = stats;
-    R.err = rerr;
-    R.labelIdx = dIdx;
-    R.labelSurprise = lsur;
-    R.nLabel = nLab;
-    R.scrPk = scr;
-    R.scrBytes = scrBytes;
-    R.nPts = nPts;
-    R.radius = er;
-    R.maxDepth = er > 0 ? cfg->maxWaves : 0;
-    // an idle warp waits while others finish their tiles: allow far more than the
-    // integration of one point (~1e-7 s per step at most) before calling it stuck
-    const double stepsPerPoint = (double)dj.nSkip + 2.0 * (double)dj.nRecord * (double)dj.nNT;
-    R.maxIdleNs = (unsigned long long)(60e9 + stepsPerPoint * 1000.0);
-    if ((e = launch_regime_refine(dj, R, s)) != cudaSuccess) return report_cuda_error(e, "recompute");
-    RefineStats hs;
+    long long resident = lle_regime_resident_points(dj);
+    if (resident < 4096) resident = 4096;
+    const long long target = 2 * resident;
+    // Rounds with rule points: at most ceil(n0 / (target/4)).  Expansion marks
+    // come from the labels and the rounds before round maxWaves, and every round
+    // takes all of them: rounds with marks alone, at most maxWaves + 1.  One
+    // more round finds nothing and sets `stop`.
+    const int maxRounds =
+        (int)((n0 + target / 4 - 1) / (target / 4)) + (er > 0 ? cfg->maxWaves + 1 : 0) + 1;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long fillBlocks = (long long)sms * 8;
+    auto gridFor = [&](long long m) { return (unsigned)((m + 255) / 256 < fillBlocks ? (m + 255) / 256 : fillBlocks); };
+    DevJob rj = dj;
+    rj.pointIndex = list;
+    rj.firstPoint = 0;
+    rj.nPoints = n;
+    const long long* nSel = &stats->nSel;
+    const int* stop = &stats->stop;
+    for (int w = 0; w < maxRounds; ++w) {
+        if (w > 0 && w % 64 == 0) {  // long expansion chains: stop launching once a round found nothing
+            int hostStop = 0;
+            e = cudaMemcpyAsync(&hostStop, stop, sizeof(int), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) return report_cuda_error(e, "recompute rounds");
+            if (hostStop) break;
+        }
+        count_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, kExpand, blockCount, stop);
+        scan_kernel<<<1, 1024, 0, s>>>(blockCount, nb, offsets, stop);
+        compact_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, kExpand, offsets, list, stop);
+        plan_kernel<<<1, 1, 0, s>>>(offsets + nb, stats, target, w);
+        copy_rule_kernel<<<gridFor(target), 256, 0, s>>>(rule, list, stats);
+        note_launch(5);
+        if ((e = cudaGetLastError()) != cudaSuccess) return report_cuda_error(e, "recompute list");
+        if ((e = launch_lle_regime_list(rj, nSel, n, rl, rc, scr, scrBytes, rerr, s)) != cudaSuccess)
+            return report_cuda_error(e, "recompute");
+        merge_kernel<<<gridFor(n), 256, 0, s>>>(list, nSel, rl, rc, flag, dLle, dCls, src, sur, stats);
+        note_launch();
+        if (er > 0 && w < cfg->maxWaves) {
+            expand_kernel<<<gridFor(n), 256, 0, s>>>(list, sur, nSel, 0, nPts, er, flag);
+            note_launch();
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return report_cuda_error(e, "merge");
+    }
+    Refine hs;
     memset(&hs, 0, sizeof(hs));
     int hostErr = 0;
-    e = cudaMemcpyAsync(&hs, stats, sizeof(RefineStats), cudaMemcpyDeviceToHost, s);
+    e = cudaMemcpyAsync(&hs, stats, sizeof(Refine), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&hostErr, rerr, sizeof(int), cudaMemcpyDeviceToHost, s);
     cudaEventRecord(ev[5], s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return report_cuda_error(e, "recompute");
-    if (hostErr == 2 || hostErr == 4)
-        return report_error(CBF_ERR_TIMEOUT, "surrogate recompute: a bounded device-side wait gave up");
     if (hostErr) return report_error(CBF_ERR_INTERNAL, "surrogate recompute: a device-side check failed");
+    if (!hs.stop) return report_error(CBF_ERR_INTERNAL, "surrogate recompute: rounds left work undone");
 
     if (rep) {
         memset(rep, 0, sizeof(*rep));
         rep->points = n;
         rep->labelled = nLab;
-        rep->refined = (int64_t)hs.computed;
+        rep->refined = (int64_t)hs.refined;
         rep->expanded = (int64_t)hs.expanded;
-        rep->waves = hs.deepest;
+        rep->waves = hs.rounds;
         rep->refineTiles = (int64_t)hs.tiles;
         rep->boundary = (int64_t)hs.boundary;
         rep->lowConfidence = (int64_t)hs.lowConf;

@@ -234,9 +234,11 @@ cbf_status cbf_mlp_grid_features(const cbf_job* job, const int64_t* dIdx, int64_
  * randomPoints seeded random points; the network above is trained on them,
  * predicts every grid point, and the plain method recomputes every point on a
  * predicted regime boundary, below confThreshold softmax confidence, or in the
- * random audit sample; then, in waves, the neighbours of every label or
- * recomputed point whose plain class differs from the prediction.  Labelled and
- * recomputed points carry plain values. */
+ * random audit sample; then, in later rounds, the neighbours of every label or
+ * recomputed point whose plain class differs from the prediction.  The rule
+ * points are computed in chunks of about two waves of resident LLE_REGIME
+ * threads, each round together with every point the previous rounds marked.
+ * Labelled and recomputed points carry plain values. */
 typedef struct cbf_surrogate_config {
     int32_t coarseSide;      /* training sub-grid side (512) */
     int32_t randomPoints;    /* extra random training points (65536) */
@@ -253,9 +255,8 @@ typedef struct cbf_surrogate_config {
     int32_t expandRadius;    /* neighbours within this radius of a point whose plain class
                                 differs from the prediction are recomputed next; -1 (default):
                                 ceil(nPts / 8192); 0: no expansion */
-    int32_t maxWaves;        /* expansion depth: a point is recomputed through the expansion
-                                only within this many expansion steps of a rule point or
-                                label (20) */
+    int32_t maxWaves;        /* rounds that expand: the labels and the points computed in
+                                the first maxWaves rounds mark their neighbours (20) */
     int32_t predictor;       /* 0: the trained network (default); 1: no network -- every
                                 point takes the class and LLE of its nearest coarse-grid
                                 label, confidence 1 (the ablation that measures what the
@@ -278,8 +279,8 @@ typedef struct cbf_surrogate_report {
     float finalLoss;           /* mean training loss over the last 100 steps */
     double msLabel, msTrain, msPredict, msMask, msRefine, msTotal;  /* stream time */
     int64_t expanded;          /* recomputed points selected only by the expansion */
-    int32_t waves;             /* largest expansion depth reached */
-    int64_t refineTiles;       /* 32-lane warp tiles the recompute ran (lane use =
+    int32_t waves;             /* recompute rounds that computed at least one point */
+    int64_t refineTiles;       /* 32-point warp tiles of the recompute rounds (lane use =
                                   refined / (32 * refineTiles)) */
 } cbf_surrogate_report;
 
