@@ -714,6 +714,19 @@ def run_surrogate(args) -> int:
                 "computed_fraction": float((s_src > 0).double().mean().item()),
                 "kept_lle_mean_abs_err": float(abl_err[abl_kept].mean().item()) if abl_kept.any() else None,
                 "refined": int(abl_rep.refined), "waves": int(abl_rep.waves)}
+    # The two predictors alone (refine 0: no recompute), on every point that is
+    # not a label: class agreement and LLE error against the plain map.
+    raw = {}
+    for name, kind in (("network", 0), ("nearest_label", 1)):
+        cbf.lle_map_surrogate(job, cbf.surrogate_config(refine=0, predictor=kind), s_lle.data_ptr(),
+                              s_cls.data_ptr(), s_src.data_ptr(), stream=stream.cuda_stream)
+        stream.synchronize()
+        pred = s_src == 0
+        lerr = (s_lle - p_lle).abs()
+        fin = pred & torch.isfinite(lerr)
+        raw[name] = {"class_agreement": float((s_cls[pred] == p_cls[pred]).double().mean().item()),
+                     "lle_mean_abs_err": float(lerr[fin].mean().item())}
+    ablation["raw_predictions"] = raw
 
     r = reps[-1].as_dict()
     plain_points = r["labelled"] + r["refined"]

@@ -121,6 +121,7 @@ class SurrogateConfig(C.Structure):
         ("expandRadius", C.c_int32),
         ("maxWaves", C.c_int32),
         ("predictor", C.c_int32),
+        ("auditFill", C.c_int32),
     ]
 
 

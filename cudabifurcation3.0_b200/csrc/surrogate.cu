@@ -126,24 +126,25 @@ __global__ void mask_kernel(const int* __restrict__ cls, const float* __restrict
     src[g] = 0;
 }
 
-// Points with one of the `want` reasons that are neither labels nor computed.
-__device__ __forceinline__ bool selected(unsigned char f, unsigned char want)
+// Points with one of the `want` reasons and none of the `exclude` bits that are
+// neither labels nor computed.
+__device__ __forceinline__ bool selected(unsigned char f, unsigned char want, unsigned char exclude)
 {
-    return (f & want) && !(f & (kLabel | kDone));
+    return (f & want) && !(f & (kLabel | kDone | exclude));
 }
 
 // `stop` (optional): nonzero once the recompute rounds have ended; every round
 // kernel then returns at once.
 __global__ void __launch_bounds__(kChunkThreads) count_kernel(const unsigned char* __restrict__ flag, long long n,
-                                                              unsigned char want, int* __restrict__ blockCount,
-                                                              const int* stop)
+                                                              unsigned char want, unsigned char exclude,
+                                                              int* __restrict__ blockCount, const int* stop)
 {
     if (stop && *stop) return;
     const long long base = (long long)blockIdx.x * kChunk;
     int total = 0;
     for (int r = 0; r < kChunk; r += kChunkThreads) {
         const long long g = base + r + threadIdx.x;
-        total += __syncthreads_count(g < n && selected(flag[g], want));
+        total += __syncthreads_count(g < n && selected(flag[g], want, exclude));
     }
     if (threadIdx.x == 0) blockCount[blockIdx.x] = total;
 }
@@ -177,7 +178,7 @@ __global__ void __launch_bounds__(1024) scan_kernel(const int* __restrict__ bloc
 
 // Selected grid indices in ascending order.
 __global__ void __launch_bounds__(kChunkThreads) compact_kernel(const unsigned char* __restrict__ flag, long long n,
-                                                                unsigned char want,
+                                                                unsigned char want, unsigned char exclude,
                                                                 const long long* __restrict__ offsets,
                                                                 long long* __restrict__ list, const int* stop)
 {
@@ -188,7 +189,7 @@ __global__ void __launch_bounds__(kChunkThreads) compact_kernel(const unsigned c
     const long long base = (long long)blockIdx.x * kChunk;
     for (int r = 0; r < kChunk; r += kChunkThreads) {
         const long long g = base + r + threadIdx.x;
-        const bool sel = g < n && selected(flag[g], want);
+        const bool sel = g < n && selected(flag[g], want, exclude);
         const unsigned ball = __ballot_sync(0xffffffffu, sel);
         if (lane == 0) warpTot[w] = __popc(ball);
         __syncthreads();
@@ -209,11 +210,15 @@ struct Refine {
     unsigned long long boundary, lowConf, audit, auditOnly, auditOnlyAgree, changed, expanded;
     double errSum;
     unsigned long long errMaxBits;
-    long long n0;       // rule-selected points (ascending grid index in `rule`)
-    long long pos;      // rule points taken by the rounds so far
+    long long n0;       // rule-selected points fed first (ascending grid index in `rule`)
+    long long pos;      // of which taken by the rounds so far
+    long long d0;       // audit-only points that fill rounds (ascending, in `fill`)
+    long long dpos;     // of which taken so far
     long long nA, nB;   // this round: expansion marks, then rule points rule[from, from + nB)
     long long from;
-    long long nSel;     // nA + nB: the round's list length
+    long long nC;       // then fill points fill[dfrom, dfrom + nC)
+    long long dfrom;
+    long long nSel;     // nA + nB + nC: the round's list length
     long long refined;  // points computed by all rounds
     long long tiles;    // 32-point warp tiles of all rounds
     int rounds;         // rounds that computed at least one point
@@ -223,18 +228,28 @@ struct Refine {
 // One thread: the round's list is every expansion mark of the previous rounds
 // (nMarked, already compacted to the list's head) and the next chunk of rule
 // points, at least target/4 of them, so that the chain of expansion rounds
-// overlaps the bulk of the recompute; together about `target` points.
-__global__ void plan_kernel(const long long* __restrict__ nMarked, Refine* R, long long target, int round)
+// overlaps the bulk of the recompute; together about `target` points.  Then,
+// when audit-only points are kept back (d0 > 0), as many of them as fill the
+// round up to a whole number of waves of `wave` resident points (a round with
+// nothing else takes `target` of them).
+__global__ void plan_kernel(const long long* __restrict__ nMarked, Refine* R, long long target, long long wave,
+                            int round)
 {
     if (R->stop) return;
     const long long nA = *nMarked;
     long long nB = target - nA > target / 4 ? target - nA : target / 4;
     if (nB > R->n0 - R->pos) nB = R->n0 - R->pos;
-    const long long nSel = nA + nB;
+    const long long base = nA + nB;
+    long long nC = base == 0 ? target : (base + wave - 1) / wave * wave - base;
+    if (nC > R->d0 - R->dpos) nC = R->d0 - R->dpos;
+    const long long nSel = base + nC;
     R->nA = nA;
     R->nB = nB;
     R->from = R->pos;
     R->pos += nB;
+    R->nC = nC;
+    R->dfrom = R->dpos;
+    R->dpos += nC;
     R->nSel = nSel;
     R->refined += nSel;
     R->tiles += (nSel + 31) / 32;
@@ -242,14 +257,14 @@ __global__ void plan_kernel(const long long* __restrict__ nMarked, Refine* R, lo
     else R->stop = 1;
 }
 
-// The round's rule chunk after its expansion marks.
-__global__ void copy_rule_kernel(const long long* __restrict__ rule, long long* __restrict__ list,
-                                 const Refine* R)
+// The round's rule chunk and fill chunk after its expansion marks.
+__global__ void copy_rule_kernel(const long long* __restrict__ rule, const long long* __restrict__ fill,
+                                 long long* __restrict__ list, const Refine* R)
 {
-    const long long nA = R->nA, nB = R->nB, from = R->from;
+    const long long nA = R->nA, nB = R->nB, from = R->from, nC = R->nC, dfrom = R->dfrom;
     const long long step = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nB; i += step)
-        list[nA + i] = rule[from + i];
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nB + nC; i += step)
+        list[nA + i] = i < nB ? rule[from + i] : fill[dfrom + i - nB];
 }
 
 // Plain results into the map; statistics of the predictions they replace;
@@ -356,7 +371,7 @@ cudaError_t launch1d(long long n, cudaStream_t s, F f)
 // map allocates nothing.  cbf_surrogate_release frees them.
 enum Slot {
     kSlotIdx, kSlotLabLle, kSlotLabCls, kSlotX, kSlotYl, kSlotConf, kSlotFlag, kSlotSrc, kSlotBlock,
-    kSlotOffsets, kSlotStats, kSlotLsur, kSlotRule, kSlotList, kSlotRl, kSlotRc, kSlotSur, kSlotErr,
+    kSlotOffsets, kSlotStats, kSlotLsur, kSlotRule, kSlotFill, kSlotList, kSlotRl, kSlotRc, kSlotSur, kSlotErr,
     kSlotScratch, kNumSlots
 };
 
@@ -461,7 +476,7 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
     if (job->nPts < 3 || cfg->coarseSide < 2 || cfg->randomPoints < 0 || cfg->batch < 1 ||
         cfg->trainSteps < 0 || !(cfg->lr > 0) || cfg->boundaryRadius < 0 || cfg->boundaryRadius > 8 ||
         cfg->expandRadius < -1 || cfg->expandRadius > 16 || cfg->maxWaves < 0 || cfg->maxWaves > 1000000 ||
-        cfg->predictor < 0 || cfg->predictor > 1 || !(cfg->auditFraction >= 0 && cfg->auditFraction <= 1))
+        cfg->predictor < 0 || cfg->predictor > 1 || cfg->auditFill < 0 || cfg->auditFill > 1 || !(cfg->auditFraction >= 0 && cfg->auditFraction <= 1))
         return report_error(CBF_ERR_INVALID_ARG, "bad surrogate configuration");
     DevJob dj;
     cbf_status st = lower_job_for(job, &dj);
@@ -634,12 +649,16 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
     // index) are fed in chunks; every round also takes all points the expansion
     // marked in the previous rounds, so the chain of expansion rounds overlaps
     // the bulk of the recompute.  A round is sized to about two waves of
-    // resident threads of the LLE_REGIME kernel.  plan_kernel sizes each round
-    // on the device; the host launches a fixed number of rounds, enough for
-    // every rule chunk and every expansion round, and the rounds after the last
-    // one with work return at once.
-    const unsigned char want = kBoundary | kLowConf | kAudit;
+    // resident threads of the LLE_REGIME kernel.  With auditFill, points that
+    // only the audit selected are kept back and fill every round up to a whole
+    // number of waves.  plan_kernel sizes each round on the device; the host
+    // launches a fixed number of rounds, enough for every chunk and every
+    // expansion round, and the rounds after the last one with work return at
+    // once.
+    const bool fillAudit = cfg->auditFill != 0;
+    const unsigned char want = kBoundary | kLowConf | (fillAudit ? 0 : kAudit);
     long long* rule = nullptr;
+    long long* fillList = nullptr;
     long long* list = nullptr;
     double* rl = nullptr;
     int* rc = nullptr;
@@ -648,6 +667,7 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
     double* scr = nullptr;
     const size_t scrBytes = lle_regime_scratch_bytes(dj);
     e = buf.get(kSlotRule, &rule, n);
+    if (e == cudaSuccess) e = buf.get(kSlotFill, &fillList, fillAudit ? n : 1);
     if (e == cudaSuccess) e = buf.get(kSlotList, &list, n);
     if (e == cudaSuccess) e = buf.get(kSlotRl, &rl, n);
     if (e == cudaSuccess) e = buf.get(kSlotRc, &rc, n);
@@ -656,14 +676,24 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
     if (e == cudaSuccess) e = buf.get(kSlotScratch, &scr, (long long)(scrBytes / sizeof(double)) + 1);
     if (e != cudaSuccess) return report_cuda_error(e, "recompute buffers");
     if (scrBytes == 0) return report_error(CBF_ERR_INTERNAL, "recompute: no resident LLE_REGIME blocks");
-    count_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, want, blockCount, nullptr);
+    long long n0 = 0, d0 = 0;
+    count_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, want, 0, blockCount, nullptr);
     scan_kernel<<<1, 1024, 0, s>>>(blockCount, nb, offsets, nullptr);
-    compact_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, want, offsets, rule, nullptr);
+    compact_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, want, 0, offsets, rule, nullptr);
     note_launch(3);
-    long long n0 = 0;
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(&stats->n0, offsets + nb, sizeof(long long), cudaMemcpyDeviceToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&n0, offsets + nb, sizeof(long long), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && fillAudit) {
+        count_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, kAudit, kBoundary | kLowConf, blockCount, nullptr);
+        scan_kernel<<<1, 1024, 0, s>>>(blockCount, nb, offsets, nullptr);
+        compact_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, kAudit, kBoundary | kLowConf, offsets, fillList, nullptr);
+        note_launch(3);
+        e = cudaGetLastError();
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(&stats->d0, offsets + nb, sizeof(long long), cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&d0, offsets + nb, sizeof(long long), cudaMemcpyDeviceToHost, s);
+    }
     if (e == cudaSuccess) e = cudaMemsetAsync(rerr, 0, sizeof(int), s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return report_cuda_error(e, "recompute list");
@@ -672,10 +702,11 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
     const long long target = 2 * resident;
     // Rounds with rule points: at most ceil(n0 / (target/4)).  Expansion marks
     // come from the labels and the rounds before round maxWaves, and every round
-    // takes all of them: rounds with marks alone, at most maxWaves + 1.  One
-    // more round finds nothing and sets `stop`.
-    const int maxRounds =
-        (int)((n0 + target / 4 - 1) / (target / 4)) + (er > 0 ? cfg->maxWaves + 1 : 0) + 1;
+    // takes all of them: rounds with marks but no rule points, at most
+    // maxWaves + 1.  Rounds with fill points alone take `target` of them: at
+    // most ceil(d0 / target).  One more round finds nothing and sets `stop`.
+    const int maxRounds = (int)((n0 + target / 4 - 1) / (target / 4)) + (er > 0 ? cfg->maxWaves + 1 : 0) +
+                          (int)((d0 + target - 1) / target) + 1;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long fillBlocks = (long long)sms * 8;
@@ -694,11 +725,11 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
             if (e != cudaSuccess) return report_cuda_error(e, "recompute rounds");
             if (hostStop) break;
         }
-        count_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, kExpand, blockCount, stop);
+        count_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, kExpand, 0, blockCount, stop);
         scan_kernel<<<1, 1024, 0, s>>>(blockCount, nb, offsets, stop);
-        compact_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, kExpand, offsets, list, stop);
-        plan_kernel<<<1, 1, 0, s>>>(offsets + nb, stats, target, w);
-        copy_rule_kernel<<<gridFor(target), 256, 0, s>>>(rule, list, stats);
+        compact_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, kExpand, 0, offsets, list, stop);
+        plan_kernel<<<1, 1, 0, s>>>(offsets + nb, stats, target, resident, w);
+        copy_rule_kernel<<<gridFor(target), 256, 0, s>>>(rule, fillList, list, stats);
         note_launch(5);
         if ((e = cudaGetLastError()) != cudaSuccess) return report_cuda_error(e, "recompute list");
         if ((e = launch_lle_regime_list(rj, nSel, n, rl, rc, scr, scrBytes, rerr, s)) != cudaSuccess)

@@ -261,6 +261,10 @@ typedef struct cbf_surrogate_config {
                                 point takes the class and LLE of its nearest coarse-grid
                                 label, confidence 1 (the ablation that measures what the
                                 learning adds; same mask, audit and expansion rules) */
+    int32_t auditFill;       /* 1: points that only the audit sample selected are not fed
+                                with the other rule points; they fill every recompute round
+                                up to a whole number of waves of resident LLE_REGIME
+                                threads (0) */
 } cbf_surrogate_config;
 void cbf_surrogate_config_init(cbf_surrogate_config* cfg);
 
