@@ -122,6 +122,7 @@ class SurrogateConfig(C.Structure):
         ("maxWaves", C.c_int32),
         ("predictor", C.c_int32),
         ("auditFill", C.c_int32),
+        ("idleRadius", C.c_int32),
     ]
 
 
@@ -392,7 +393,7 @@ def grid_coordinates(job: Job) -> np.ndarray:
     return out
 
 
-NUM_LLE_VARIANTS = 5
+NUM_LLE_VARIANTS = 8
 
 
 def autotune(job: Job):

@@ -174,7 +174,7 @@ constexpr int kBifBlockThreads = 128;
 // Launchers (defined in lle.cu / bif.cu / probes.cu).  All return a CUDA error.
 cudaError_t launch_lle(const DevJob& J, double* d_out, cudaStream_t s);
 // LLE kernel shapes (lle.cu): the autotuner's search space.
-constexpr int kNumLleVariants = 5;
+constexpr int kNumLleVariants = CBF_NUM_LLE_VARIANTS;
 cudaError_t launch_lle_variant(const DevJob& J, double* d_out, cudaStream_t s, int variant);
 // The shape cbf_run uses for `system` on the current device (capi.cu).
 int lle_variant_for(int system);

@@ -24,7 +24,7 @@ namespace cbf {
 
 namespace {
 
-template <class S, bool IC, int PPT, int THREADS, int MINB>
+template <class S, bool IC, int PPT, int THREADS, int MINB, int UNR>
 __global__ void __launch_bounds__(THREADS, MINB) lle_kernel(const DevJob J, double* __restrict__ out)
 {
     constexpr int D = S::DIM;
@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(THREADS, MINB) lle_kernel(const DevJob J, doub
             to_stored<S>(x[j], c[j]);
         }
 
-        run_checked<S, PPT>(x, c, J.nSkip, J);
+        run_checked<S, PPT, UNR>(x, c, J.nSkip, J);
 
 #pragma unroll
         for (int j = 0; j < PPT; ++j) {
@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(THREADS, MINB) lle_kernel(const DevJob J, doub
 #pragma unroll
         for (int j = 0; j < PPT; ++j) result[j] = 0;
         for (int b = 0; b < J.nRecord; ++b) {
-            run_pair<S, PPT>(x, y, c, J.nNT, J);
+            run_pair<S, PPT, UNR>(x, y, c, J.nNT, J);
 #pragma unroll
             for (int j = 0; j < PPT; ++j) {
                 double t = 0;
@@ -107,25 +107,29 @@ cudaError_t launch_seeds_d(const DevJob& J, double* d_out, cudaStream_t s)
     return cudaGetLastError();
 }
 
-template <class S, bool IC, int PPT, int THREADS, int MINB>
+template <class S, bool IC, int PPT, int THREADS, int MINB, int UNR = 2>
 cudaError_t launch_variant(const DevJob& J, double* d_out, cudaStream_t s)
 {
     const long long nq = (J.nPoints + PPT - 1) / PPT;
     const long long blocks = (nq + THREADS - 1) / THREADS;
     const unsigned grid = (unsigned)(blocks < (1ll << 30) ? blocks : (1ll << 30));
     if (grid == 0) return cudaSuccess;
-    lle_kernel<S, IC, PPT, THREADS, MINB><<<grid, THREADS, 0, s>>>(J, d_out);
+    lle_kernel<S, IC, PPT, THREADS, MINB, UNR><<<grid, THREADS, 0, s>>>(J, d_out);
     note_launch();
     return cudaGetLastError();
 }
 
 // The kernel shapes the autotuner chooses from: {points per thread, threads per
-// block, minimum resident blocks per SM (a register cap for the compiler)}.
-//   0: 1 pt, 128 thr, >= 8 blocks/SM  (<= 64 registers, 32 warps/SM)  default
-//   1: 1 pt, 128 thr, no cap
-//   2: 1 pt, 256 thr, >= 4 blocks/SM  (<= 64 registers)
-//   3: 2 pt, 128 thr, >= 4 blocks/SM  (<= 128 registers, 4 chains per thread)
-//   4: 2 pt, 128 thr, >= 3 blocks/SM  (<= 170 registers)
+// block, minimum resident blocks per SM (a register cap for the compiler),
+// unrolling of the step loop}.
+//   0: 1 pt, 128 thr, >= 8 blocks/SM  (<= 64 registers, 32 warps/SM), unroll 2  default
+//   1: 1 pt, 128 thr, no cap, unroll 2
+//   2: 1 pt, 256 thr, >= 4 blocks/SM  (<= 64 registers), unroll 2
+//   3: 2 pt, 128 thr, >= 4 blocks/SM  (<= 128 registers, 4 chains per thread), unroll 2
+//   4: 2 pt, 128 thr, >= 3 blocks/SM  (<= 170 registers), unroll 2
+//   5: 1 pt, 128 thr, no cap, unroll 4
+//   6: 1 pt, 128 thr, >= 8 blocks/SM, unroll 4
+//   7: 1 pt, 128 thr, no cap, unroll 8
 template <class S, bool IC>
 cudaError_t launch_lle_v(const DevJob& J, double* d_out, cudaStream_t s, int variant)
 {
@@ -134,6 +138,9 @@ cudaError_t launch_lle_v(const DevJob& J, double* d_out, cudaStream_t s, int var
     case 2: return launch_variant<S, IC, 1, 256, 4>(J, d_out, s);
     case 3: return launch_variant<S, IC, 2, 128, 4>(J, d_out, s);
     case 4: return launch_variant<S, IC, 2, 128, 3>(J, d_out, s);
+    case 5: return launch_variant<S, IC, 1, 128, 1, 4>(J, d_out, s);
+    case 6: return launch_variant<S, IC, 1, 128, 8, 4>(J, d_out, s);
+    case 7: return launch_variant<S, IC, 1, 128, 1, 8>(J, d_out, s);
     default: return launch_variant<S, IC, 1, 128, 8>(J, d_out, s);
     }
 }

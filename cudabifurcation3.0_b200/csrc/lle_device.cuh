@@ -19,14 +19,15 @@ __device__ __forceinline__ void copy_state(double (&d)[D], const double (&s)[D])
 
 // loopCalculateDiscreteModel(x, values, h, n, 1, 0, maxValue, nullptr) for PPT
 // independent points: n steps each, a point stops after its first step with
-// |x[0]| past the bound and stays stopped for the rest of the call.
-template <class S, int PPT>
+// |x[0]| past the bound and stays stopped for the rest of the call.  UNR: the
+// unrolling of the step loop (a kernel-shape parameter).
+template <class S, int PPT, int UNR = 2>
 __device__ __forceinline__ void run_checked(double (&x)[PPT][S::DIM],
                                             const typename S::Coef (&c)[PPT], int n,
                                             const DevJob& J)
 {
     if (!J.checkDiv) {
-#pragma unroll 2
+#pragma unroll UNR
         for (int i = 0; i < n; ++i) {
 #pragma unroll
             for (int j = 0; j < PPT; ++j) S::step(x[j], c[j]);
@@ -45,7 +46,7 @@ __device__ __forceinline__ void run_checked(double (&x)[PPT][S::DIM],
             copy_state<S::DIM>(x0[j], x[j]);
             mx[j] = 0;
         }
-#pragma unroll 2
+#pragma unroll UNR
         for (int i = 0; i < m; ++i) {
 #pragma unroll
             for (int j = 0; j < PPT; ++j) {
@@ -74,12 +75,12 @@ __device__ __forceinline__ void run_checked(double (&x)[PPT][S::DIM],
 // The two NT-interval integrations of one renormalisation block
 // (cudaLibrary.cu:748-754) for PPT points, interleaved; each trajectory stops at
 // its own first violation within the interval.
-template <class S, int PPT>
+template <class S, int PPT, int UNR = 2>
 __device__ __forceinline__ void run_pair(double (&x)[PPT][S::DIM], double (&y)[PPT][S::DIM],
                                          const typename S::Coef (&c)[PPT], int n, const DevJob& J)
 {
     if (!J.checkDiv) {
-#pragma unroll 2
+#pragma unroll UNR
         for (int i = 0; i < n; ++i) {
 #pragma unroll
             for (int j = 0; j < PPT; ++j) {
@@ -97,7 +98,7 @@ __device__ __forceinline__ void run_pair(double (&x)[PPT][S::DIM], double (&y)[P
         copy_state<S::DIM>(y0[j], y[j]);
         mx[j] = my[j] = 0;
     }
-#pragma unroll 2
+#pragma unroll UNR
     for (int i = 0; i < n; ++i) {
 #pragma unroll
         for (int j = 0; j < PPT; ++j) {

@@ -223,6 +223,7 @@ struct Refine {
     long long tiles;    // 32-point warp tiles of all rounds
     int rounds;         // rounds that computed at least one point
     int stop;           // a round found nothing to compute: the later rounds are empty
+    int radius;         // expansion radius after this round
 };
 
 // One thread: the round's list is every expansion mark of the previous rounds
@@ -232,8 +233,11 @@ struct Refine {
 // when audit-only points are kept back (d0 > 0), as many of them as fill the
 // round up to a whole number of waves of `wave` resident points (a round with
 // nothing else takes `target` of them).
+// The expansion after the round uses radius `idleR` when the round fills less
+// than half a wave (the chain of expansion rounds alone: the wider ring costs
+// no time there), else `busyR`.
 __global__ void plan_kernel(const long long* __restrict__ nMarked, Refine* R, long long target, long long wave,
-                            int round)
+                            int round, int busyR, int idleR)
 {
     if (R->stop) return;
     const long long nA = *nMarked;
@@ -253,6 +257,7 @@ __global__ void plan_kernel(const long long* __restrict__ nMarked, Refine* R, lo
     R->nSel = nSel;
     R->refined += nSel;
     R->tiles += (nSel + 31) / 32;
+    R->radius = 2 * nSel < wave ? idleR : busyR;
     if (nSel > 0) R->rounds = round + 1;
     else R->stop = 1;
 }
@@ -335,10 +340,11 @@ __global__ void merge_kernel(const long long* __restrict__ list, const long long
 // selected points are computed in their own chunk and expand from there).
 // The list length is *nDev when given, else nHost.
 __global__ void expand_kernel(const long long* __restrict__ list, const unsigned char* __restrict__ surprise,
-                              const long long* __restrict__ nDev, long long nHost, int nPts, int radius,
-                              unsigned char* __restrict__ flag)
+                              const long long* __restrict__ nDev, long long nHost, int nPts, int radiusHost,
+                              const int* radiusDev, unsigned char* __restrict__ flag)
 {
     const long long n = nDev ? *nDev : nHost;
+    const int radius = radiusDev ? *radiusDev : radiusHost;
     const long long step = (long long)gridDim.x * blockDim.x;
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += step) {
         if (!surprise[k]) continue;
@@ -476,7 +482,7 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
     if (job->nPts < 3 || cfg->coarseSide < 2 || cfg->randomPoints < 0 || cfg->batch < 1 ||
         cfg->trainSteps < 0 || !(cfg->lr > 0) || cfg->boundaryRadius < 0 || cfg->boundaryRadius > 8 ||
         cfg->expandRadius < -1 || cfg->expandRadius > 16 || cfg->maxWaves < 0 || cfg->maxWaves > 1000000 ||
-        cfg->predictor < 0 || cfg->predictor > 1 || cfg->auditFill < 0 || cfg->auditFill > 1 || !(cfg->auditFraction >= 0 && cfg->auditFraction <= 1))
+        cfg->predictor < 0 || cfg->predictor > 1 || cfg->auditFill < 0 || cfg->auditFill > 1 || cfg->idleRadius < 0 || cfg->idleRadius > 16 || !(cfg->auditFraction >= 0 && cfg->auditFraction <= 1))
         return report_error(CBF_ERR_INVALID_ARG, "bad surrogate configuration");
     DevJob dj;
     cbf_status st = lower_job_for(job, &dj);
@@ -639,7 +645,7 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
         });
     if (e == cudaSuccess && er > 0)
         e = launch1d(nLab, s, [&](unsigned b, int t) {
-            expand_kernel<<<b, t, 0, s>>>(dIdx, lsur, nullptr, nLab, nPts, er, flag);
+            expand_kernel<<<b, t, 0, s>>>(dIdx, lsur, nullptr, nLab, nPts, er, nullptr, flag);
         });
     if (e == cudaSuccess) e = cudaMemsetAsync(stats, 0, sizeof(Refine), s);
     if (e != cudaSuccess) return report_cuda_error(e, "refinement mask");
@@ -656,6 +662,7 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
     // expansion round, and the rounds after the last one with work return at
     // once.
     const bool fillAudit = cfg->auditFill != 0;
+    const int idleR = cfg->idleRadius > 0 && er > 0 ? cfg->idleRadius : er;
     const unsigned char want = kBoundary | kLowConf | (fillAudit ? 0 : kAudit);
     long long* rule = nullptr;
     long long* fillList = nullptr;
@@ -728,7 +735,7 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
         count_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, kExpand, 0, blockCount, stop);
         scan_kernel<<<1, 1024, 0, s>>>(blockCount, nb, offsets, stop);
         compact_kernel<<<nb, kChunkThreads, 0, s>>>(flag, n, kExpand, 0, offsets, list, stop);
-        plan_kernel<<<1, 1, 0, s>>>(offsets + nb, stats, target, resident, w);
+        plan_kernel<<<1, 1, 0, s>>>(offsets + nb, stats, target, resident, w, er, idleR);
         copy_rule_kernel<<<gridFor(target), 256, 0, s>>>(rule, fillList, list, stats);
         note_launch(5);
         if ((e = cudaGetLastError()) != cudaSuccess) return report_cuda_error(e, "recompute list");
@@ -737,7 +744,7 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
         merge_kernel<<<gridFor(n), 256, 0, s>>>(list, nSel, rl, rc, flag, dLle, dCls, src, sur, stats);
         note_launch();
         if (er > 0 && w < cfg->maxWaves) {
-            expand_kernel<<<gridFor(n), 256, 0, s>>>(list, sur, nSel, 0, nPts, er, flag);
+            expand_kernel<<<gridFor(n), 256, 0, s>>>(list, sur, nSel, 0, nPts, 0, &stats->radius, flag);
             note_launch();
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return report_cuda_error(e, "merge");

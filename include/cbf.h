@@ -152,11 +152,11 @@ cbf_status cbf_run(const cbf_job* job, void* d_out, void* d_aux, void* stream);
 
 /* ---- autotuning ------------------------------------------------------ */
 /* The LLE kernel exists in CBF_NUM_LLE_VARIANTS shapes (points per thread 1|2,
- * threads per block, register cap).  cbf_autotune times all of them on a
+ * threads per block, register cap, unrolling of the step loop).  cbf_autotune times all of them on a
  * shortened copy of `job` on the current device and makes the fastest the one
  * cbf_run (and every LLE entry point) uses for job->system on this device.
  * msPerVariant (optional) receives each shape's trial time. */
-#define CBF_NUM_LLE_VARIANTS 5
+#define CBF_NUM_LLE_VARIANTS 8
 cbf_status cbf_autotune(const cbf_job* job, int32_t* chosenVariant, double* msPerVariant);
 /* Set (variant >= 0) or reset to the default (-1) the shape for a system. */
 cbf_status cbf_set_lle_variant(int32_t system, int32_t variant);
@@ -265,6 +265,10 @@ typedef struct cbf_surrogate_config {
                                 with the other rule points; they fill every recompute round
                                 up to a whole number of waves of resident LLE_REGIME
                                 threads (0) */
+    int32_t idleRadius;      /* expansion radius after a round that computed fewer points than
+                                half a wave of resident LLE_REGIME threads (only the chain
+                                of expansion rounds is left; the idle threads pay for the
+                                wider ring); 0 (default): expandRadius */
 } cbf_surrogate_config;
 void cbf_surrogate_config_init(cbf_surrogate_config* cfg);
 

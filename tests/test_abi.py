@@ -283,7 +283,7 @@ def test_surrogate_config_defaults(cbf):
     assert (c.coarseSide, c.randomPoints, c.batch, c.trainSteps) == (512, 65536, 4096, 1500)
     assert c.confThreshold == pytest.approx(0.4) and c.auditFraction == pytest.approx(0.01)
     assert (c.boundaryRadius, c.expandRadius, c.maxWaves, c.refine) == (1, -1, 20, 1)
-    assert (c.predictor, c.auditFill) == (0, 0)
+    assert (c.predictor, c.auditFill, c.idleRadius) == (0, 0, 0)
     with pytest.raises(AttributeError):
         cbf.surrogate_config(noSuchField=1)
 

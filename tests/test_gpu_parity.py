@@ -262,6 +262,30 @@ def test_lle_map_matches_oracle(cbf, orc, gpu_ok, extra):
     assert np.isfinite(want).mean() > 0.9
 
 
+@pytest.mark.parametrize("extra", [dict(), dict(maxValue=20.0), dict(sweepIC=True, idxMut=[0, 2],
+                                                                    ranges=[-16, 16, 5, 30])])
+def test_every_lle_kernel_shape_gives_the_same_map(cbf, orc, gpu_ok, extra):
+    """Every shape the autotuner chooses from (points per thread, block size,
+    register cap, step-loop unrolling) runs the same arithmetic: its map equals
+    the oracle's, and shape 0's bit for bit; 37 points leave partial
+    blocks and, with two points per thread, a half-used thread."""
+    kw = dict(CHEN_LLE, nPts=37)
+    kw.update(extra)
+    j, o = both(cbf, orc, task=cbf.TASK_LLE, **kw)
+    want = orc.map_lle_seeded(o, 0, 37 * 37, cbf.lle_seeds(j))
+    maps = []
+    try:
+        for v in range(cbf.NUM_LLE_VARIANTS):
+            cbf.set_lle_variant("chen", v)
+            got, _ = cbf.run_host(j)
+            assert_lle_close(got, want)
+            maps.append(got)
+    finally:
+        cbf.set_lle_variant("chen", -1)
+    for m in maps[1:]:
+        assert np.array_equal(m, maps[0], equal_nan=True)
+
+
 @pytest.mark.parametrize("params,extra", [
     (LORENZ, dict(ranges=[5, 20, 20, 200], idxMut=[1, 2], h=0.005)),
     (ROSSLER, dict(ranges=[0.05, 0.35, 0.05, 0.35], idxMut=[1, 2], h=0.01)),
