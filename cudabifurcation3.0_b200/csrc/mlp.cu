@@ -3,22 +3,21 @@
 //
 // Output 0 is the (normalised) LLE, outputs 1..16 the logits of the 16-way
 // peak-count regime class.  Parameters live as FP32 masters (Adam state next to
-// them) plus BF16 copies that feed the tensor cores.  Prediction over a whole
-// grid runs as one fused tcgen05 kernel (mlp_tc.cuh).  Training and the
-// prediction of explicit feature rows put every matrix product -- forward,
-// input gradients, weight gradients -- through one tensor-core
-// GEMM: mma.sync m16n8k16 BF16 x BF16 -> FP32, 64x64 CTA tiles, operands staged
-// in shared memory in their memory order (k- or m/n-contiguous) by double-buffered
-// 16-byte cp.async copies and read with ldmatrix (.trans for m/n-contiguous
-// tiles), so transposed products need no copies, and fused epilogues (bias, SiLU
-// with the pre-activation kept,
-// SiLU-derivative product for the backward pass, FP32 and/or BF16 stores).  A
-// training step (minibatch gather, 4 forward GEMMs, loss, 7 backward GEMMs, bias
-// reductions, Adam) is captured once as a CUDA graph and replayed.
+// them) plus BF16 copies that feed the tensor cores.  Every matrix product --
+// forward, input gradients, weight gradients, the prediction of explicit
+// feature rows -- runs on the 5th-generation tensor cores through one kernel
+// (mlp_gemm_tc.cuh: TMA-staged operands, tcgen05.mma into tensor memory, fused
+// epilogues); prediction over a whole grid runs as one fused tcgen05 kernel
+// (mlp_tc.cuh).  A training step (minibatch gather, 4 forward products, loss,
+// 7 backward products with their split-K and bias reductions, Adam) is captured
+// once as a CUDA graph and replayed.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <math.h>
 #include <string.h>
 
+#include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "mlp.cuh"
@@ -38,220 +37,20 @@ constexpr long long kW3 = kB2 + kHid, kB3 = kW3 + kHid * kHid;
 constexpr long long kW4 = kB3 + kHid, kB4 = kW4 + kOut * kHid;
 constexpr long long kNumParams = kB4 + kOut;
 
-struct GemmDesc {
-    const bf16* A;       // element (m, k) at A[m*a_m + k*a_k]
-    long long a_m, a_k;
-    const bf16* B;       // element (k, n) at B[k*b_k + n*b_n]
-    long long b_k, b_n;
-    int M, N, K;
-    const float* bias;   // [N] or null
-    int act;             // 1: SiLU
-    const float* dz;     // optional: result *= silu'(dz[m*ldz + n])
-    long long ldz;
-    float* Z;            // optional: pre-activation (after bias)
-    long long ldZ;
-    float* C;            // optional FP32 result at C[m*c_m + n*c_n]
-    long long c_m, c_n;
-    bf16* Cb;            // optional BF16 result, row-major with ldCb
-    long long ldCb;
-    int splitK;          // >1: FP32 partials over K slices into ws[z][M*N], then summed
-    float* ws;
-};
-
-constexpr int BM = 64, BN = 64, BK = 32, kGemmThreads = 128;
+// Tensor-core operand copies of the weights: seven 256 x 256 BF16 slots (row
+// pitch 256), zero outside the weights: W1 (256 x 4, K padded to 16), W2, W3,
+// W4 (17 x 256, rows padded), W2^T, W3^T, W4^T (256 x 17, K padded to 32).
+constexpr long long kSlot = (long long)kHid * kHid;
+enum { kSlotW1 = 0, kSlotW2, kSlotW3, kSlotW4, kSlotW2T, kSlotW3T, kSlotW4T, kNumSlots };
+constexpr int kXPitch = 16;    // BF16 input rows: 4 features padded to one K = 16 step
+constexpr int kDOutPitch = 32;  // BF16 output-gradient rows: 17 values padded to K = 32
+constexpr int kDOutTRows = 128; // rows of dOut^T (17 used): one full 128-row operand tile
 
 __device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
 __device__ __forceinline__ float silu_grad(float z)
 {
     const float s = 1.0f / (1.0f + __expf(-z));
     return s * (1.0f + z * (1.0f - s));
-}
-
-__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], const uint32_t (&b)[2])
-{
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
-        "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-
-// Operand staging modes: K-major (k contiguous in memory), MN-major (m or n
-// contiguous) -- both 16-byte cp.async copies, double-buffered -- or scalar
-// loads for operands whose rows are not 16-byte multiples (K = 4, N = 17).
-enum { kScalar = 0, kKMajor = 1, kMNMajor = 2 };
-constexpr int kTileElems = BM * (BK + 8);  // >= BK * (BM + 8): both tile shapes fit
-constexpr int kPitchK = BK + 8;            // K-major tile [64][40]: 80-byte rows
-constexpr int kPitchMN = BM + 8;           // MN-major tile [32][72]: 144-byte rows
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid)
-{
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    const int bytes = valid ? 16 : 0;  // 0: zero-fill, nothing read
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
-
-__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], const bf16* p)
-{
-    const unsigned s = (unsigned)__cvta_generic_to_shared(p);
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(s));
-}
-__device__ __forceinline__ void ldsm_x4_t(uint32_t (&r)[4], const bf16* p)
-{
-    const unsigned s = (unsigned)__cvta_generic_to_shared(p);
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(s));
-}
-
-// One operand tile (rows r0 .. r0+64 of the M or N dimension, k0 .. k0+32) into
-// shared memory.  Element (r, k) of the operand is at P[r*sr + k*sk].
-template <int MODE>
-__device__ __forceinline__ void load_tile(bf16* sm, const bf16* P, long long sr, long long sk, int R, int r0,
-                                          int k0, int kEnd)
-{
-    if (MODE == kKMajor) {  // sm[r][k]
-        for (int c = threadIdx.x; c < BM * (BK / 8); c += kGemmThreads) {
-            const int r = c / (BK / 8), kc = (c % (BK / 8)) * 8;
-            const bool v = r0 + r < R && k0 + kc < kEnd;
-            cp_async16(sm + r * kPitchK + kc, v ? P + (long long)(r0 + r) * sr + (k0 + kc) : P, v);
-        }
-    } else if (MODE == kMNMajor) {  // sm[k][r]
-        for (int c = threadIdx.x; c < BK * (BM / 8); c += kGemmThreads) {
-            const int k = c / (BM / 8), rc = (c % (BM / 8)) * 8;
-            const bool v = k0 + k < kEnd && r0 + rc < R;
-            cp_async16(sm + k * kPitchMN + rc, v ? P + (long long)(k0 + k) * sk + (r0 + rc) : P, v);
-        }
-    } else {  // scalar, into the K-major shape; walks the unit-stride dimension fastest
-        const bf16 zero = __float2bfloat16_rn(0.f);
-        const bool kFast = sk == 1;
-        for (int e = threadIdx.x; e < BM * BK; e += kGemmThreads) {
-            const int r = kFast ? e / BK : e % BM, c = kFast ? e % BK : e / BM;
-            const int rr = r0 + r, k = k0 + c;
-            sm[r * kPitchK + c] = (rr < R && k < kEnd) ? P[rr * sr + k * sk] : zero;
-        }
-    }
-}
-
-template <int AM, int BMD>
-__global__ void __launch_bounds__(kGemmThreads) gemm_bf16_kernel(const GemmDesc g)
-{
-    __shared__ __align__(128) bf16 smA[2][kTileElems];
-    __shared__ __align__(128) bf16 smB[2][kTileElems];
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    const int gq = lane >> 2, tq = lane & 3;
-    const int lq = lane >> 3, l8 = lane & 7;  // ldmatrix: matrix and row of this lane's address
-    float acc[2][4][4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.f;
-
-    // K slice of this CTA (split-K: gridDim.z slices of whole BK blocks)
-    const int kPer = ((g.K + BK - 1) / BK + gridDim.z - 1) / gridDim.z * BK;
-    const int kBeg = blockIdx.z * kPer;
-    const int kEnd = min(g.K, kBeg + kPer);
-    const int nk = kEnd > kBeg ? (kEnd - kBeg + BK - 1) / BK : 0;
-
-    if (nk > 0) {
-        load_tile<AM>(smA[0], g.A, g.a_m, g.a_k, g.M, m0, kBeg, kEnd);
-        load_tile<BMD>(smB[0], g.B, g.b_n, g.b_k, g.N, n0, kBeg, kEnd);
-    }
-    cp_async_commit();
-    for (int it = 0; it < nk; ++it) {
-        const int cur = it & 1;
-        if (it + 1 < nk) {
-            const int k1 = kBeg + (it + 1) * BK;
-            load_tile<AM>(smA[cur ^ 1], g.A, g.a_m, g.a_k, g.M, m0, k1, kEnd);
-            load_tile<BMD>(smB[cur ^ 1], g.B, g.b_n, g.b_k, g.N, n0, k1, kEnd);
-        }
-        cp_async_commit();
-        cp_async_wait1();
-        __syncthreads();
-        const bf16* As = smA[cur];
-        const bf16* Bs = smB[cur];
-#pragma unroll
-        for (int kk = 0; kk < BK; kk += 16) {
-            uint32_t a[2][4], b[4][2];
-#pragma unroll
-            for (int mi = 0; mi < 2; ++mi) {
-                const int mb = wm + mi * 16;
-                if (AM == kMNMajor)
-                    ldsm_x4_t(a[mi], As + (kk + (lq >> 1) * 8 + l8) * kPitchMN + mb + (lq & 1) * 8);
-                else
-                    ldsm_x4(a[mi], As + (mb + (lq & 1) * 8 + l8) * kPitchK + kk + (lq >> 1) * 8);
-            }
-#pragma unroll
-            for (int np = 0; np < 2; ++np) {
-                const int nb = wn + np * 16;
-                uint32_t r[4];
-                if (BMD == kMNMajor)
-                    ldsm_x4_t(r, Bs + (kk + (lq & 1) * 8 + l8) * kPitchMN + nb + (lq >> 1) * 8);
-                else
-                    ldsm_x4(r, Bs + (nb + (lq >> 1) * 8 + l8) * kPitchK + kk + (lq & 1) * 8);
-                b[2 * np][0] = r[0];
-                b[2 * np][1] = r[1];
-                b[2 * np + 1][0] = r[2];
-                b[2 * np + 1][1] = r[3];
-            }
-#pragma unroll
-            for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-                for (int ni = 0; ni < 4; ++ni) mma_bf16(acc[mi][ni], a[mi], b[ni]);
-        }
-        __syncthreads();
-    }
-
-#pragma unroll
-    for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-        for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                const int m = m0 + wm + mi * 16 + gq + (v >= 2 ? 8 : 0);
-                const int n = n0 + wn + ni * 8 + 2 * tq + (v & 1);
-                if (m >= g.M || n >= g.N) continue;
-                float z = acc[mi][ni][v];
-                if (g.splitK > 1) {
-                    g.ws[((long long)blockIdx.z * g.M + m) * g.N + n] = z;
-                    continue;
-                }
-                if (g.bias) z += g.bias[n];
-                if (g.Z) g.Z[m * g.ldZ + n] = z;
-                if (g.dz) z *= silu_grad(g.dz[m * g.ldz + n]);
-                const float y = g.act ? silu(z) : z;
-                if (g.C) g.C[m * g.c_m + n * g.c_n] = y;
-                if (g.Cb) g.Cb[m * g.ldCb + n] = __float2bfloat16_rn(y);
-            }
-}
-
-bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
-
-// Staging mode of an operand: element (r, k) at P[r*sr + k*sk], R rows.
-int stage_mode(const void* P, long long sr, long long sk, int R, int K)
-{
-    if (!aligned16(P)) return kScalar;
-    if (sk == 1 && sr % 8 == 0 && K % 8 == 0) return kKMajor;
-    if (sr == 1 && sk % 8 == 0 && R % 8 == 0) return kMNMajor;
-    return kScalar;
-}
-
-template <int AM>
-void launch_gemm_b(int bm, dim3 grid, const GemmDesc& g, cudaStream_t s)
-{
-    switch (bm) {
-    case kKMajor: gemm_bf16_kernel<AM, kKMajor><<<grid, kGemmThreads, 0, s>>>(g); break;
-    case kMNMajor: gemm_bf16_kernel<AM, kMNMajor><<<grid, kGemmThreads, 0, s>>>(g); break;
-    default: gemm_bf16_kernel<AM, kScalar><<<grid, kGemmThreads, 0, s>>>(g); break;
-    }
 }
 
 // C[m*c_m + n*c_n] = sum over z of ws[z][m*N + n], slices added in order.
@@ -267,34 +66,6 @@ __global__ void splitk_reduce_kernel(const float* __restrict__ ws, int splits, i
     C[m * c_m + n * c_n] = acc;
 }
 
-cudaError_t gemm(const GemmDesc& g, cudaStream_t s)
-{
-    const int splits = g.splitK > 1 ? g.splitK : 1;
-    dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM, splits);
-    if (grid.x == 0 || grid.y == 0) return cudaSuccess;
-    const int am = stage_mode(g.A, g.a_m, g.a_k, g.M, g.K);
-    const int bm = stage_mode(g.B, g.b_n, g.b_k, g.N, g.K);
-    switch (am) {
-    case kKMajor: launch_gemm_b<kKMajor>(bm, grid, g, s); break;
-    case kMNMajor: launch_gemm_b<kMNMajor>(bm, grid, g, s); break;
-    default: launch_gemm_b<kScalar>(bm, grid, g, s); break;
-    }
-    note_launch();
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess || splits == 1) return e;
-    const long long MN = (long long)g.M * g.N;
-    splitk_reduce_kernel<<<(unsigned)((MN + 255) / 256), 256, 0, s>>>(g.ws, splits, g.M, g.N, g.C, g.c_m, g.c_n);
-    note_launch();
-    return cudaGetLastError();
-}
-
-GemmDesc gdesc()
-{
-    GemmDesc g;
-    memset(&g, 0, sizeof(g));
-    return g;
-}
-
 // ---- element-wise kernels -------------------------------------------------
 
 __device__ __forceinline__ unsigned long long mix64(unsigned long long z)
@@ -306,33 +77,49 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long z)
 }
 
 // Minibatch of B rows drawn uniformly (with replacement) from N, keyed by the
-// device step counter so a replayed graph draws a new batch every step.
+// device step counter so a replayed graph draws a new batch every step.  The
+// BF16 input rows go to xb (pitch 16, columns 4..15 stay zero) and, transposed,
+// to xT (row f = feature f, pitch ldT) for the first layer's weight gradient.
 __global__ void gather_kernel(const float* __restrict__ X, const float* __restrict__ ylle,
                               const int* __restrict__ ycls, long long N, int B,
-                              const unsigned long long* step, unsigned long long seed,
-                              bf16* __restrict__ xb, float* __restrict__ bl, int* __restrict__ bc)
+                              const unsigned long long* step, unsigned long long seed, bf16* __restrict__ xb,
+                              bf16* __restrict__ xT, long long ldT, float* __restrict__ bl, int* __restrict__ bc)
 {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= B) return;
     const unsigned long long h = mix64(seed ^ mix64(*step * 0x100000001B3ull + (unsigned long long)r));
     const long long i = (long long)(h % (unsigned long long)N);
 #pragma unroll
-    for (int f = 0; f < kIn; ++f) xb[(long long)r * kIn + f] = __float2bfloat16_rn(X[i * kIn + f]);
+    for (int f = 0; f < kIn; ++f) {
+        const bf16 v = __float2bfloat16_rn(X[i * kIn + f]);
+        xb[(long long)r * kXPitch + f] = v;
+        xT[f * ldT + r] = v;
+    }
     bl[r] = ylle[i];
     bc[r] = ycls[i];
 }
 
 // Loss: mean squared error on output 0 (normalised LLE) + cross-entropy of
-// outputs 1..16; writes dLoss/dOut (FP32 and BF16) and accumulates the loss.
+// outputs 1..16; writes dLoss/dOut in FP32 (dOut, pitch 17, for the bias
+// gradient), in BF16 (dOutB, pitch 32, columns 17..31 zero) and transposed in
+// BF16 (dOutT, pitch ldT) for the products, and accumulates the loss.  Rows
+// n <= r < rows (the rest of the last 128-row tile) write zero gradients.
 __global__ void loss_kernel(const float* __restrict__ out, const float* __restrict__ yl,
-                            const int* __restrict__ yc, int B, float wLle, float* __restrict__ dOut,
-                            bf16* __restrict__ dOutB, float* __restrict__ lossAcc)
+                            const int* __restrict__ yc, int n, int rows, float wLle, float* __restrict__ dOut,
+                            bf16* __restrict__ dOutB, bf16* __restrict__ dOutT, long long ldT,
+                            float* __restrict__ lossAcc)
 {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= B) return;
+    if (r >= rows) return;
+    const bf16 zero = __float2bfloat16_rn(0.0f);
+    if (r >= n) {
+        for (int c = 0; c < kDOutPitch; ++c) dOutB[(long long)r * kDOutPitch + c] = zero;
+        for (int c = 0; c < kOut; ++c) dOutT[c * ldT + r] = zero;
+        return;
+    }
     const float* o = out + (long long)r * kOut;
-    float* d = dOut + (long long)r * kOut;
-    const float invB = 1.0f / (float)B;
+    float d[kOut];
+    const float invB = 1.0f / (float)n;
     const float e = o[0] - yl[r];
     d[0] = 2.0f * wLle * e * invB;
     float mx = o[1];
@@ -346,7 +133,13 @@ __global__ void loss_kernel(const float* __restrict__ out, const float* __restri
         d[1 + c] = (p - (c == t ? 1.0f : 0.0f)) * invB;
         if (c == t) lossCe = -logf(fmaxf(p, 1e-30f));
     }
-    for (int c = 0; c < kOut; ++c) dOutB[(long long)r * kOut + c] = __float2bfloat16_rn(d[c]);
+    for (int c = 0; c < kOut; ++c) {
+        const bf16 v = __float2bfloat16_rn(d[c]);
+        dOut[(long long)r * kOut + c] = d[c];
+        dOutB[(long long)r * kDOutPitch + c] = v;
+        dOutT[c * ldT + r] = v;
+    }
+    for (int c = kOut; c < kDOutPitch; ++c) dOutB[(long long)r * kDOutPitch + c] = zero;
     atomicAdd(lossAcc, (wLle * e * e + lossCe) * invB);
 }
 
@@ -377,10 +170,32 @@ cudaError_t colsum(const float* G, int M, int N, long long ld, float* db, cudaSt
     return cudaGetLastError();
 }
 
-// Adam on the flat FP32 parameters; refreshes the BF16 weight copies.
+// BF16 weight w = parameter i into its tensor-core operand slots (and, for W2,
+// W3 and W4, the transposed slot).
+__device__ __forceinline__ void put_weight(bf16* __restrict__ tw, long long i, bf16 w)
+{
+    if (i < kB1) {
+        tw[kSlotW1 * kSlot + (i / kIn) * kHid + i % kIn] = w;
+    } else if (i >= kW2 && i < kB2) {
+        const long long j = i - kW2;
+        tw[kSlotW2 * kSlot + j] = w;
+        tw[kSlotW2T * kSlot + (j % kHid) * kHid + j / kHid] = w;
+    } else if (i >= kW3 && i < kB3) {
+        const long long j = i - kW3;
+        tw[kSlotW3 * kSlot + j] = w;
+        tw[kSlotW3T * kSlot + (j % kHid) * kHid + j / kHid] = w;
+    } else if (i >= kW4 && i < kB4) {
+        const long long j = i - kW4;
+        tw[kSlotW4 * kSlot + j] = w;
+        tw[kSlotW4T * kSlot + (j % kHid) * kHid + j / kHid] = w;
+    }
+}
+
+// Adam on the flat FP32 parameters; refreshes the BF16 weight copies (flat and
+// tensor-core operand slots).
 __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ gr, float* __restrict__ m1,
-                            float* __restrict__ m2, bf16* __restrict__ pb, long long n, float lr0,
-                            int horizon, float b1, float b2, float eps, const unsigned long long* step)
+                            float* __restrict__ m2, bf16* __restrict__ pb, bf16* __restrict__ tw, long long n,
+                            float lr0, int horizon, float b1, float b2, float eps, const unsigned long long* step)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const float t = (float)(*step + 1);
@@ -400,17 +215,34 @@ __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ gr,
         const float vh = v / (1.f - powf(b2, t));
         const float w = p[i] - lr * ah / (sqrtf(vh) + eps);
         p[i] = w;
-        pb[i] = __float2bfloat16_rn(w);
+        const bf16 wb = __float2bfloat16_rn(w);
+        pb[i] = wb;
+        put_weight(tw, i, wb);
     }
 }
 
-__global__ void bump_kernel(unsigned long long* step) { *step += 1; }
-
-__global__ void to_bf16_kernel(const float* __restrict__ a, bf16* __restrict__ b, long long n)
+// BF16 copies (flat and operand slots) of the FP32 parameters.
+__global__ void expand_params_kernel(const float* __restrict__ p, bf16* __restrict__ pb, bf16* __restrict__ tw,
+                                     long long n)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) b[i] = __float2bfloat16_rn(a[i]);
+    if (i >= n) return;
+    const bf16 wb = __float2bfloat16_rn(p[i]);
+    pb[i] = wb;
+    put_weight(tw, i, wb);
 }
+
+// FP32 feature rows [n x 4] -> BF16 operand rows (pitch 16; columns 4..15 are
+// left as they are: zero).
+__global__ void rows_to_bf16_kernel(const float* __restrict__ X, long long n, bf16* __restrict__ xb)
+{
+    const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+#pragma unroll
+    for (int f = 0; f < kIn; ++f) xb[r * kXPitch + f] = __float2bfloat16_rn(X[r * kIn + f]);
+}
+
+__global__ void bump_kernel(unsigned long long* step) { *step += 1; }
 
 // Prediction head: LLE (de-normalised), argmax class, softmax confidence.
 __global__ void head_kernel(const float* __restrict__ out, long long n, float lleMean, float lleStd,
@@ -456,6 +288,7 @@ __global__ void features_kernel(const FeatureSpec f, const long long* __restrict
 }
 
 #include "mlp_tc.cuh"
+#include "mlp_gemm_tc.cuh"
 
 template <class F>
 cudaError_t launch1d(long long n, cudaStream_t s, F f)
@@ -472,28 +305,44 @@ cudaError_t launch1d(long long n, cudaStream_t s, F f)
 
 // ---------------------------------------------------------------------------
 
+// Tensor maps of every operand the products read (fixed buffers, built once).
+struct TcMaps {
+    // A operands (128-row tiles): the training batch ...
+    CUtensorMap aX, aH1, aH2, aH3, aDOut, aDZ3, aDZ2, aDOutT, aDZ3T, aDZ2T, aDZ1T;
+    // ... and the prediction workspace
+    CUtensorMap pX, pH1, pH2, pH3;
+    // B operands: weights, transposed weights, transposed activations
+    CUtensorMap bW1, bW2, bW3, bW4, bW4T, bW3T, bW2T, bH3T, bH2T, bH1T, bXT;
+};
+
 struct Mlp {
     int B = 0;               // training batch
+    long long Ba = 0;        // rows of every batch buffer: B rounded up to 128, at least 4096
     unsigned long long seed = 0;
     float* params = nullptr;  // FP32 masters (kNumParams)
     float* grads = nullptr;
     float* m1 = nullptr;
     float* m2 = nullptr;
-    bf16* pb = nullptr;       // BF16 copies
-    // batch buffers
-    bf16* xb = nullptr;
+    bf16* pb = nullptr;       // BF16 copies, flat layout (packed for the grid prediction)
+    bf16* tw = nullptr;       // BF16 copies in the tensor-core operand slots
+    // batch buffers (row-major; "T": transposed, pitch Ba)
+    bf16 *xb = nullptr, *xT = nullptr;
     float* yl = nullptr;
     int* yc = nullptr;
     float *z1 = nullptr, *z2 = nullptr, *z3 = nullptr;
     bf16 *h1 = nullptr, *h2 = nullptr, *h3 = nullptr;
+    bf16 *h1T = nullptr, *h2T = nullptr, *h3T = nullptr;
     float* out = nullptr;
     float* dOut = nullptr;
-    bf16* dOutB = nullptr;
+    bf16 *dOutB = nullptr, *dOutT = nullptr;
     float* dz = nullptr;      // FP32 dZ of the layer being reduced
-    bf16 *dz3 = nullptr, *dz2 = nullptr, *dz1 = nullptr;
+    bf16 *dz3 = nullptr, *dz2 = nullptr;
+    bf16 *dz3T = nullptr, *dz2T = nullptr, *dz1T = nullptr;
     float* loss = nullptr;
     float* ws = nullptr;      // split-K partials
+    int* gemmErr = nullptr;   // set by a product whose bounded wait ran out
     unsigned long long* step = nullptr;
+    TcMaps* maps = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     const float* gX = nullptr;  // training set the graph was captured for
@@ -502,7 +351,7 @@ struct Mlp {
     int gHorizon = 0;
     float gW = 0.f;
     unsigned long long gSeed = 0;
-    // inference workspace (rows per chunk = kPredRows), no pre-activations
+    // prediction workspace (rows per chunk = kPredRows), no pre-activations
     bf16 *pxb = nullptr, *ph1 = nullptr, *ph2 = nullptr, *ph3 = nullptr;
     float* pout = nullptr;
     // grid prediction on tcgen05: weights in the shared-memory operand layout
@@ -513,111 +362,145 @@ struct Mlp {
 constexpr int kPredRows = 262144;
 
 namespace {
+
+template <class T>
+cudaError_t alloc_zero(T** p, long long n)
+{
+    const size_t bytes = (size_t)(n > 0 ? n : 1) * sizeof(T);
+    cudaError_t e = cudaMalloc((void**)p, bytes);
+    if (e == cudaSuccess) e = cudaMemset(*p, 0, bytes);
+    return e;
+}
+
 cudaError_t pred_workspace(Mlp* m)
 {
     if (m->pxb) return cudaSuccess;
-    cudaError_t e = cudaMalloc((void**)&m->pxb, (size_t)kPredRows * kIn * sizeof(bf16));
-    if (e == cudaSuccess) e = cudaMalloc((void**)&m->ph1, (size_t)kPredRows * kHid * sizeof(bf16));
-    if (e == cudaSuccess) e = cudaMalloc((void**)&m->ph2, (size_t)kPredRows * kHid * sizeof(bf16));
-    if (e == cudaSuccess) e = cudaMalloc((void**)&m->ph3, (size_t)kPredRows * kHid * sizeof(bf16));
-    if (e == cudaSuccess) e = cudaMalloc((void**)&m->pout, (size_t)kPredRows * kOut * sizeof(float));
+    cudaError_t e = alloc_zero(&m->pxb, (long long)kPredRows * kXPitch);
+    if (e == cudaSuccess) e = alloc_zero(&m->ph1, (long long)kPredRows * kHid);
+    if (e == cudaSuccess) e = alloc_zero(&m->ph2, (long long)kPredRows * kHid);
+    if (e == cudaSuccess) e = alloc_zero(&m->ph3, (long long)kPredRows * kHid);
+    if (e == cudaSuccess) e = alloc_zero(&m->pout, (long long)kPredRows * kOut);
+    TcMaps& mp = *m->maps;
+    if (e == cudaSuccess) e = operand_map(&mp.pX, m->pxb, kPredRows, kXPitch, kXPitch, kGtM, 16);
+    if (e == cudaSuccess) e = operand_map(&mp.pH1, m->ph1, kPredRows, kHid, kHid, kGtM, 64);
+    if (e == cudaSuccess) e = operand_map(&mp.pH2, m->ph2, kPredRows, kHid, kHid, kGtM, 64);
+    if (e == cudaSuccess) e = operand_map(&mp.pH3, m->ph3, kPredRows, kHid, kHid, kGtM, 64);
     return e;
 }
-}  // namespace
 
-namespace {
+// Buffers of one forward pass: A-operand maps of the input and hidden
+// activations, and where the pass writes (Z and the transposes may be null).
+struct FwdBufs {
+    const CUtensorMap *aX, *aH1, *aH2, *aH3;
+    float *z1, *z2, *z3;
+    bf16 *h1, *h2, *h3;
+    bf16 *h1T, *h2T, *h3T;
+    long long ldT;
+    float* out;
+};
 
-// Forward on a batch already in xb (n rows).  Keeps Z for the backward pass.
-cudaError_t forward(Mlp& m, int n, const bf16* xb, float* out, float* z1, float* z2, float* z3,
-                    bf16* h1, bf16* h2, bf16* h3, cudaStream_t s)
+FwdBufs train_bufs(Mlp& m)
 {
-    const bf16* W = m.pb;
+    const TcMaps& mp = *m.maps;
+    return FwdBufs{&mp.aX, &mp.aH1, &mp.aH2, &mp.aH3, m.z1, m.z2, m.z3, m.h1, m.h2, m.h3,
+                   m.h1T, m.h2T, m.h3T, m.Ba, m.out};
+}
+
+FwdBufs pred_bufs(Mlp& m)
+{
+    const TcMaps& mp = *m.maps;
+    return FwdBufs{&mp.pX, &mp.pH1, &mp.pH2, &mp.pH3, nullptr, nullptr, nullptr, m.ph1, m.ph2, m.ph3,
+                   nullptr, nullptr, nullptr, 0, m.pout};
+}
+
+// Forward on n rows whose BF16 inputs are in the buffer behind f.aX.
+cudaError_t forward(Mlp& m, int n, const FwdBufs& f, cudaStream_t s)
+{
+    const TcMaps& mp = *m.maps;
     cudaError_t e;
-    GemmDesc g = gdesc();
-    g.A = xb; g.a_m = kIn; g.a_k = 1;
-    g.B = W + kW1; g.b_k = 1; g.b_n = kIn;
-    g.M = n; g.N = kHid; g.K = kIn;
-    g.bias = m.params + kB1; g.act = 1; g.Z = z1; g.ldZ = kHid; g.Cb = h1; g.ldCb = kHid;
-    if ((e = gemm(g, s)) != cudaSuccess) return e;
-    g = gdesc();
-    g.A = h1; g.a_m = kHid; g.a_k = 1;
-    g.B = W + kW2; g.b_k = 1; g.b_n = kHid;
-    g.M = n; g.N = kHid; g.K = kHid;
-    g.bias = m.params + kB2; g.act = 1; g.Z = z2; g.ldZ = kHid; g.Cb = h2; g.ldCb = kHid;
-    if ((e = gemm(g, s)) != cudaSuccess) return e;
-    g.A = h2; g.B = W + kW3; g.bias = m.params + kB3; g.Z = z3; g.Cb = h3;
-    if ((e = gemm(g, s)) != cudaSuccess) return e;
-    g = gdesc();
-    g.A = h3; g.a_m = kHid; g.a_k = 1;
-    g.B = W + kW4; g.b_k = 1; g.b_n = kHid;
-    g.M = n; g.N = kOut; g.K = kHid;
-    g.bias = m.params + kB4; g.C = out; g.c_m = kOut; g.c_n = 1;
-    return gemm(g, s);
+    TcGemm g = tc_gemm(kEpiHidden, m.gemmErr);
+    g.M = n; g.N = kHid; g.BN = 128; g.Mv = n; g.Nv = kHid;
+    g.K = kXPitch; g.KC = 16; g.kSlice = kXPitch;
+    g.bias = m.params + kB1; g.Z = f.z1; g.ldZ = kHid; g.Hb = f.h1; g.ldh = kHid; g.HT = f.h1T; g.ldht = f.ldT;
+    if ((e = gemm_tc(*f.aX, mp.bW1, g, s)) != cudaSuccess) return e;
+    g.K = kHid; g.KC = 64; g.kSlice = kHid;
+    g.bias = m.params + kB2; g.Z = f.z2; g.Hb = f.h2; g.HT = f.h2T;
+    if ((e = gemm_tc(*f.aH1, mp.bW2, g, s)) != cudaSuccess) return e;
+    g.bias = m.params + kB3; g.Z = f.z3; g.Hb = f.h3; g.HT = f.h3T;
+    if ((e = gemm_tc(*f.aH2, mp.bW3, g, s)) != cudaSuccess) return e;
+    g = tc_gemm(kEpiOut, m.gemmErr);
+    g.M = n; g.N = 32; g.BN = 32; g.Mv = n; g.Nv = kOut;
+    g.K = kHid; g.KC = 64; g.kSlice = kHid;
+    g.bias = m.params + kB4; g.C = f.out; g.ldc = kOut;
+    return gemm_tc(*f.aH3, mp.bW4, g, s);
 }
 
-// K slices for the weight-gradient products (K = batch rows): ~512 rows each.
+// K slices of the weight-gradient products (K = the batch rows padded to 64):
+// 256 rows each, wider when that would exceed kMaxSplit slices.
 constexpr int kMaxSplit = 16;
-int split_for(int n)
+int wgrad_slice(int K)
 {
-    int sp = (n + 511) / 512;
-    return sp < 1 ? 1 : (sp > kMaxSplit ? kMaxSplit : sp);
+    int sl = 256;
+    while ((K + sl - 1) / sl > kMaxSplit) sl += 64;
+    return sl;
 }
 
-// Backward from dOut (FP32 in m.dOut, BF16 in m.dOutB) to m.grads.
+// Backward from dOut (m.dOut FP32, m.dOutB and m.dOutT BF16) to m.grads.
 cudaError_t backward(Mlp& m, int n, cudaStream_t s)
 {
-    const bf16* W = m.pb;
+    const TcMaps& mp = *m.maps;
     float* G = m.grads;
     cudaError_t e;
-    // dW4 = dOut^T H3 ; db4 = colsum(dOut)
-    GemmDesc g = gdesc();
-    g.A = m.dOutB; g.a_m = 1; g.a_k = kOut;
-    g.B = m.h3; g.b_k = kHid; g.b_n = 1;
-    g.M = kOut; g.N = kHid; g.K = n;
-    g.C = G + kW4; g.c_m = kHid; g.c_n = 1;
-    g.splitK = split_for(n); g.ws = m.ws;
-    if ((e = gemm(g, s)) != cudaSuccess) return e;
+    const int Kb = (n + 63) / 64 * 64;
+    TcGemm w = tc_gemm(kEpiWgrad, m.gemmErr);  // dW = dZ^T H_prev over the batch
+    w.K = Kb; w.KC = 64; w.kSlice = wgrad_slice(Kb); w.ws = m.ws;
+    TcGemm d = tc_gemm(kEpiDgrad, m.gemmErr);  // dZ_prev = (dZ W) * silu'(Z_prev)
+    d.M = n; d.N = kHid; d.BN = 128; d.Mv = n; d.Nv = kHid;
+    d.ldzp = kHid; d.C = m.dz; d.ldc = kHid; d.ldh = kHid; d.ldht = m.Ba;
+
+    // layer 4: dW4 = dOut^T H3, db4 = colsum(dOut), dZ3 = (dOut W4) * silu'(Z3)
+    TcGemm g = w;
+    g.M = kOut; g.N = kHid; g.BN = 128; g.Mv = kOut; g.Nv = kHid; g.C = G + kW4; g.ldc = kHid;
+    if ((e = gemm_tc(mp.aDOutT, mp.bH3T, g, s)) != cudaSuccess) return e;
     if ((e = colsum(m.dOut, n, kOut, kOut, G + kB4, s)) != cudaSuccess) return e;
-    // dZ3 = (dOut W4) * silu'(Z3)
-    g = gdesc();
-    g.A = m.dOutB; g.a_m = kOut; g.a_k = 1;
-    g.B = W + kW4; g.b_k = kHid; g.b_n = 1;
-    g.M = n; g.N = kHid; g.K = kOut;
-    g.dz = m.z3; g.ldz = kHid; g.C = m.dz; g.c_m = kHid; g.c_n = 1; g.Cb = m.dz3; g.ldCb = kHid;
-    if ((e = gemm(g, s)) != cudaSuccess) return e;
-    // layers 3, 2, 1: dW = dZ^T H_prev, db = colsum(dZ), dZ_prev = (dZ W) * silu'(Z_prev)
-    const bf16* dzb[3] = {m.dz3, m.dz2, m.dz1};
-    const bf16* hp[3] = {m.h2, m.h1, m.xb};
-    const long long wOff[3] = {kW3, kW2, kW1};
-    const long long bOff[3] = {kB3, kB2, kB1};
-    const int nIn[3] = {kHid, kHid, kIn};
-    const float* zPrev[3] = {m.z2, m.z1, nullptr};
-    bf16* dzPrev[3] = {m.dz2, m.dz1, nullptr};
-    for (int l = 0; l < 3; ++l) {
-        g = gdesc();
-        g.A = dzb[l]; g.a_m = 1; g.a_k = kHid;
-        g.B = hp[l]; g.b_k = nIn[l]; g.b_n = 1;
-        g.M = kHid; g.N = nIn[l]; g.K = n;
-        g.C = G + wOff[l]; g.c_m = nIn[l]; g.c_n = 1;
-        g.splitK = split_for(n); g.ws = m.ws;
-        if ((e = gemm(g, s)) != cudaSuccess) return e;
+    g = d;
+    g.K = kDOutPitch; g.KC = 32; g.kSlice = kDOutPitch; g.zp = m.z3; g.Hb = m.dz3; g.HT = m.dz3T;
+    if ((e = gemm_tc(mp.aDOut, mp.bW4T, g, s)) != cudaSuccess) return e;
+    // layers 3, 2: dW = dZ^T H_prev, db = colsum(dZ), dZ_prev
+    const CUtensorMap* aDzT[2] = {&mp.aDZ3T, &mp.aDZ2T};
+    const CUtensorMap* bHT[2] = {&mp.bH2T, &mp.bH1T};
+    const CUtensorMap* aDz[2] = {&mp.aDZ3, &mp.aDZ2};
+    const CUtensorMap* bWT[2] = {&mp.bW3T, &mp.bW2T};
+    const long long wOff[2] = {kW3, kW2}, bOff[2] = {kB3, kB2};
+    const float* zPrev[2] = {m.z2, m.z1};
+    bf16* dzPrev[2] = {m.dz2, nullptr};
+    bf16* dzPrevT[2] = {m.dz2T, m.dz1T};
+    for (int l = 0; l < 2; ++l) {
+        g = w;
+        g.M = kHid; g.N = kHid; g.BN = 128; g.Mv = kHid; g.Nv = kHid; g.C = G + wOff[l]; g.ldc = kHid;
+        if ((e = gemm_tc(*aDzT[l], *bHT[l], g, s)) != cudaSuccess) return e;
         if ((e = colsum(m.dz, n, kHid, kHid, G + bOff[l], s)) != cudaSuccess) return e;
-        if (l == 2) break;
-        g = gdesc();
-        g.A = dzb[l]; g.a_m = kHid; g.a_k = 1;
-        g.B = W + wOff[l]; g.b_k = kHid; g.b_n = 1;
-        g.M = n; g.N = kHid; g.K = kHid;
-        g.dz = zPrev[l]; g.ldz = kHid; g.C = m.dz; g.c_m = kHid; g.c_n = 1;
-        g.Cb = dzPrev[l]; g.ldCb = kHid;
-        if ((e = gemm(g, s)) != cudaSuccess) return e;
+        g = d;
+        g.K = kHid; g.KC = 64; g.kSlice = kHid; g.zp = zPrev[l]; g.Hb = dzPrev[l]; g.HT = dzPrevT[l];
+        if ((e = gemm_tc(*aDz[l], *bWT[l], g, s)) != cudaSuccess) return e;
     }
-    return cudaSuccess;
+    // layer 1: dW1 = dZ1^T X, db1
+    g = w;
+    g.M = kHid; g.N = kXPitch; g.BN = kXPitch; g.Mv = kHid; g.Nv = kIn; g.C = G + kW1; g.ldc = kIn;
+    if ((e = gemm_tc(mp.aDZ1T, mp.bXT, g, s)) != cudaSuccess) return e;
+    return colsum(m.dz, n, kHid, kHid, G + kB1, s);
 }
 
-template <class T>
-cudaError_t alloc(T** p, long long n)
+// Reads and clears the products' error flag (call after a synchronisation).
+cudaError_t gemm_status(Mlp& m)
 {
-    return cudaMalloc((void**)p, (size_t)(n > 0 ? n : 1) * sizeof(T));
+    int h = 0;
+    cudaError_t e = cudaMemcpy(&h, m.gemmErr, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && h) {
+        cudaMemset(m.gemmErr, 0, sizeof(int));
+        e = cudaErrorLaunchTimeout;
+    }
+    return e;
 }
 
 }  // namespace
@@ -634,22 +517,52 @@ cbf_status mlp_alloc(cbf_mlp* m, int B)
 {
     cudaError_t e = cudaSuccess;
     m->B = B;
-#define A_(ptr, n) if (e == cudaSuccess) e = alloc(&m->ptr, (n))
+    const long long Ba = std::max<long long>(4096, ((long long)B + kGtM - 1) / kGtM * kGtM);
+    m->Ba = Ba;
+#define A_(ptr, n) if (e == cudaSuccess) e = alloc_zero(&m->ptr, (n))
     A_(params, kNumParams); A_(grads, kNumParams); A_(m1, kNumParams); A_(m2, kNumParams);
-    A_(pb, kNumParams);
-    A_(xb, (long long)B * kIn); A_(yl, B); A_(yc, B);
-    A_(z1, (long long)B * kHid); A_(z2, (long long)B * kHid); A_(z3, (long long)B * kHid);
-    A_(h1, (long long)B * kHid); A_(h2, (long long)B * kHid); A_(h3, (long long)B * kHid);
-    A_(out, (long long)B * kOut); A_(dOut, (long long)B * kOut); A_(dOutB, (long long)B * kOut);
-    A_(dz, (long long)B * kHid); A_(dz3, (long long)B * kHid); A_(dz2, (long long)B * kHid);
-    A_(dz1, (long long)B * kHid);
-    A_(loss, 1); A_(step, 1);
+    A_(pb, kNumParams); A_(tw, kNumSlots * kSlot);
+    A_(xb, Ba * kXPitch); A_(xT, kXPitch * Ba); A_(yl, Ba); A_(yc, Ba);
+    A_(z1, Ba * kHid); A_(z2, Ba * kHid); A_(z3, Ba * kHid);
+    A_(h1, Ba * kHid); A_(h2, Ba * kHid); A_(h3, Ba * kHid);
+    A_(h1T, kHid * Ba); A_(h2T, kHid * Ba); A_(h3T, kHid * Ba);
+    A_(out, Ba * kOut); A_(dOut, Ba * kOut); A_(dOutB, Ba * kDOutPitch); A_(dOutT, kDOutTRows * Ba);
+    A_(dz, Ba * kHid); A_(dz3, Ba * kHid); A_(dz2, Ba * kHid);
+    A_(dz3T, kHid * Ba); A_(dz2T, kHid * Ba); A_(dz1T, kHid * Ba);
+    A_(loss, 1); A_(step, 1); A_(gemmErr, 1);
     A_(ws, (long long)kMaxSplit * kHid * kHid);
 #undef A_
     if (e != cudaSuccess) return report_cuda_error(e, "surrogate network buffers");
-    cudaMemset(m->m1, 0, kNumParams * sizeof(float));
-    cudaMemset(m->m2, 0, kNumParams * sizeof(float));
-    cudaMemset(m->step, 0, sizeof(unsigned long long));
+    m->maps = new TcMaps();
+    TcMaps& mp = *m->maps;
+    const auto slot = [&](int k) { return m->tw + k * kSlot; };
+#define M_(map, p, R, C, ld, rows, kc) if (e == cudaSuccess) e = operand_map(&mp.map, p, R, C, ld, rows, kc)
+    M_(aX, m->xb, Ba, kXPitch, kXPitch, kGtM, 16);
+    M_(aH1, m->h1, Ba, kHid, kHid, kGtM, 64);
+    M_(aH2, m->h2, Ba, kHid, kHid, kGtM, 64);
+    M_(aH3, m->h3, Ba, kHid, kHid, kGtM, 64);
+    M_(aDOut, m->dOutB, Ba, kDOutPitch, kDOutPitch, kGtM, 32);
+    M_(aDZ3, m->dz3, Ba, kHid, kHid, kGtM, 64);
+    M_(aDZ2, m->dz2, Ba, kHid, kHid, kGtM, 64);
+    M_(aDOutT, m->dOutT, kDOutTRows, Ba, Ba, kGtM, 64);
+    M_(aDZ3T, m->dz3T, kHid, Ba, Ba, kGtM, 64);
+    M_(aDZ2T, m->dz2T, kHid, Ba, Ba, kGtM, 64);
+    M_(aDZ1T, m->dz1T, kHid, Ba, Ba, kGtM, 64);
+    M_(bW1, slot(kSlotW1), kHid, kHid, kHid, 128, 16);
+    M_(bW2, slot(kSlotW2), kHid, kHid, kHid, 128, 64);
+    M_(bW3, slot(kSlotW3), kHid, kHid, kHid, 128, 64);
+    M_(bW4, slot(kSlotW4), kHid, kHid, kHid, 32, 64);
+    M_(bW4T, slot(kSlotW4T), kHid, kHid, kHid, 128, 32);
+    M_(bW3T, slot(kSlotW3T), kHid, kHid, kHid, 128, 64);
+    M_(bW2T, slot(kSlotW2T), kHid, kHid, kHid, 128, 64);
+    M_(bH3T, m->h3T, kHid, Ba, Ba, 128, 64);
+    M_(bH2T, m->h2T, kHid, Ba, Ba, 128, 64);
+    M_(bH1T, m->h1T, kHid, Ba, Ba, 128, 64);
+    M_(bXT, m->xT, kXPitch, Ba, Ba, kXPitch, 64);
+#undef M_
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGtMaxSmem);
+    if (e != cudaSuccess) return report_cuda_error(e, "surrogate network tensor maps");
     return CBF_OK;
 }
 
@@ -657,11 +570,13 @@ void mlp_free(cbf_mlp* m)
 {
     if (m->exec) cudaGraphExecDestroy(m->exec);
     if (m->graph) cudaGraphDestroy(m->graph);
-    void* ptrs[] = {m->params, m->grads, m->m1, m->m2, m->pb, m->xb, m->yl, m->yc, m->z1, m->z2,
-                    m->z3, m->h1, m->h2, m->h3, m->out, m->dOut, m->dOutB, m->dz, m->dz3,
-                    m->dz2, m->dz1, m->loss, m->ws, m->step, m->pxb, m->ph1, m->ph2, m->ph3, m->pout,
-                    m->wpack, m->tcErr};
+    void* ptrs[] = {m->params, m->grads, m->m1, m->m2, m->pb, m->tw, m->xb, m->xT, m->yl, m->yc, m->z1,
+                    m->z2, m->z3, m->h1, m->h2, m->h3, m->h1T, m->h2T, m->h3T, m->out, m->dOut, m->dOutB,
+                    m->dOutT, m->dz, m->dz3, m->dz2, m->dz3T, m->dz2T, m->dz1T, m->loss, m->ws, m->gemmErr,
+                    m->step, m->pxb, m->ph1, m->ph2, m->ph3, m->pout, m->wpack, m->tcErr};
     for (void* p : ptrs) cudaFree(p);
+    delete m->maps;
+    m->maps = nullptr;
 }
 
 // He-style uniform init from a fixed seed (host side, deterministic).
@@ -690,7 +605,7 @@ cbf_status upload_params(cbf_mlp* m, const float* host)
     cudaError_t e = cudaMemcpy(m->params, host, kNumParams * sizeof(float), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
         e = launch1d(kNumParams, 0, [&](unsigned b, int t) {
-            to_bf16_kernel<<<b, t>>>(m->params, m->pb, kNumParams);
+            expand_params_kernel<<<b, t>>>(m->params, m->pb, m->tw, kNumParams);
         });
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return report_cuda_error(e, "surrogate parameters");
@@ -757,19 +672,26 @@ cbf_status cbf_mlp_forward_backward(cbf_mlp* m, const float* hx, const float* hy
 {
     if (!m || !hx || !hyl || !hyc || n < 1 || n > m->B)
         return report_error(CBF_ERR_INVALID_ARG, "bad batch");
-    std::vector<bf16> xb((size_t)n * kIn);
-    for (long long i = 0; i < (long long)n * kIn; ++i) xb[i] = __float2bfloat16_rn(hx[i]);
+    // BF16 input rows (pitch 16) and their transpose, zero outside the n rows
+    const long long Ba = m->Ba;
+    std::vector<bf16> xb((size_t)Ba * kXPitch, __float2bfloat16_rn(0.0f)), xT((size_t)kXPitch * Ba, xb[0]);
+    for (long long r = 0; r < n; ++r)
+        for (int f = 0; f < kIn; ++f) xb[r * kXPitch + f] = xT[f * Ba + r] = __float2bfloat16_rn(hx[r * kIn + f]);
+    const int rows = (n + kGtM - 1) / kGtM * kGtM;
     cudaError_t e = cudaMemcpy(m->xb, xb.data(), xb.size() * sizeof(bf16), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(m->xT, xT.data(), xT.size() * sizeof(bf16), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(m->yl, hyl, (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(m->yc, hyc, (size_t)n * sizeof(int), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(m->loss, 0, sizeof(float));
-    if (e == cudaSuccess) e = forward(*m, n, m->xb, m->out, m->z1, m->z2, m->z3, m->h1, m->h2, m->h3, 0);
+    if (e == cudaSuccess) e = forward(*m, n, train_bufs(*m), 0);
     if (e == cudaSuccess)
-        e = launch1d(n, 0, [&](unsigned b, int t) {
-            loss_kernel<<<b, t>>>(m->out, m->yl, m->yc, n, wLle, m->dOut, m->dOutB, m->loss);
+        e = launch1d(rows, 0, [&](unsigned b, int t) {
+            loss_kernel<<<b, t>>>(m->out, m->yl, m->yc, n, rows, wLle, m->dOut, m->dOutB, m->dOutT, m->Ba,
+                                  m->loss);
         });
     if (e == cudaSuccess) e = backward(*m, n, 0);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = gemm_status(*m);
     if (e == cudaSuccess && hloss) e = cudaMemcpy(hloss, m->loss, sizeof(float), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess && hgrads)
         e = cudaMemcpy(hgrads, m->grads, kNumParams * sizeof(float), cudaMemcpyDeviceToHost);
@@ -802,17 +724,19 @@ cbf_status cbf_mlp_train(cbf_mlp* m, const float* dX, const float* dYl, const in
         if (e != cudaSuccess) return report_cuda_error(e, "begin capture of the training step");
         cudaError_t ce = launch1d(B, s, [&](unsigned b, int t) {
             gather_kernel<<<b, t, 0, s>>>(dX, dYl, (const int*)dYc, N, B, m->step, m->seed, m->xb,
-                                          m->yl, m->yc);
+                                          m->xT, m->Ba, m->yl, m->yc);
         });
-        if (ce == cudaSuccess) ce = forward(*m, B, m->xb, m->out, m->z1, m->z2, m->z3, m->h1, m->h2, m->h3, s);
+        const int rows = (B + kGtM - 1) / kGtM * kGtM;
+        if (ce == cudaSuccess) ce = forward(*m, B, train_bufs(*m), s);
         if (ce == cudaSuccess)
-            ce = launch1d(B, s, [&](unsigned b, int t) {
-                loss_kernel<<<b, t, 0, s>>>(m->out, m->yl, m->yc, B, wLle, m->dOut, m->dOutB, m->loss);
+            ce = launch1d(rows, s, [&](unsigned b, int t) {
+                loss_kernel<<<b, t, 0, s>>>(m->out, m->yl, m->yc, B, rows, wLle, m->dOut, m->dOutB, m->dOutT,
+                                            m->Ba, m->loss);
             });
         if (ce == cudaSuccess) ce = backward(*m, B, s);
         if (ce == cudaSuccess)
             ce = launch1d(kNumParams, s, [&](unsigned b, int t) {
-                adam_kernel<<<b, t, 0, s>>>(m->params, m->grads, m->m1, m->m2, m->pb, kNumParams, lr,
+                adam_kernel<<<b, t, 0, s>>>(m->params, m->grads, m->m1, m->m2, m->pb, m->tw, kNumParams, lr,
                                             horizon, 0.9f, 0.999f, 1e-8f, m->step);
             });
         if (ce == cudaSuccess) {
@@ -845,13 +769,15 @@ cbf_status cbf_mlp_train(cbf_mlp* m, const float* dX, const float* dYl, const in
             e = cudaMemcpyAsync(&hLosses[i], m->loss, sizeof(float), cudaMemcpyDeviceToHost, s);
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = gemm_status(*m);
     if (e != cudaSuccess) return report_cuda_error(e, "training");
     return CBF_OK;
 }
 
 // Predictions for N feature rows (device X [N x 4] FP32): LLE (de-normalised
-// with lleMean/lleStd), class, softmax confidence.  Runs in chunks of `batch`
-// rows through the training buffers.
+// with lleMean/lleStd), class, softmax confidence.  Runs in chunks of kPredRows
+// rows through its own workspace, then waits for the stream to read the
+// products' error flag.
 cbf_status cbf_mlp_predict(cbf_mlp* m, const float* dX, int64_t N, float lleMean, float lleStd,
                            float* dLle, int32_t* dCls, float* dConf, void* stream)
 {
@@ -861,17 +787,18 @@ cbf_status cbf_mlp_predict(cbf_mlp* m, const float* dX, int64_t N, float lleMean
     if ((e = pred_workspace(m)) != cudaSuccess) return report_cuda_error(e, "prediction workspace");
     for (long long r0 = 0; r0 < N && e == cudaSuccess; r0 += kPredRows) {
         const int n = (int)((N - r0) < kPredRows ? (N - r0) : kPredRows);
-        e = launch1d((long long)n * kIn, s, [&](unsigned b, int t) {
-            to_bf16_kernel<<<b, t, 0, s>>>(dX + r0 * kIn, m->pxb, (long long)n * kIn);
+        e = launch1d(n, s, [&](unsigned b, int t) {
+            rows_to_bf16_kernel<<<b, t, 0, s>>>(dX + r0 * kIn, n, m->pxb);
         });
-        if (e == cudaSuccess)
-            e = forward(*m, n, m->pxb, m->pout, nullptr, nullptr, nullptr, m->ph1, m->ph2, m->ph3, s);
+        if (e == cudaSuccess) e = forward(*m, n, pred_bufs(*m), s);
         if (e == cudaSuccess)
             e = launch1d(n, s, [&](unsigned b, int t) {
                 head_kernel<<<b, t, 0, s>>>(m->pout, n, lleMean, lleStd, dLle ? dLle + r0 : nullptr,
                                             dCls ? (int*)dCls + r0 : nullptr, dConf ? dConf + r0 : nullptr);
             });
     }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = gemm_status(*m);
     if (e != cudaSuccess) return report_cuda_error(e, "prediction");
     return CBF_OK;
 }

@@ -38,11 +38,14 @@ def test_mlp_init_matches_oracle(cbf, gpu_ok):
     assert np.array_equal(net.get_params().astype(np.float64), M.init_params(11))
 
 
-@pytest.mark.parametrize("n", [37, 1000])
+@pytest.mark.parametrize("n", [37, 1000, 4096, 9000])
 def test_mlp_gradients_match_oracle(cbf, gpu_ok, n):
-    """n=37: ragged tiles; n=1000: two split-K slices in the weight gradients."""
+    """Every product on tcgen05 against the oracle.  n=37: one ragged 128-row
+    tile; n=1000: four K slices in the weight gradients; n=4096 (the training
+    batch): sixteen; n=9000: sixteen slices of 576 rows, each run in three
+    passes of at most four 64-row chunks."""
     rng = np.random.default_rng(n)
-    net = cbf.Mlp(1024, seed=5)
+    net = cbf.Mlp(max(1024, n), seed=5)
     p = M.init_params(5)
     off = M.offsets()
     for b in ("b1", "b2", "b3", "b4"):
@@ -85,9 +88,9 @@ def test_mlp_predict_matches_forward(cbf, gpu_ok):
 
 @pytest.mark.parametrize("side,seed", [(37, 3), (256, 8)])
 def test_mlp_grid_prediction_tcgen05_matches_list_path(cbf, gpu_ok, side, seed):
-    """The fused tcgen05 grid kernel against the mma.sync GEMM path on the same
-    grid points and weights: the same BF16 rounding points, FP32 accumulation in
-    another order, so outputs agree to accumulation error (a rare BF16 rounding
+    """The fused tcgen05 grid kernel against the product kernel's forward pass
+    over explicit feature rows (cbf_mlp_predict) on the same grid points and
+    weights: the same BF16 rounding points, FP32 accumulation in another order, so outputs agree to accumulation error (a rare BF16 rounding
     flip of a hidden unit moves an output by ~1e-3), classes up to near-ties.
     side 37: a ragged last tile of 128 points."""
     torch = pytest.importorskip("torch")
