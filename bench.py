@@ -64,7 +64,8 @@ SUR_WORKLOAD = dict(WORKLOAD, nPts=8192, seedChunk=200000, maxAmountOfPeaks=512,
 FLOPS_PER_STEP = {"chen": 19, "lorenz": 19, "rossler": 17, "memristive5": 66}
 FP64_INSTR_PER_STEP = {"chen": 14, "lorenz": 14, "rossler": 10, "memristive5": 52}
 # the rescaled Chen/Lorenz step (systems.cuh QuadScaled: 4 MUL + 6 FMA)
-SCALED_FLOPS_PER_STEP, SCALED_INSTR_PER_STEP = 16, 10
+# the rescaled form: (flops, FP64 instructions) per step for s = 1/2 and for other s
+SCALED_COST = {2: (14, 8, "rescaled 8-instruction CD step (s = 1/2)"), 1: (15, 9, "rescaled 9-instruction CD step")}
 FP64_LANES_PER_SM = 64
 
 # The other measured configurations (printed as their own JSON lines with
@@ -304,13 +305,15 @@ class ClockSampler:
 
 def step_cost(cbf, job, system: str):
     """(flops, FP64 instructions, form) of one CD step of the job: the rescaled
-    Chen/Lorenz form (4 MUL + 6 FMA) where the job's grid admits it
-    (cbf_job_scaled_step), the 14-instruction forms otherwise."""
+    Chen/Lorenz form (6 FMA + 2 MUL at s = 1/2, one more MUL otherwise) where the
+    job's grid admits it (cbf_job_scaled_step), the 14-instruction forms
+    otherwise."""
     L = cbf.lib()
     L.cbf_job_scaled_step.restype = C.c_int32
     L.cbf_job_scaled_step.argtypes = [C.c_void_p]
-    if L.cbf_job_scaled_step(C.addressof(job)) == 1:
-        return SCALED_FLOPS_PER_STEP, SCALED_INSTR_PER_STEP, "rescaled 10-instruction CD step"
+    form = L.cbf_job_scaled_step(C.addressof(job))
+    if form in SCALED_COST:
+        return SCALED_COST[form]
     return FLOPS_PER_STEP[system], FP64_INSTR_PER_STEP[system], "reference-order CD step"
 
 

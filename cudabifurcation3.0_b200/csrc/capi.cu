@@ -172,14 +172,15 @@ void divergence_threshold(double M, int* active, double* T)
 
 namespace {
 
-// Whether every point of a Chen or Lorenz job can run the rescaled 10-instruction
-// step (systems.cuh, QuadScaled): s = values[0] not swept, and every value each
-// other parameter takes (the fixed value, or all nPts values of its swept axis,
-// whatever points the job selects) finite and within 2^64 in magnitude, with
-// A = values[1] (a or sigma) and the step's denominators 1 + h1 A, 1 - k B,
-// 1 + h1 B and the y-equation factors (Chen 1 + k c, 1 - h1 c; Lorenz 1 - k,
-// 1 + h1) at least 2^-64 in magnitude.  Every derived coefficient then lies far
-// inside the double range and sy is nonzero.  The oracle applies the same rule.
+// Whether every point of a Chen or Lorenz job can run the rescaled step
+// (systems.cuh, QuadScaled): s = values[0] not swept, k = h s at least 2^-64 in
+// magnitude, and every value each other parameter takes (the fixed value, or all
+// nPts values of its swept axis, whatever points the job selects) finite and
+// within 2^64 in magnitude, with A = values[1] (a or sigma) and the step's
+// denominators 1 + h1 A, 1 - k B, 1 + h1 B and the y-equation factors (Chen
+// 1 + k c, 1 - h1 c; Lorenz 1 - k, 1 + h1) at least 2^-64 in magnitude.  Every
+// derived coefficient then lies far inside the double range and sy, sz are
+// nonzero.  The oracle applies the same rule.
 bool scaled_step_ok(const cbf_job* j)
 {
     const bool chen = j->system == CBF_SYS_CHEN, lorenz = j->system == CBF_SYS_LORENZ;
@@ -196,6 +197,7 @@ bool scaled_step_ok(const cbf_job* j)
     const double h = j->h, s = j->values[0];
     if (!(fin(h) && away(h) && fin(s))) return false;
     const double k = h * s, h1 = h * (1.0 - s);
+    if (!away(k)) return false;
     if (lorenz && !(away(1.0 - k) && away(1.0 + h1))) return false;
     for (int slot = 1; slot <= 3; ++slot) {
         const int ax = sweptAxis[slot];
@@ -260,6 +262,7 @@ cbf_status lower_job(const cbf_job* j, DevJob* d)
     d->system = j->system;
     d->sweepIC = j->sweepIC ? 1 : 0;
     d->scaledStep = scaled_step_ok(j) ? 1 : 0;
+    d->unitStep = d->scaledStep && j->h * j->values[0] == j->h * (1.0 - j->values[0]);
     d->dims = j->dims;
     d->nPts = j->nPts;
     d->nIC = j->nIC;
@@ -666,7 +669,7 @@ int32_t cbf_job_scaled_step(const cbf_job* job)
 {
     DevJob d;
     if (lower_job(job, &d) != CBF_OK) return -1;
-    return d.scaledStep;
+    return d.scaledStep ? (d.unitStep ? 2 : 1) : 0;
 }
 
 cbf_status cbf_run(const cbf_job* job, void* d_out, void* d_aux, void* stream)

@@ -50,7 +50,8 @@ struct DevJob {
     int task;
     int system;
     int sweepIC;
-    int scaledStep;     // Chen/Lorenz: the 10-instruction rescaled step (systems.cuh) for this job
+    int scaledStep;     // Chen/Lorenz: the rescaled step (systems.cuh, QuadScaled) for this job
+    int unitStep;       // ... with k = h1 (s = 1/2): its 8-instruction form
 };
 
 // Grid index of the job's k-th point: an explicit list, or a contiguous range.

@@ -159,8 +159,8 @@ cudaError_t launch_lle_variant(const DevJob& J, double* d_out, cudaStream_t s, i
     switch (J.system) {
     case CBF_SYS_MEMRISTIVE5: return launch_lle_s<Memristive5>(J, d_out, s, variant);
     case CBF_SYS_ROSSLER: return launch_lle_s<Rossler>(J, d_out, s, variant);
-    case CBF_SYS_LORENZ: return J.scaledStep ? launch_lle_s<LorenzScaled>(J, d_out, s, variant) : launch_lle_s<Lorenz>(J, d_out, s, variant);
-    case CBF_SYS_CHEN: return J.scaledStep ? launch_lle_s<ChenScaled>(J, d_out, s, variant) : launch_lle_s<Chen>(J, d_out, s, variant);
+    case CBF_SYS_LORENZ: return J.scaledStep ? (J.unitStep ? launch_lle_s<LorenzScaledU>(J, d_out, s, variant) : launch_lle_s<LorenzScaled>(J, d_out, s, variant)) : launch_lle_s<Lorenz>(J, d_out, s, variant);
+    case CBF_SYS_CHEN: return J.scaledStep ? (J.unitStep ? launch_lle_s<ChenScaledU>(J, d_out, s, variant) : launch_lle_s<ChenScaled>(J, d_out, s, variant)) : launch_lle_s<Chen>(J, d_out, s, variant);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -296,8 +296,8 @@ long long lle_regime_resident_points(const DevJob& J)
     switch (J.system) {
     case CBF_SYS_MEMRISTIVE5: return resident_s<Memristive5>(J);
     case CBF_SYS_ROSSLER: return resident_s<Rossler>(J);
-    case CBF_SYS_LORENZ: return J.scaledStep ? resident_s<LorenzScaled>(J) : resident_s<Lorenz>(J);
-    case CBF_SYS_CHEN: return J.scaledStep ? resident_s<ChenScaled>(J) : resident_s<Chen>(J);
+    case CBF_SYS_LORENZ: return J.scaledStep ? (J.unitStep ? resident_s<LorenzScaledU>(J) : resident_s<LorenzScaled>(J)) : resident_s<Lorenz>(J);
+    case CBF_SYS_CHEN: return J.scaledStep ? (J.unitStep ? resident_s<ChenScaledU>(J) : resident_s<ChenScaled>(J)) : resident_s<Chen>(J);
     default: return 0;
     }
 }
@@ -307,8 +307,8 @@ cudaError_t launch_lle_regime(const DevJob& J, double* d_lle, int* d_cls, cudaSt
     switch (J.system) {
     case CBF_SYS_MEMRISTIVE5: return launch_s<Memristive5>(J, d_lle, d_cls, s);
     case CBF_SYS_ROSSLER: return launch_s<Rossler>(J, d_lle, d_cls, s);
-    case CBF_SYS_LORENZ: return J.scaledStep ? launch_s<LorenzScaled>(J, d_lle, d_cls, s) : launch_s<Lorenz>(J, d_lle, d_cls, s);
-    case CBF_SYS_CHEN: return J.scaledStep ? launch_s<ChenScaled>(J, d_lle, d_cls, s) : launch_s<Chen>(J, d_lle, d_cls, s);
+    case CBF_SYS_LORENZ: return J.scaledStep ? (J.unitStep ? launch_s<LorenzScaledU>(J, d_lle, d_cls, s) : launch_s<LorenzScaled>(J, d_lle, d_cls, s)) : launch_s<Lorenz>(J, d_lle, d_cls, s);
+    case CBF_SYS_CHEN: return J.scaledStep ? (J.unitStep ? launch_s<ChenScaledU>(J, d_lle, d_cls, s) : launch_s<ChenScaled>(J, d_lle, d_cls, s)) : launch_s<Chen>(J, d_lle, d_cls, s);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -326,10 +326,10 @@ cudaError_t launch_lle_regime_list(const DevJob& J, const long long* nDev, long 
     switch (J.system) {
     case CBF_SYS_ROSSLER: return launch_list_s<Rossler>(J, nDev, maxPoints, d_lle, d_cls, scratch, scratchBytes, err, s);
     case CBF_SYS_LORENZ:
-        return J.scaledStep ? launch_list_s<LorenzScaled>(J, nDev, maxPoints, d_lle, d_cls, scratch, scratchBytes, err, s)
+        return J.scaledStep ? (J.unitStep ? launch_list_s<LorenzScaledU>(J, nDev, maxPoints, d_lle, d_cls, scratch, scratchBytes, err, s) : launch_list_s<LorenzScaled>(J, nDev, maxPoints, d_lle, d_cls, scratch, scratchBytes, err, s))
                             : launch_list_s<Lorenz>(J, nDev, maxPoints, d_lle, d_cls, scratch, scratchBytes, err, s);
     case CBF_SYS_CHEN:
-        return J.scaledStep ? launch_list_s<ChenScaled>(J, nDev, maxPoints, d_lle, d_cls, scratch, scratchBytes, err, s)
+        return J.scaledStep ? (J.unitStep ? launch_list_s<ChenScaledU>(J, nDev, maxPoints, d_lle, d_cls, scratch, scratchBytes, err, s) : launch_list_s<ChenScaled>(J, nDev, maxPoints, d_lle, d_cls, scratch, scratchBytes, err, s))
                             : launch_list_s<Chen>(J, nDev, maxPoints, d_lle, d_cls, scratch, scratchBytes, err, s);
     default: return cudaErrorInvalidValue;
     }

@@ -211,35 +211,40 @@ struct Lorenz {
 };
 
 // ---------------------------------------------------------------------------
-// Chen and Lorenz in a rescaled state: 10 FP64 instructions per step (4 MUL,
-// 6 FMA; 16 flops) instead of 14.
+// Chen and Lorenz in a rescaled state: 8 FP64 instructions per step (6 FMA,
+// 2 MUL; 14 flops) when s = 1/2, 9 otherwise, instead of 14.
 //
 // Written out, both CD steps read (A = a or sigma, B = b or beta)
 //   z1 = (1 - kB) z + k x y,  w = W0 - z1,  y1 = cy y + k x w,
 //   x2 = r1 (1 - kA) x + r1 A h y1,  y2 = r2 (y1 + h1 x2 w),  z2 = r3 (z1 + h1 x2 y2),
 // r1 = 1/(1 + h1 A), r3 = 1/(1 + h1 B); Chen: W0 = c - a, cy = 1 + k c,
 // r2 = 1/(1 - h1 c); Lorenz: W0 = rho, cy = 1 - k, r2 = 1/(1 + h1).
-// Every parameter factor that the 14-instruction form applies with a MUL can be
-// folded into an FMA operand by measuring y, and the intermediates z1, w, y1, in
-// suitable units: y is stored as Y = sy*y with sy = ups*cy, ups = r1 A h (x and z
-// stay in physical units), and with om = 1 - kB, th = ups*sy*om
-//   p = k1 x;  Z1 = fma(p, Y, z) = z1/om;  W = fma(al, Z1, be) = th w;
-//   Y1 = fma(p, W, Y) = ups y1;  x2 = fma(rho, x, Y1);  q = k2 x2;
-//   Y2 = ly fma(q, W, Y1) = sy y2;  z2 = lz fma(q, Y2, Z1),
-// k1 = k/(om sy), k2 = h1/(om sy), al = -th om, be = th W0, rho = r1 (1 - kA),
-// ly = cy r2, lz = om r3.  The mathematics is the CD step; the rounding is this
+// Measuring y and z, and the intermediates, in suitable units turns every
+// parameter factor of the quadratic terms into 1: with ups = r1 A h, om = 1 - kB,
+// the state is stored as (x, Y, Z) = (x, sy y, sz z), sy = ups cy, sz = om sy / k,
+// and one step is
+//   Z1 = fma(x, Y, Z) = (sy/k) z1;   W = fma(al, Z1, be) = ups k w;
+//   Y1 = fma(x, W, Y) = (sy/cy) y1;  x2 = fma(rho, x, Y1);
+//   q = c5 x2;  Y2 = ly fma(q, W, Y1) = sy y2;  Z2 = lz fma(q, Y2, Z1) = sz z2,
+// al = -(ups k)(k/sy), be = (ups k) W0, rho = r1 (1 - kA), c5 = h1/k, ly = cy r2,
+// lz = om r3.  The two multiplications by ly and lz are the per-step decay of
+// the linear parts of y and z, which no constant change of units removes; c5 is
+// exactly 1 when k = h1 (s = 1/2), and the UNIT form then skips that product --
+// a multiplication by 1.0 is exact, so both forms give identical results and the
+// oracle always multiplies.  The mathematics is the CD step; the rounding is this
 // form's own, and the oracle evaluates the same operations.  The form needs
-// A != 0 (else sy = 0) and factors well inside the double range; a job whose
-// every point qualifies runs it (capi.cu: scaled_step_ok), others the
-// 14-instruction form.  Outputs read y as Y * (1/sy) (phys_comp); LLE and
-// Lyapunov-spectrum distances are taken in physical units.
-template <bool LORENZ>
+// A != 0 and k != 0 (else sy or sz is 0 or undefined) and factors well inside
+// the double range; a job whose every point qualifies runs it (capi.cu:
+// scaled_step_ok), others the 14-instruction form.  Outputs read y and z as
+// Y * (1/sy), Z * (1/sz) (phys_comp); LLE and Lyapunov-spectrum distances are
+// taken in physical units.
+template <bool LORENZ, bool UNIT>
 struct QuadScaled {
     static constexpr int DIM = 3;
     static constexpr int NV = 4;
-    static constexpr int FLOPS = 16;
+    static constexpr int FLOPS = UNIT ? 14 : 15;
     static constexpr bool SCALED = true;
-    struct Coef { double k1, al, be, rho, k2, ly, lz, sy, iy; };
+    struct Coef { double al, be, rho, c5, ly, lz, sy, iy, sz, iz; };
     __host__ __device__ static Coef prep(const double* v, double h)
     {
         Coef q;
@@ -256,46 +261,48 @@ struct QuadScaled {
         const double ups = (r1 * A) * h;
         const double om = 1.0 - k * B;
         q.sy = ups * cy;
-        const double th = (ups * q.sy) * om;
-        const double osy = om * q.sy;
-        q.k1 = k / osy;
-        q.k2 = h1 / osy;
-        q.al = -(th * om);
-        q.be = th * W0;
+        q.sz = (om * q.sy) / k;
+        const double uk = ups * k;
+        q.al = -(uk * (k / q.sy));
+        q.be = uk * W0;
         q.rho = r1 * (1.0 - k * A);
+        q.c5 = h1 / k;
         q.ly = cy * r2;
         q.lz = om * r3;
         q.iy = 1.0 / q.sy;
+        q.iz = 1.0 / q.sz;
         return q;
     }
     __device__ __forceinline__ static void step(double* X, const Coef& q)
     {
         const double x = X[0], y = X[1], z = X[2];
-        const double p = q.k1 * x;
-        const double z1 = fma(p, y, z);
+        const double z1 = fma(x, y, z);
         const double w = fma(q.al, z1, q.be);
-        const double y1 = fma(p, w, y);
+        const double y1 = fma(x, w, y);
         const double x2 = fma(q.rho, x, y1);
-        const double qq = q.k2 * x2;
+        const double qq = UNIT ? x2 : q.c5 * x2;
         const double y2 = q.ly * fma(qq, w, y1);
         const double z2 = q.lz * fma(qq, y2, z1);
         X[0] = x2; X[1] = y2; X[2] = z2;
     }
 };
-using ChenScaled = QuadScaled<false>;
-using LorenzScaled = QuadScaled<true>;
+using ChenScaled = QuadScaled<false, false>;
+using LorenzScaled = QuadScaled<true, false>;
+using ChenScaledU = QuadScaled<false, true>;    // s = 1/2
+using LorenzScaledU = QuadScaled<true, true>;  // s = 1/2
 
 // ---------------------------------------------------------------------------
 // Physical view of a stored state.  Systems with SCALED keep component 1 in
-// units of Coef::sy; every other component, and every component of the other
-// systems, is stored in physical units (the conversions compile away).
+// units of Coef::sy and component 2 in units of Coef::sz; component 0, and every
+// component of the other systems, is stored in physical units (the conversions
+// compile away).
 
 // Component i (a compile-time index after unrolling) of a state difference or
 // value, from stored to physical units.
 template <class S>
 __host__ __device__ __forceinline__ double phys_comp(double v, int i, const typename S::Coef& c)
 {
-    if constexpr (S::SCALED) return i == 1 ? v * c.iy : v;
+    if constexpr (S::SCALED) return i == 1 ? v * c.iy : (i == 2 ? v * c.iz : v);
     else return v;
 }
 
@@ -303,7 +310,7 @@ __host__ __device__ __forceinline__ double phys_comp(double v, int i, const type
 template <class S>
 __host__ __device__ __forceinline__ double stored_comp(double v, int i, const typename S::Coef& c)
 {
-    if constexpr (S::SCALED) return i == 1 ? v * c.sy : v;
+    if constexpr (S::SCALED) return i == 1 ? v * c.sy : (i == 2 ? v * c.sz : v);
     else return v;
 }
 
@@ -311,7 +318,10 @@ __host__ __device__ __forceinline__ double stored_comp(double v, int i, const ty
 template <class S>
 __host__ __device__ __forceinline__ void to_stored(double* x, const typename S::Coef& c)
 {
-    if constexpr (S::SCALED) x[1] = x[1] * c.sy;
+    if constexpr (S::SCALED) {
+        x[1] = x[1] * c.sy;
+        x[2] = x[2] * c.sz;
+    }
 }
 
 }  // namespace cbf

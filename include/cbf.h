@@ -135,11 +135,13 @@ int32_t cbf_record_length(const cbf_job* job);   /* (int)(tMax/h/preScaller) or 
 int32_t cbf_peak_capacity(const cbf_job* job);   /* peaks a PEAKS row can hold = record/2 */
 int64_t cbf_job_points(const cbf_job* job);      /* nPoints, or nPts^dims when 0 */
 cbf_status cbf_validate(const cbf_job* job);
-/* 1 when the job's Chen or Lorenz steps use the rescaled 10-instruction form (y
- * stored in units of a per-point constant, 4 MUL + 6 FMA per step), 0 for the
- * 14-instruction form (other systems, s swept, A = 0, or factors near 0 or
- * beyond 2^64), -1 for an invalid job.  Both are the same CD step; each has its
- * own rounding, and the CPU oracle follows the one the job uses. */
+/* 2 when the job's Chen or Lorenz steps use the rescaled form with s = 1/2 (y and
+ * z stored in units of per-point constants; 6 FMA + 2 MUL per step), 1 for the
+ * rescaled form with another s (one more MUL), 0 for the 14-instruction form
+ * (other systems, s swept or 0, A = 0, or factors near 0 or beyond 2^64), -1 for
+ * an invalid job.  All are the same CD step; each form has its own rounding
+ * (forms 2 and 1 round identically), and the CPU oracle follows the one the job
+ * uses. */
 int32_t cbf_job_scaled_step(const cbf_job* job);
 
 /* ---- device-resident interface --------------------------------------- */

@@ -158,15 +158,17 @@ static void step_lorenz(double* X, const double* v, double h)
     X[0] = x2; X[1] = y2; X[2] = z2;
 }
 
-/* The library's rescaled Chen / Lorenz step (10 FP64 operations), for the jobs
- * orc_scaled_step admits.  The state's y is stored as Y = sy * y; x and z are
- * physical.  With A = a or sigma, B = b or beta, om = 1 - k B, ups = r1 A h,
- * sy = ups cy, th = ups sy om, the CD step becomes
- *   p = k1 x;  Z1 = fma(p, Y, z);  W = fma(al, Z1, be);  Y1 = fma(p, W, Y);
- *   x2 = fma(rho, x, Y1);  q = k2 x2;  Y2 = ly fma(q, W, Y1);  z2 = lz fma(q, Y2, Z1)
- * (coefficients below, in the kernels' operation order). */
+/* The library's rescaled Chen / Lorenz step (systems.cuh, QuadScaled: 8 FP64
+ * operations when s = 1/2, where c5 = 1, else 9), for the jobs orc_scaled_step
+ * admits.  The state is stored as (x, Y, Z) = (x, sy y, sz z).  With A = a or
+ * sigma, B = b or beta, om = 1 - k B, ups = r1 A h, sy = ups cy, sz = om sy / k,
+ * the CD step becomes
+ *   Z1 = fma(x, Y, Z);  W = fma(al, Z1, be);  Y1 = fma(x, W, Y);  x2 = fma(rho, x, Y1);
+ *   q = c5 x2;  Y2 = ly fma(q, W, Y1);  Z2 = lz fma(q, Y2, Z1)
+ * (coefficients below, in the kernels' operation order; the kernels skip the
+ * product c5 x2 when c5 = 1, which changes nothing). */
 typedef struct {
-    double k1, al, be, rho, k2, ly, lz, sy, iy;
+    double al, be, rho, c5, ly, lz, sy, iy, sz, iz;
 } scaled_coef;
 
 static void scaled_coef_of(int lorenz, const double* v, double h, scaled_coef* q)
@@ -184,16 +186,16 @@ static void scaled_coef_of(int lorenz, const double* v, double h, scaled_coef* q
     const double ups = (r1 * A) * h;
     const double om = 1.0 - k * B;
     q->sy = ups * cy;
-    const double th = (ups * q->sy) * om;
-    const double osy = om * q->sy;
-    q->k1 = k / osy;
-    q->k2 = h1 / osy;
-    q->al = -(th * om);
-    q->be = th * W0;
+    q->sz = (om * q->sy) / k;
+    const double uk = ups * k;
+    q->al = -(uk * (k / q->sy));
+    q->be = uk * W0;
     q->rho = r1 * (1.0 - k * A);
+    q->c5 = h1 / k;
     q->ly = cy * r2;
     q->lz = om * r3;
     q->iy = 1.0 / q->sy;
+    q->iz = 1.0 / q->sz;
 }
 
 static void step_quad_scaled(int lorenz, double* X, const double* v, double h)
@@ -201,12 +203,11 @@ static void step_quad_scaled(int lorenz, double* X, const double* v, double h)
     scaled_coef q;
     scaled_coef_of(lorenz, v, h, &q);
     const double x = X[0], y = X[1], z = X[2];
-    const double p = q.k1 * x;
-    const double z1 = fma(p, y, z);
+    const double z1 = fma(x, y, z);
     const double w = fma(q.al, z1, q.be);
-    const double y1 = fma(p, w, y);
+    const double y1 = fma(x, w, y);
     const double x2 = fma(q.rho, x, y1);
-    const double qq = q.k2 * x2;
+    const double qq = q.c5 * x2;
     const double y2 = q.ly * fma(qq, w, y1);
     const double z2 = q.lz * fma(qq, y2, z1);
     X[0] = x2; X[1] = y2; X[2] = z2;
@@ -241,28 +242,49 @@ void orc_model_step(int system, double* x, const double* a, double h)
     }
 }
 
-/* 1/sy of a rescaled system (the factor that turns a stored y into a physical
- * one), 1 for the others. */
-static double y_phys_factor(int system, const double* v, double h)
+/* Units of a stored state: component i is stored as (physical * s[i]) and read
+ * back as (stored * is[i]); every factor is 1 except y (sy, 1/sy) and z (sz,
+ * 1/sz) of a rescaled system.  A multiplication by 1 is exact, so the unscaled
+ * systems see their values unchanged. */
+typedef struct {
+    double s[8], is[8];
+} state_units;
+
+static state_units units_of(int system, const double* v, double h)
 {
-    if (!is_scaled(system))
-        return 1.0;
-    scaled_coef q;
-    scaled_coef_of((system & ~ORC_SCALED) == ORC_SYS_LORENZ, v, h, &q);
-    return q.iy;
+    state_units u;
+    for (int i = 0; i < 8; ++i)
+        u.s[i] = u.is[i] = 1.0;
+    if (is_scaled(system)) {
+        scaled_coef q;
+        scaled_coef_of((system & ~ORC_SCALED) == ORC_SYS_LORENZ, v, h, &q);
+        u.s[1] = q.sy;
+        u.is[1] = q.iy;
+        u.s[2] = q.sz;
+        u.is[2] = q.iz;
+    }
+    return u;
 }
 
-/* Stored component i -> physical (multiplied by 1/sy for y of a rescaled system). */
-static double to_phys(int system, double value, int i, double iy)
+/* Stored component i -> physical. */
+static double to_phys(double value, int i, const state_units* u)
 {
-    return (is_scaled(system) && i == 1) ? value * iy : value;
+    return value * u->is[i];
+}
+
+/* A physical quantity (initial value or perturbation) of component i -> stored. */
+static double to_stored(double value, int i, const state_units* u)
+{
+    return value * u->s[i];
 }
 
 /* Whether a Chen / Lorenz job runs the rescaled step (the library's
- * scaled_step_ok, capi.cu): s not swept; every value of a, b, c (sigma, rho,
- * beta) the job's grid holds finite and within 2^64; A = values[1] and the
- * factors 1 + h1 A, 1 - k B, 1 + h1 B, Chen 1 + k c, 1 - h1 c, Lorenz 1 - k,
- * 1 + h1 at least 2^-64 in magnitude. */
+ * scaled_step_ok, capi.cu): s not swept; k = h s at least 2^-64 in magnitude;
+ * every value of a, b, c (sigma, rho, beta) the job's grid holds finite and
+ * within 2^64; A = values[1] and the factors 1 + h1 A, 1 - k B, 1 + h1 B, Chen
+ * 1 + k c, 1 - h1 c, Lorenz 1 - k, 1 + h1 at least 2^-64 in magnitude.  Returns
+ * 2 when k = h1 (s = 1/2: the library's 8-instruction form), 1 for the other
+ * rescaled jobs, 0 otherwise (cbf_job_scaled_step). */
 static int fin64(double v) { return isfinite(v) && fabs(v) <= 0x1p64; }
 static int away64(double v) { return isfinite(v) && fabs(v) >= 0x1p-64; }
 
@@ -284,6 +306,8 @@ int orc_scaled_step(const orc_job* job)
     if (!(fin64(h) && away64(h) && fin64(s)))
         return 0;
     const double k = h * s, h1 = h * (1.0 - s);
+    if (!away64(k))
+        return 0;
     if (lorenz && !(away64(1.0 - k) && away64(1.0 + h1)))
         return 0;
     for (int slot = 1; slot <= 3; ++slot) {
@@ -309,7 +333,7 @@ int orc_scaled_step(const orc_job* job)
                 return 0;
         }
     }
-    return 1;
+    return k == h1 ? 2 : 1;
 }
 
 /* `if (maxValue != 0) if (fabsf(x[writableVar]) > maxValue)`: fabsf rounds the
@@ -325,16 +349,16 @@ int orc_loop(int system, double* x, const double* values, double h, int amountOf
              int preScaller, int writableVar, double maxValue, double* data,
              int64_t startDataIndex, int writeStep)
 {
-    /* x[writableVar] in physical units (a rescaled system stores y times sy) */
-    const double iy = y_phys_factor(system, values, h);
+    /* x[writableVar] in physical units (a rescaled system stores y and z scaled) */
+    const state_units u = units_of(system, values, h);
     for (int i = 0; i < amountOfIterations; ++i) {
         if (data != NULL)
-            data[startDataIndex + (int64_t)i * writeStep] = to_phys(system, x[writableVar], writableVar, iy);
+            data[startDataIndex + (int64_t)i * writeStep] = to_phys(x[writableVar], writableVar, &u);
         for (int j = 0; j < preScaller - 1; ++j)
             orc_model_step(system, x, values, h);
         orc_model_step(system, x, values, h);
         if (maxValue != 0)
-            if ((double)fabsf((float)to_phys(system, x[writableVar], writableVar, iy)) > maxValue)
+            if ((double)fabsf((float)to_phys(x[writableVar], writableVar, &u)) > maxValue)
                 return 0;
     }
     return 1;
@@ -550,18 +574,17 @@ static void setup_point(const orc_job* job, int64_t g, double* x, double* v)
 
 /* setup_point, then the state converted to the units the job's step uses; returns
  * the system id the loops integrate (a rescaled form where the job admits it) and
- * sets *sy (1 for unscaled systems). */
-static int setup_state(const orc_job* job, int64_t g, double* x, double* v, double* sy)
+ * sets *u to its units. */
+static int setup_state(const orc_job* job, int64_t g, double* x, double* v, state_units* u)
 {
     setup_point(job, g, x, v);
-    *sy = 1.0;
-    if (!orc_scaled_step(job))
-        return job->system;
-    scaled_coef q;
-    scaled_coef_of(job->system == ORC_SYS_LORENZ, v, job->h, &q);
-    x[1] = x[1] * q.sy;
-    *sy = q.sy;
-    return job->system | ORC_SCALED;
+    const int sys = orc_scaled_step(job) ? (job->system | ORC_SCALED) : job->system;
+    *u = units_of(sys, v, job->h);
+    if (is_scaled(sys)) {
+        x[1] = x[1] * u->s[1];
+        x[2] = x[2] * u->s[2];
+    }
+    return sys;
 }
 
 /* The regime window of the LLE + regime point: x[recVar] (physical) recorded
@@ -571,9 +594,9 @@ static int setup_state(const orc_job* job, int64_t g, double* x, double* v, doub
 static int loop_window(int system, double* x, const double* values, double h, int n, int recVar,
                        double maxValue, double* data)
 {
-    const double iy = y_phys_factor(system, values, h);
+    const state_units u = units_of(system, values, h);
     for (int i = 0; i < n; ++i) {
-        data[i] = to_phys(system, x[recVar], recVar, iy);
+        data[i] = to_phys(x[recVar], recVar, &u);
         orc_model_step(system, x, values, h);
         if (maxValue != 0 && (double)fabsf((float)x[0]) > maxValue)
             return 0;
@@ -581,18 +604,13 @@ static int loop_window(int system, double* x, const double* values, double h, in
     return 1;
 }
 
-/* A physical perturbation component in stored units. */
-static double to_stored(int system, double value, int i, double sy)
-{
-    return (is_scaled(system) && i == 1) ? value * sy : value;
-}
-
 /* cudaLibrary.cu:107-114 (and :194-201): unchecked transient, then the recorded
  * loop with the divergence check on x[writableVar]. */
 int orc_trajectory_point(const orc_job* job, int64_t g, double* data)
 {
-    double x[8], v[16], sy;
-    const int sys = setup_state(job, g, x, v, &sy);
+    double x[8], v[16];
+    state_units u;
+    const int sys = setup_state(job, g, x, v, &u);
     orc_loop(sys, x, v, job->h, orc_skip_len(job), 1, 0, 0, NULL, 0, 1);
     int ok = orc_loop(sys, x, v, job->h, orc_record_len(job), job->preScaller,
                       job->writableVar, job->maxValue, data, 0, 1);
@@ -633,8 +651,9 @@ double orc_lle_point(const orc_job* job, int64_t g)
 /* zIn: the normalised perturbation to start from (NULL: orc_lle_seed). */
 double orc_lle_point_seeded(const orc_job* job, int64_t g, const double* zIn)
 {
-    double x[8], y[8], z[8], v[16], sy;
-    const int sys = setup_state(job, g, x, v, &sy);
+    double x[8], y[8], z[8], v[16];
+    state_units u;
+    const int sys = setup_state(job, g, x, v, &u);
 
     const int nIC = job->nIC;
     if (zIn) {
@@ -649,13 +668,12 @@ double orc_lle_point_seeded(const orc_job* job, int64_t g, const double* zIn)
     const int nNT = (int)(size_t)(job->NT / h);
     const int sizeOfBlock = (int)(job->tMax / job->NT);
     const double eps = job->lleEps;
-    const double iy = y_phys_factor(sys, v, h);
 
     orc_loop(sys, x, v, h, skip, 1, 0, job->maxValue, NULL, 0, 1);
 
     /* the perturbation in physical units; distances measured in physical units */
     for (int i = 0; i < nIC; ++i)
-        y[i] = to_stored(sys, z[i] * eps, i, sy) + x[i];
+        y[i] = to_stored(z[i] * eps, i, &u) + x[i];
 
     double result = 0;
     for (int i = 0; i < sizeOfBlock; ++i) {
@@ -664,7 +682,7 @@ double orc_lle_point_seeded(const orc_job* job, int64_t g, const double* zIn)
 
         double tempData = 0;
         for (int l = 0; l < nIC; ++l) {
-            const double d = to_phys(sys, x[l] - y[l], l, iy);
+            const double d = to_phys(x[l] - y[l], l, &u);
             tempData += d * d;
         }
         tempData = sqrt(tempData) / eps;
@@ -682,8 +700,9 @@ double orc_lle_point_seeded(const orc_job* job, int64_t g, const double* zIn)
 
 double orc_lle_regime_point(const orc_job* job, int64_t g, const double* zIn, int32_t* cls)
 {
-    double x[8], y[8], z[8], v[16], sy;
-    const int sys = setup_state(job, g, x, v, &sy);
+    double x[8], y[8], z[8], v[16];
+    state_units u;
+    const int sys = setup_state(job, g, x, v, &u);
     const int nIC = job->nIC;
     if (zIn) {
         for (int i = 0; i < nIC; ++i)
@@ -692,7 +711,6 @@ double orc_lle_regime_point(const orc_job* job, int64_t g, const double* zIn, in
         orc_lle_seed(job, g, z);
     }
     const double h = job->h;
-    const double iy = y_phys_factor(sys, v, h);
     const int nNT = (int)(size_t)(job->NT / h);
     const int sizeOfBlock = (int)(job->tMax / job->NT);
     const double eps = job->lleEps;
@@ -704,7 +722,7 @@ double orc_lle_regime_point(const orc_job* job, int64_t g, const double* zIn, in
 
     orc_loop(sys, x, v, h, orc_skip_len(job), 1, 0, job->maxValue, NULL, 0, 1);
     for (int i = 0; i < nIC; ++i)
-        y[i] = to_stored(sys, z[i] * eps, i, sy) + x[i];
+        y[i] = to_stored(z[i] * eps, i, &u) + x[i];
 
     double result = 0;
     int t = 0;
@@ -726,7 +744,7 @@ double orc_lle_regime_point(const orc_job* job, int64_t g, const double* zIn, in
 
         double tempData = 0;
         for (int l = 0; l < nIC; ++l) {
-            const double d = to_phys(sys, x[l] - y[l], l, iy);
+            const double d = to_phys(x[l] - y[l], l, &u);
             tempData += d * d;
         }
         tempData = sqrt(tempData) / eps;
@@ -1088,9 +1106,10 @@ void orc_ls_seed(const orc_job* job, int64_t g, double* z)
  * optional) replaces the seed rows. */
 void orc_ls_point(const orc_job* job, int64_t g, const double* zIn, double* out)
 {
-    double x[8], y[64], z[64], v[16], den[8], result[8], sy;
+    double x[8], y[64], z[64], v[16], den[8], result[8];
     const int n = job->nIC;
-    const int sys = setup_state(job, g, x, v, &sy);
+    state_units u;
+    const int sys = setup_state(job, g, x, v, &u);
     if (zIn) {
         for (int i = 0; i < n * n; ++i)
             z[i] = zIn[i];
@@ -1101,7 +1120,6 @@ void orc_ls_point(const orc_job* job, int64_t g, const double* zIn, double* out)
     const int nNT = (int)(size_t)(job->NT / h);
     const int sizeOfBlock = (int)(job->tMax / job->NT);
     const double eps = job->lleEps;
-    const double iy = y_phys_factor(sys, v, h);
     for (int i = 0; i < n; ++i)
         result[i] = 0;
 
@@ -1110,7 +1128,7 @@ void orc_ls_point(const orc_job* job, int64_t g, const double* zIn, double* out)
     /* perturbations placed, and deviations orthonormalised, in physical units */
     for (int j = 0; j < n; ++j)
         for (int i = 0; i < n; ++i)
-            y[j * n + i] = to_stored(sys, y[j * n + i] * eps, i, sy) + x[i];
+            y[j * n + i] = to_stored(y[j * n + i] * eps, i, &u) + x[i];
 
     for (int b = 0; b < sizeOfBlock; ++b) {
         /* every trajectory stops at its own first violation (cudaLibrary.cu:1049-1060) */
@@ -1119,12 +1137,12 @@ void orc_ls_point(const orc_job* job, int64_t g, const double* zIn, double* out)
             orc_loop(sys, y + j * n, v, h, nNT, 1, 0, job->maxValue, NULL, 0, 1);
         for (int k = 0; k < n; ++k)
             for (int l = 0; l < n; ++l)
-                y[k * n + l] = to_phys(sys, y[k * n + l] - x[l], l, iy);
+                y[k * n + l] = to_phys(y[k * n + l] - x[l], l, &u);
         orc_gram_schmidt(y, z, n, den);
         for (int k = 0; k < n; ++k) {
             result[k] += log(den[k] / eps);
             for (int j = 0; j < n; ++j)
-                y[k * n + j] = (double)(x[j] + to_stored(sys, z[k * n + j] * eps, j, sy));
+                y[k * n + j] = (double)(x[j] + to_stored(z[k * n + j] * eps, j, &u));
         }
     }
     for (int i = 0; i < n; ++i)

@@ -289,19 +289,24 @@ def test_surrogate_config_defaults(cbf):
 
 
 @pytest.mark.parametrize("kw,want", [
-    (dict(), 1),                                              # Chen a in [30, 45]: rescaled step
-    (dict(system="lorenz", values=[0.5, 10, 28, 8 / 3], ranges=[5, 20, 20, 200], idxMut=[1, 2]), 1),
+    (dict(), 2),                                              # Chen a in [30, 45], s = 1/2: 8-instruction form
+    (dict(system="lorenz", values=[0.5, 10, 28, 8 / 3], ranges=[5, 20, 20, 200], idxMut=[1, 2]), 2),
+    (dict(values=[0.3, 35, 3, 28]), 1),                       # s != 1/2: the 9-instruction form
+    (dict(values=[0.0, 35, 3, 28]), 0),                       # s = 0 (k = 0): 14-instruction form
+    (dict(values=[1.0, 35, 3, 28]), 1),                       # s = 1 (h1 = 0)
     (dict(ranges=[-5, 5, 20, 30], nPts=11), 0),               # a = 0 on the grid: 14-instruction form
-    (dict(ranges=[-5, 5, 20, 30], nPts=10), 1),               # a never exactly 0
+    (dict(ranges=[-5, 5, 20, 30], nPts=10), 2),               # a never exactly 0
     (dict(idxMut=[0, 3], ranges=[0.2, 0.8, 20, 30]), 0),      # s swept
     (dict(system="rossler", values=[0.5, 0.2, 0.2, 5.7], ranges=[0.05, 0.35, 0.05, 0.35], idxMut=[1, 2]), 0),
-    (dict(sweepIC=True, idxMut=[0, 2], ranges=[-5, 5, -5, 5]), 1),
+    (dict(sweepIC=True, idxMut=[0, 2], ranges=[-5, 5, -5, 5]), 2),
     (dict(values=[0.5, 0.0, 3, 28], sweepIC=True, idxMut=[0, 2], ranges=[-5, 5, -5, 5]), 0),
     (dict(values=[0.5, 35, 3, 1e30], idxMut=[1, 2], ranges=[30, 45, 1, 5]), 0),  # c beyond 2^64
 ])
 def test_step_form_choice_matches_oracle(cbf, orc, kw, want):
     """The rescaled Chen/Lorenz step is chosen per job by the same rule in the
-    library and the oracle (every value the grid holds is checked)."""
+    library and the oracle (every value the grid holds is checked): 2 for its
+    8-instruction form (s = 1/2), 1 for the 9-instruction form, 0 for the
+    14-instruction form."""
     base = dict(system="chen", nPts=16, ranges=[30, 45, 20, 30], idxMut=[1, 3], ic=[0.1, 0.1, 0.1],
                 values=[0.5, 35, 3, 28], h=0.002, tMax=10, NT=0.5, lleEps=1e-8, transientTime=1, maxValue=1e4)
     base.update(kw)

@@ -70,6 +70,9 @@ def test_grid_coordinates_match_oracle(cbf, orc, gpu_ok, nPts, first, count):
     (ROSSLER, dict(ranges=[0.05, 0.35, 0.05, 0.35], idxMut=[1, 2], h=0.01, writableVar=0)),
     (LORENZ, dict(ranges=[5, 20, 20, 200], idxMut=[1, 2], h=0.005, writableVar=2)),
     (CHEN, dict(ranges=[30, 45, 20, 30], idxMut=[1, 3], h=0.002, writableVar=1)),
+    # s = 0.3: the rescaled step's 9-instruction form, z (stored scaled) recorded
+    (dict(CHEN, values=[0.3, 35.0, 3.0, 28.0]), dict(ranges=[30, 45, 20, 30], idxMut=[1, 3], h=0.002,
+                                                    writableVar=2)),
     (MEMRISTIVE, dict(ranges=[-6, 6, -15, 15], idxMut=[4, 3], h=0.005, writableVar=4)),
 ])
 @pytest.mark.parametrize("sweepIC", [False, True])
@@ -245,6 +248,7 @@ CHEN_LLE = dict(nPts=8, ranges=[30, 45, 20, 30], idxMut=[1, 3], h=0.002, NT=0.5,
     dict(maxValue=20.0),                                    # early exits every interval
     dict(sweepIC=True, idxMut=[0, 2], ranges=[-16, 16, 5, 30]),
     dict(dims=1),
+    dict(values=[0.3, 35.0, 3.0, 28.0]),                    # the rescaled step's 9-instruction form
 ])
 def test_lle_map_matches_oracle(cbf, orc, gpu_ok, extra):
     kw = dict(CHEN_LLE)
