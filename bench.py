@@ -63,8 +63,9 @@ SUR_WORKLOAD = dict(WORKLOAD, nPts=8192, seedChunk=200000, maxAmountOfPeaks=512,
 # FP64 work of one CD step of each system (csrc/systems.cuh; FMA = 2 flops)
 FLOPS_PER_STEP = {"chen": 19, "lorenz": 19, "rossler": 17, "memristive5": 66}
 FP64_INSTR_PER_STEP = {"chen": 14, "lorenz": 14, "rossler": 10, "memristive5": 52}
-# the rescaled Chen/Lorenz step (systems.cuh QuadScaled: 4 MUL + 6 FMA)
-# the rescaled form: (flops, FP64 instructions) per step for s = 1/2 and for other s
+# the rescaled Chen/Lorenz step (systems.cuh QuadScaled): (flops, FP64 instructions)
+# per step for s = 1/2 (6 FMA + 2 MUL) and for other s (one more MUL), keyed by
+# cbf_job_scaled_step
 SCALED_COST = {2: (14, 8, "rescaled 8-instruction CD step (s = 1/2)"), 1: (15, 9, "rescaled 9-instruction CD step")}
 FP64_LANES_PER_SM = 64
 

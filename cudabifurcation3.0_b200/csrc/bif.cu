@@ -405,8 +405,8 @@ cudaError_t launch_bif(const DevJob& J, void* d_out, int* d_aux, cudaStream_t s)
     switch (J.system) {
     case CBF_SYS_MEMRISTIVE5: return launch_bif_s<Memristive5>(J, d_out, d_aux, s);
     case CBF_SYS_ROSSLER: return launch_bif_s<Rossler>(J, d_out, d_aux, s);
-    case CBF_SYS_LORENZ: return J.scaledStep ? launch_bif_s<LorenzScaled>(J, d_out, d_aux, s) : launch_bif_s<Lorenz>(J, d_out, d_aux, s);
-    case CBF_SYS_CHEN: return J.scaledStep ? launch_bif_s<ChenScaled>(J, d_out, d_aux, s) : launch_bif_s<Chen>(J, d_out, d_aux, s);
+    case CBF_SYS_LORENZ: return J.scaledStep ? (J.unitStep ? launch_bif_s<LorenzScaledU>(J, d_out, d_aux, s) : launch_bif_s<LorenzScaled>(J, d_out, d_aux, s)) : launch_bif_s<Lorenz>(J, d_out, d_aux, s);
+    case CBF_SYS_CHEN: return J.scaledStep ? (J.unitStep ? launch_bif_s<ChenScaledU>(J, d_out, d_aux, s) : launch_bif_s<ChenScaled>(J, d_out, d_aux, s)) : launch_bif_s<Chen>(J, d_out, d_aux, s);
     default: return cudaErrorInvalidValue;
     }
 }

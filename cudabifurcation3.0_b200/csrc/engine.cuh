@@ -1,5 +1,6 @@
 // Internal definitions shared by the kernels and the C-ABI layer.
 #pragma once
+#include <limits.h>
 
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -113,6 +114,40 @@ __device__ __forceinline__ unsigned abs_hi(double v)
 {
     return (unsigned)(__double_as_longlong(v) >> 32) & 0x7fffffffu;
 }
+
+// Conservative magnitude tracker of a stream of doubles against a threshold T:
+// |v| >= T needs hi(|v|) >= hi(T) (the high word is monotone in the magnitude),
+// and the signed high word of v is hi(|v|) for v >= 0, while its unsigned high
+// word is 2^31 + hi(|v|) for v < 0.  So the signed maximum of the high words
+// reaches hi(T) only if some positive value may have reached T, and the
+// unsigned maximum reaches 2^31 + hi(T) only if some negative one may have
+// (NaNs count as reaching it).  Two three-input maxima (the sm_90+ DPX integer
+// instructions) take two values per update with no masking: half the integer
+// work of tracking max |hi| of each value, which competes with the FP64 step
+// for issue slots.
+struct HiTrack {
+    int s;
+    unsigned u;
+    __device__ __forceinline__ void init()
+    {
+        s = INT_MIN;
+        u = 0;
+    }
+    __device__ __forceinline__ void add2(double a, double b)
+    {
+        const int ha = __double2hiint(a), hb = __double2hiint(b);
+        s = __vimax3_s32(s, ha, hb);
+        u = __vimax3_u32(u, (unsigned)ha, (unsigned)hb);
+    }
+    __device__ __forceinline__ void add1(double a)
+    {
+        const int ha = __double2hiint(a);
+        s = max(s, ha);
+        u = max(u, (unsigned)ha);
+    }
+    // hiT = the threshold's high word without sign (DevJob::divHi)
+    __device__ __forceinline__ bool maybe(unsigned hiT) const { return s >= (int)hiT || u >= 0x80000000u + hiT; }
+};
 
 // Exact divergence test of loopCalculateDiscreteModel (cudaLibrary.cu:69-71).
 __device__ __forceinline__ bool diverged(double v, double thresh)

@@ -40,25 +40,35 @@ __device__ __forceinline__ void run_checked(double (&x)[PPT][S::DIM],
     for (int done = 0; done < n; done += kTransientChunk) {
         const int m = min(kTransientChunk, n - done);
         double x0[PPT][S::DIM];
-        unsigned mx[PPT];
+        HiTrack tr[PPT];
 #pragma unroll
         for (int j = 0; j < PPT; ++j) {
             copy_state<S::DIM>(x0[j], x[j]);
-            mx[j] = 0;
+            tr[j].init();
         }
+        // two steps per update of the tracker
 #pragma unroll UNR
-        for (int i = 0; i < m; ++i) {
+        for (int i = 0; i + 1 < m; i += 2) {
 #pragma unroll
             for (int j = 0; j < PPT; ++j) {
                 S::step(x[j], c[j]);
-                mx[j] = max(mx[j], abs_hi(x[j][0]));
+                const double a = x[j][0];
+                S::step(x[j], c[j]);
+                tr[j].add2(a, x[j][0]);
+            }
+        }
+        if (m & 1) {
+#pragma unroll
+            for (int j = 0; j < PPT; ++j) {
+                S::step(x[j], c[j]);
+                tr[j].add1(x[j][0]);
             }
         }
 #pragma unroll
         for (int j = 0; j < PPT; ++j) {
             if (!alive[j]) {
                 copy_state<S::DIM>(x[j], x0[j]);  // stopped earlier: state frozen
-            } else if (mx[j] >= J.divHi) {
+            } else if (tr[j].maybe(J.divHi)) {
                 copy_state<S::DIM>(x[j], x0[j]);
                 for (int i = 0; i < m; ++i) {
                     S::step(x[j], c[j]);
@@ -91,12 +101,12 @@ __device__ __forceinline__ void run_pair(double (&x)[PPT][S::DIM], double (&y)[P
         return;
     }
     double x0[PPT][S::DIM], y0[PPT][S::DIM];
-    unsigned mx[PPT], my[PPT];
+    HiTrack tr[PPT];  // x and y of a point share one tracker
 #pragma unroll
     for (int j = 0; j < PPT; ++j) {
         copy_state<S::DIM>(x0[j], x[j]);
         copy_state<S::DIM>(y0[j], y[j]);
-        mx[j] = my[j] = 0;
+        tr[j].init();
     }
 #pragma unroll UNR
     for (int i = 0; i < n; ++i) {
@@ -104,20 +114,17 @@ __device__ __forceinline__ void run_pair(double (&x)[PPT][S::DIM], double (&y)[P
         for (int j = 0; j < PPT; ++j) {
             S::step(x[j], c[j]);
             S::step(y[j], c[j]);
-            mx[j] = max(mx[j], abs_hi(x[j][0]));
-            my[j] = max(my[j], abs_hi(y[j][0]));
+            tr[j].add2(x[j][0], y[j][0]);
         }
     }
 #pragma unroll
     for (int j = 0; j < PPT; ++j) {
-        if (mx[j] >= J.divHi) {
+        if (tr[j].maybe(J.divHi)) {  // either trajectory may have stopped: replay both exactly
             copy_state<S::DIM>(x[j], x0[j]);
             for (int i = 0; i < n; ++i) {
                 S::step(x[j], c[j]);
                 if (diverged(x[j][0], J.divThresh)) break;
             }
-        }
-        if (my[j] >= J.divHi) {
             copy_state<S::DIM>(y[j], y0[j]);
             for (int i = 0; i < n; ++i) {
                 S::step(y[j], c[j]);

@@ -2,12 +2,12 @@
 // tcgen05.mma (BF16 x BF16 -> FP32, M = 128) with the accumulator in tensor
 // memory, operands in shared memory, weights brought in by bulk async copies.
 // Included by mlp.cu inside its anonymous namespace (uses its constants,
-// point_features and silu).
+// point_features, encode8, pack_bf16x2 and silu).
 //
 // One persistent CTA per SM (512 threads, 192 KB of shared memory) takes tiles
 // of 128 grid points:
-//   features (4 inputs, zero-padded to K = 16) -> A buffer
-//   layer 1: 1 MMA (K 16, N 256) | layers 2, 3: 16 MMAs (K 256, N 256)
+//   features (4 inputs and their 124 Fourier terms, K = 128) -> A buffer
+//   layer 1: 8 MMAs (K 128, N 256) | layers 2, 3: 16 MMAs (K 256, N 256)
 //   | layer 4: 16 MMAs (K 256, N 32: the 17 outputs and zero rows)
 // Between layers the accumulator (128 lanes x 256 FP32 columns of tensor
 // memory) is read with tcgen05.ld, bias + SiLU applied, rounded to BF16 and
@@ -29,7 +29,7 @@ constexpr int kTcCols = 256;     // tensor-memory columns allocated (FP32 accumu
 constexpr int kTcN4 = 32;        // layer-4 MMA N: 17 outputs padded with zero rows
 constexpr uint32_t kTcABytes = kTcM * kHid * 2;      // 65536
 constexpr uint32_t kTcBBytes = kHid * kHid * 2;      // 131072
-constexpr uint32_t kTcW1Bytes = kHid * 16 * 2;       // 8192 (K padded to 16)
+constexpr uint32_t kTcW1Bytes = kHid * kIn * 2;      // 65536
 constexpr uint32_t kTcW4Bytes = kTcN4 * kHid * 2;    // 16384
 constexpr uint32_t kTcPackBytes = kTcW1Bytes + 2 * kTcBBytes + kTcW4Bytes;
 constexpr size_t kTcSmem = kTcABytes + kTcBBytes + 64;
@@ -143,11 +143,6 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
     for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
 }
 
-__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi)
-{
-    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
-    return *reinterpret_cast<const uint32_t*>(&v);
-}
 
 // The BF16 weights (flat layout of the parameter buffer) in the shared-memory
 // operand layout: W1 (256 x 4, K padded to 16), W2, W3 (256 x 256), W4 (17 x
@@ -243,7 +238,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         if (tid == 0) {
             if (mbar_wait(wbar, wph)) {
                 tc_fence_after();
-                if (L == 0) tc_issue(tmem, aAddr, bAddr, 1, kHid * 16, tc_idesc(kTcM, kHid));
+                if (L == 0) tc_issue(tmem, aAddr, bAddr, kIn / 16, kHid * 16, tc_idesc(kTcM, kHid));
                 else if (L < 3) tc_issue(tmem, aAddr, bAddr, kHid / 16, kHid * 16, tc_idesc(kTcM, kHid));
                 else tc_issue(tmem, aAddr, bAddr, kHid / 16, kTcN4 * 16, tc_idesc(kTcM, kTcN4));
                 tc_commit(mbar);
@@ -271,12 +266,20 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     for (long long tile = blockIdx.x; tile < nTiles && !bad; tile += gridDim.x) {
         const long long r0 = tile * kTcM;
         fetch(0);
-        if (tid < kTcM) {
-            float x[kIn] = {0.f, 0.f, 0.f, 0.f};
-            if (r0 + tid < nPoints) point_features(f, r0 + tid, x);
-            *reinterpret_cast<uint4*>(A + tc_off(kTcM, tid, 0)) =
-                make_uint4(pack_bf16x2(x[0], x[1]), pack_bf16x2(x[2], x[3]), 0u, 0u);
-            *reinterpret_cast<uint4*>(A + tc_off(kTcM, tid, 8)) = make_uint4(0u, 0u, 0u, 0u);
+        {
+            // four threads per point, each encoding 4 of its 16 groups of 8 inputs
+            const int pt = tid >> 2, part = tid & 3;
+            float x[kRaw] = {0.f, 0.f, 0.f, 0.f};
+            const bool live = r0 + pt < nPoints;
+            if (live) point_features(f, r0 + pt, x);
+            for (int j = part; j < kIn / 8; j += 4) {
+                float e[8];
+                encode8(x, j, e);
+                *reinterpret_cast<uint4*>(A + tc_off(kTcM, pt, 8 * j)) =
+                    live ? make_uint4(pack_bf16x2(e[0], e[1]), pack_bf16x2(e[2], e[3]), pack_bf16x2(e[4], e[5]),
+                                      pack_bf16x2(e[6], e[7]))
+                         : make_uint4(0u, 0u, 0u, 0u);
+            }
         }
         handoff();
         for (int L = 0; L < 4 && !bad; ++L) {

@@ -6,13 +6,20 @@ are compared with.  The surrogate has no counterpart in the reference project,
 so the restatement follows the network's definition rather than a reference
 file:
 
-    MLP 4 -> 256 -> 256 -> 256 -> 17, SiLU on the hidden layers,
+    4 inputs -> fixed Fourier encoding (128) -> 256 -> 256 -> 256 -> 17,
+    SiLU on the hidden layers,
     output 0 = normalised LLE (loss wLle * squared error),
     outputs 1..16 = logits of the 16-way regime class (softmax cross-entropy),
     loss = batch mean of both terms.
 
+The encoding (not trained) keeps the 4 inputs and adds, for 62 fixed
+frequencies b_k (fourier_freqs), sin(2 pi p_k) and cos(2 pi p_k) of
+p_k = b_k0 x1 + b_k1 x2 over the two swept-parameter inputs: a small MLP on raw
+coordinates cannot resolve the fine regime structure of a bifurcation map
+(it fits low frequencies first), the encoded one can.
+
 With ``bf16=True`` the values are rounded to bfloat16 (round to nearest even)
-where the kernels round them: the input rows, the weights fed to the tensor
+where the kernels round them: the encoded input rows, the weights fed to the tensor
 cores, the hidden activations, the output gradient and the hidden-layer
 gradients that feed further products.  Biases, pre-activations, the outputs and
 the bias gradients stay FP32 (here: float64), and the products accumulate at
@@ -23,9 +30,10 @@ from __future__ import annotations
 
 import numpy as np
 
-K_IN, K_HID, K_OUT, K_CLS = 4, 256, 17, 16
+K_RAW, K_FREQ, K_HID, K_OUT, K_CLS = 4, 62, 256, 17, 16
+K_IN = K_RAW + 2 * K_FREQ  # first-layer inputs: 128
 
-# flat parameter layout: W1[256x4] b1 W2[256x256] b2 W3[256x256] b3 W4[17x256] b4
+# flat parameter layout: W1[256x128] b1 W2[256x256] b2 W3[256x256] b3 W4[17x256] b4
 _SHAPES = [("W1", (K_HID, K_IN)), ("b1", (K_HID,)), ("W2", (K_HID, K_HID)), ("b2", (K_HID,)),
            ("W3", (K_HID, K_HID)), ("b3", (K_HID,)), ("W4", (K_OUT, K_HID)), ("b4", (K_OUT,))]
 NUM_PARAMS = sum(int(np.prod(s)) for _, s in _SHAPES)
@@ -57,6 +65,40 @@ def bf16(x):
     return (r & 0xFFFFFFFF).astype(np.uint32).view(np.float32).astype(np.float64)
 
 
+def fourier_freqs(seed=0x5EED):
+    """The encoding's 62 x 2 frequencies (cycles per unit of the [-1, 1] axes), as
+    mlp.cu builds them: per value one xorshift64 word (state seed * 0x9E3779B97F4A7C15
+    + 1), b = (sum of its four low bytes - 510) / 16 -- an Irwin-Hall approximation
+    of a normal distribution with standard deviation about 9, exact in float32."""
+    mask = 0xFFFFFFFFFFFFFFFF
+    s = (seed * 0x9E3779B97F4A7C15 + 1) & mask
+    b = np.empty((K_FREQ, 2), np.float32)
+    for k in range(K_FREQ):
+        for j in range(2):
+            s ^= (s << 13) & mask
+            s ^= s >> 7
+            s ^= (s << 17) & mask
+            b[k, j] = np.float32((sum((s >> (8 * i)) & 255 for i in range(4)) - 510) / 16.0)
+    return b
+
+
+def encode(x):
+    """First-layer inputs of raw rows x (n, 4): the 4 values, then for each
+    frequency k, sin(2 pi p_k) and cos(2 pi p_k), p_k = fl(fl(b_k0 x1) + fl(b_k1 x2))
+    in float32 (the kernels' operation order; the sines and cosines are evaluated
+    here in float64 and rounded to float32, the kernels' sincospif is within
+    about an ulp of that)."""
+    x = np.asarray(x, np.float32).reshape(-1, K_RAW)
+    b = fourier_freqs()
+    p = (x[:, 1:2] * b[None, :, 0]) + (x[:, 2:3] * b[None, :, 1])  # float32 products and sum
+    v = np.pi * (2.0 * p.astype(np.float64))
+    e = np.empty((len(x), K_IN), np.float32)
+    e[:, :K_RAW] = x
+    e[:, K_RAW::2] = np.sin(v).astype(np.float32)
+    e[:, K_RAW + 1::2] = np.cos(v).astype(np.float32)
+    return e
+
+
 def _silu(z):
     return z / (1.0 + np.exp(-z))
 
@@ -67,11 +109,12 @@ def _silu_grad(z):
 
 
 def forward_backward(params, x, y_lle, y_cls, w_lle, bf16_round=True):
-    """Returns (loss, grads[NUM_PARAMS], out[n, 17]) for the batch (x, y_lle, y_cls)."""
+    """Returns (loss, grads[NUM_PARAMS], out[n, 17]) for the batch of raw rows
+    (x [n, 4], y_lle, y_cls)."""
     r = bf16 if bf16_round else (lambda a: np.asarray(a, np.float64))
     P = unpack(params)
     W = {k: r(P[k]) for k in ("W1", "W2", "W3", "W4")}
-    x = r(np.asarray(x, np.float64).reshape(-1, K_IN))
+    x = r(encode(x).astype(np.float64))
     n = x.shape[0]
     z1 = x @ W["W1"].T + P["b1"]
     h1 = r(_silu(z1))
@@ -162,7 +205,7 @@ def grid_features(system, nPts, ranges, idxMut, values, grid_values):
         third += 1
     t = f32(values[third] * 0.1) if third < 4 else f32(0)
     g = np.asarray(grid_values, np.float64)
-    x = np.empty((len(g), K_IN), np.float32)
+    x = np.empty((len(g), K_RAW), np.float32)
     x[:, 0] = f32(SYSTEM_FEATURE[system])
     x[:, 1] = (g[:, 0].astype(np.float32) - lo0) * inv0 - f32(1)
     x[:, 2] = (g[:, 1].astype(np.float32) - lo1) * inv1 - f32(1)

@@ -19,7 +19,7 @@ def _batch(rng, n):
 
 def test_layout():
     off = M.offsets()
-    assert M.NUM_PARAMS == 4 * 256 + 256 + 2 * (256 * 256 + 256) + 17 * 256 + 17
+    assert M.NUM_PARAMS == 128 * 256 + 256 + 2 * (256 * 256 + 256) + 17 * 256 + 17
     assert off["b4"][0] + 17 == M.NUM_PARAMS
     p = np.arange(M.NUM_PARAMS, dtype=np.float64)
     assert np.array_equal(M.pack(M.unpack(p)), p)
@@ -65,6 +65,22 @@ def test_bf16_path_is_close_to_exact_path():
     l1, g1, _ = M.forward_backward(p, x, yl, yc, 1.0, bf16_round=True)
     assert abs(l1 - l0) < 0.02 * abs(l0)
     assert np.linalg.norm(g1 - g0) < 0.05 * np.linalg.norm(g0)
+
+
+def test_fourier_encoding():
+    """The fixed encoding: 62 exact float32 frequencies with a spread of about 9
+    cycles per unit, and rows of (x, sin 2 pi p_k, cos 2 pi p_k)."""
+    b = M.fourier_freqs()
+    assert b.shape == (62, 2) and b.dtype == np.float32
+    assert np.array_equal(b * 16, np.round(b * 16)) and np.abs(b).max() <= 510 / 16
+    assert 7 < b.std() < 11
+    x = np.array([[1.0, 0.25, -0.5, 0.3], [-1.0, 0.0, 0.0, 0.0]], np.float32)
+    e = M.encode(x)
+    assert e.shape == (2, 128) and np.array_equal(e[:, :4], x)
+    p = (b[:, 0] * np.float32(0.25) + b[:, 1] * np.float32(-0.5)).astype(np.float64)
+    assert np.allclose(e[0, 4::2], np.sin(2 * np.pi * p), atol=1e-7)
+    assert np.allclose(e[0, 5::2], np.cos(2 * np.pi * p), atol=1e-7)
+    assert np.array_equal(e[1, 4::2], np.zeros(62, np.float32)) and np.array_equal(e[1, 5::2], np.ones(62, np.float32))
 
 
 def test_init_is_deterministic_and_bounded():
