@@ -94,9 +94,10 @@ constexpr FreqTable make_freqs()
 __constant__ FreqTable c_freq = make_freqs();
 
 // Encoded first-layer inputs 8j .. 8j+7 of raw features x: e[0..3] = x, then
-// e[4 + 2k] = sin(2 pi p_k), e[5 + 2k] = cos(2 pi p_k), p_k = fl(fl(b_k0 x1) +
-// fl(b_k1 x2)) (sincospif of 2 p_k: exact argument reduction).
-__device__ __forceinline__ void encode8(const float (&x)[kRaw], int j, float (&e)[8])
+// e[4 + 2k] = sin(2 pi fs p_k), e[5 + 2k] = cos(2 pi fs p_k), p_k = fl(fl(b_k0 x1)
+// + fl(b_k1 x2)), fs the network's frequency scale (a power of two, so 2 fs p_k
+// is exact; sincospif: exact argument reduction).
+__device__ __forceinline__ void encode8(const float (&x)[kRaw], int j, float fs, float (&e)[8])
 {
 #pragma unroll
     for (int i = 0; i < 8; i += 2) {
@@ -107,7 +108,7 @@ __device__ __forceinline__ void encode8(const float (&x)[kRaw], int j, float (&e
         } else {
             const int k = (f - kRaw) >> 1;
             const float p = __fadd_rn(__fmul_rn(c_freq.b[k][0], x[1]), __fmul_rn(c_freq.b[k][1], x[2]));
-            sincospif(2.0f * p, &e[i], &e[i + 1]);
+            sincospif((2.0f * fs) * p, &e[i], &e[i + 1]);
         }
     }
 }
@@ -144,13 +145,13 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long z)
 
 // Encoded BF16 row r (x: its raw features) into xb (pitch kIn) and, if xT is
 // given, column r of xT (pitch ldT).
-__device__ __forceinline__ void put_encoded_row(const float (&x)[kRaw], long long r, bf16* __restrict__ xb,
-                                                bf16* __restrict__ xT, long long ldT)
+__device__ __forceinline__ void put_encoded_row(const float (&x)[kRaw], long long r, float fs,
+                                                bf16* __restrict__ xb, bf16* __restrict__ xT, long long ldT)
 {
 #pragma unroll 1
     for (int j = 0; j < kIn / 8; ++j) {
         float e[8];
-        encode8(x, j, e);
+        encode8(x, j, fs, e);
         reinterpret_cast<uint4*>(xb + r * kXPitch)[j] =
             make_uint4(pack_bf16x2(e[0], e[1]), pack_bf16x2(e[2], e[3]), pack_bf16x2(e[4], e[5]),
                        pack_bf16x2(e[6], e[7]));
@@ -167,8 +168,9 @@ __device__ __forceinline__ void put_encoded_row(const float (&x)[kRaw], long lon
 // ldT) for the first layer's weight gradient.
 __global__ void gather_kernel(const float* __restrict__ X, const float* __restrict__ ylle,
                               const int* __restrict__ ycls, long long N, int B,
-                              const unsigned long long* step, unsigned long long seed, bf16* __restrict__ xb,
-                              bf16* __restrict__ xT, long long ldT, float* __restrict__ bl, int* __restrict__ bc)
+                              const unsigned long long* step, unsigned long long seed, float fs,
+                              bf16* __restrict__ xb, bf16* __restrict__ xT, long long ldT, float* __restrict__ bl,
+                              int* __restrict__ bc)
 {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= B) return;
@@ -177,14 +179,14 @@ __global__ void gather_kernel(const float* __restrict__ X, const float* __restri
     float x[kRaw];
 #pragma unroll
     for (int f = 0; f < kRaw; ++f) x[f] = X[i * kRaw + f];
-    put_encoded_row(x, r, xb, xT, ldT);
+    put_encoded_row(x, r, fs, xb, xT, ldT);
     bl[r] = ylle[i];
     bc[r] = ycls[i];
 }
 
 // Encoded rows of n raw feature rows X [n x 4] (rows n <= r < rows: zeros).
-__global__ void encode_rows_kernel(const float* __restrict__ X, long long n, long long rows, bf16* __restrict__ xb,
-                                   bf16* __restrict__ xT, long long ldT)
+__global__ void encode_rows_kernel(const float* __restrict__ X, long long n, long long rows, float fs,
+                                   bf16* __restrict__ xb, bf16* __restrict__ xT, long long ldT)
 {
     const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= rows) return;
@@ -192,7 +194,7 @@ __global__ void encode_rows_kernel(const float* __restrict__ X, long long n, lon
         float x[kRaw];
 #pragma unroll
         for (int f = 0; f < kRaw; ++f) x[f] = X[r * kRaw + f];
-        put_encoded_row(x, r, xb, xT, ldT);
+        put_encoded_row(x, r, fs, xb, xT, ldT);
     } else {
         const bf16 zero = __float2bfloat16_rn(0.0f);
         for (int f = 0; f < kIn; ++f) {
@@ -412,6 +414,7 @@ struct Mlp {
     int B = 0;               // training batch
     long long Ba = 0;        // rows of every batch buffer: B rounded up to 128, at least 4096
     unsigned long long seed = 0;
+    float encScale = 1.0f;    // frequency scale of the input encoding (a power of two)
     float* params = nullptr;  // FP32 masters (kNumParams)
     float* grads = nullptr;
     float* m1 = nullptr;
@@ -446,6 +449,7 @@ struct Mlp {
     float gLr = 0.f;
     int gHorizon = 0;
     float gW = 0.f;
+    float gScale = 0.f;
     unsigned long long gSeed = 0;
     // prediction workspace (rows per chunk = kPredRows), no pre-activations
     bf16 *pxb = nullptr, *ph1 = nullptr, *ph2 = nullptr, *ph3 = nullptr;
@@ -789,6 +793,16 @@ cbf_status cbf_mlp_set_params(cbf_mlp* m, const float* host, int64_t n)
     return upload_params(m, host);
 }
 
+// Frequency scale of the input encoding: a power of two in [2^-8, 16].
+cbf_status cbf_mlp_set_encoding_scale(cbf_mlp* m, float scale)
+{
+    int ex = 0;
+    if (!m || !(scale >= 0x1p-8f && scale <= 16.0f) || frexpf(scale, &ex) != 0.5f)
+        return report_error(CBF_ERR_INVALID_ARG, "encoding scale must be a power of two in [2^-8, 16]");
+    m->encScale = scale;
+    return CBF_OK;
+}
+
 // One forward + backward on host data (n <= batch rows); for gradient checks.
 cbf_status cbf_mlp_forward_backward(cbf_mlp* m, const float* hx, const float* hyl, const int32_t* hyc,
                                     int32_t n, float wLle, float* hloss, float* hgrads, float* hout)
@@ -800,7 +814,7 @@ cbf_status cbf_mlp_forward_backward(cbf_mlp* m, const float* hx, const float* hy
     cudaError_t e = cudaMemcpy(m->xraw, hx, (size_t)n * kRaw * sizeof(float), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
         e = launch1d(rows, 0, [&](unsigned b, int t) {
-            encode_rows_kernel<<<b, t>>>(m->xraw, n, rows, m->xb, m->xT, m->Ba);
+            encode_rows_kernel<<<b, t>>>(m->xraw, n, rows, m->encScale, m->xb, m->xT, m->Ba);
         });
     if (e == cudaSuccess) e = cudaMemcpy(m->yl, hyl, (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(m->yc, hyc, (size_t)n * sizeof(int), cudaMemcpyHostToDevice);
@@ -837,7 +851,7 @@ cbf_status cbf_mlp_train(cbf_mlp* m, const float* dX, const float* dYl, const in
     const int B = m->B;
     cudaError_t e = cudaSuccess;
     if (!m->exec || m->gX != dX || m->gN != N || m->gLr != lr || m->gHorizon != horizon ||
-        m->gW != wLle || m->gSeed != m->seed) {
+        m->gW != wLle || m->gSeed != m->seed || m->gScale != m->encScale) {
         if (m->exec) cudaGraphExecDestroy(m->exec);
         if (m->graph) cudaGraphDestroy(m->graph);
         m->exec = nullptr;
@@ -845,8 +859,8 @@ cbf_status cbf_mlp_train(cbf_mlp* m, const float* dX, const float* dYl, const in
         e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return report_cuda_error(e, "begin capture of the training step");
         cudaError_t ce = launch1d(B, s, [&](unsigned b, int t) {
-            gather_kernel<<<b, t, 0, s>>>(dX, dYl, (const int*)dYc, N, B, m->step, m->seed, m->xb,
-                                          m->xT, m->Ba, m->yl, m->yc);
+            gather_kernel<<<b, t, 0, s>>>(dX, dYl, (const int*)dYc, N, B, m->step, m->seed, m->encScale,
+                                          m->xb, m->xT, m->Ba, m->yl, m->yc);
         });
         const int rows = (B + kGtM - 1) / kGtM * kGtM;
         if (ce == cudaSuccess) ce = forward(*m, B, train_bufs(*m), s);
@@ -881,6 +895,7 @@ cbf_status cbf_mlp_train(cbf_mlp* m, const float* dX, const float* dYl, const in
         m->gLr = lr;
         m->gHorizon = horizon;
         m->gW = wLle;
+        m->gScale = m->encScale;
         m->gSeed = m->seed;
     }
     for (int i = 0; i < steps && e == cudaSuccess; ++i) {
@@ -910,7 +925,7 @@ cbf_status cbf_mlp_predict(cbf_mlp* m, const float* dX, int64_t N, float lleMean
     for (long long r0 = 0; r0 < N && e == cudaSuccess; r0 += kPredRows) {
         const int n = (int)((N - r0) < kPredRows ? (N - r0) : kPredRows);
         e = launch1d(n, s, [&](unsigned b, int t) {
-            encode_rows_kernel<<<b, t, 0, s>>>(dX + r0 * kRaw, n, n, m->pxb, nullptr, 0);
+            encode_rows_kernel<<<b, t, 0, s>>>(dX + r0 * kRaw, n, n, m->encScale, m->pxb, nullptr, 0);
         });
         if (e == cudaSuccess) e = forward(*m, n, pred_bufs(*m), s);
         if (e == cudaSuccess)
@@ -998,8 +1013,8 @@ cudaError_t mlp_predict_grid(cbf_mlp* m, const FeatureSpec& f, long long nPoints
     if (e != cudaSuccess) return e;
     const long long tiles = (nPoints + kTcM - 1) / kTcM;
     const unsigned grid = (unsigned)(tiles < sms ? tiles : sms);
-    mlp_predict_tc_kernel<<<grid, kTcThreads, kTcSmem, s>>>(f, nPoints, m->wpack, m->params, lleMean, lleStd, lle,
-                                                            cls, conf, m->tcErr);
+    mlp_predict_tc_kernel<<<grid, kTcThreads, kTcSmem, s>>>(f, nPoints, m->encScale, m->wpack, m->params, lleMean,
+                                                            lleStd, lle, cls, conf, m->tcErr);
     note_launch();
     e = cudaGetLastError();
     int h = 0;

@@ -184,7 +184,7 @@ __device__ __forceinline__ void tc_issue(uint32_t tmem, uint32_t aAddr, uint32_t
 }
 
 __global__ void __launch_bounds__(kTcThreads, 1)
-    mlp_predict_tc_kernel(const FeatureSpec f, long long nPoints, const unsigned char* __restrict__ wpack,
+    mlp_predict_tc_kernel(const FeatureSpec f, long long nPoints, float fs, const unsigned char* __restrict__ wpack,
                           const float* __restrict__ params, float lleMean, float lleStd, double* __restrict__ lle,
                           int* __restrict__ cls, float* __restrict__ conf, int* __restrict__ err)
 {
@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (live) point_features(f, r0 + pt, x);
             for (int j = part; j < kIn / 8; j += 4) {
                 float e[8];
-                encode8(x, j, e);
+                encode8(x, j, fs, e);
                 *reinterpret_cast<uint4*>(A + tc_off(kTcM, pt, 8 * j)) =
                     live ? make_uint4(pack_bf16x2(e[0], e[1]), pack_bf16x2(e[2], e[3]), pack_bf16x2(e[4], e[5]),
                                       pack_bf16x2(e[6], e[7]))

@@ -599,6 +599,15 @@ cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config*
         return report_cuda_error(e, "network reset");
     }
     cbf_mlp* net = buf.net;
+    {
+        // Encoding frequencies at a fixed fraction of what the label lattice
+        // resolves: scale coarseSide/512 rounded to a power of two (measured best
+        // at 512^2 labels with scale 1, at 64^2 with 1/8; higher frequencies than
+        // the labels resolve let the network fit between labels at random).
+        int ex = (int)lrint(log2((double)cs / 512.0));
+        ex = ex < -8 ? -8 : (ex > 4 ? 4 : ex);
+        if ((st = cbf_mlp_set_encoding_scale(net, ldexpf(1.0f, ex))) != CBF_OK) return st;
+    }
     const bool learned = cfg->predictor == 0;
     const int tail = !learned ? 0 : (cfg->trainSteps < 100 ? cfg->trainSteps : 100);
     std::vector<float> losses(tail > 0 ? tail : 1, 0.f);

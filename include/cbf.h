@@ -194,17 +194,27 @@ cbf_status cbf_batch_autotune(cbf_batch* batch, void* stream, int32_t* blocksPer
                               double* msPerCandidate);
 
 /* ---- the surrogate network ------------------------------------------- */
-/* MLP 4 -> 256 -> 256 -> 256 -> 17 (SiLU): output 0 = normalised LLE, outputs
- * 1..16 = logits of the 16-way peak-count regime class.  BF16 tensor-core GEMMs
- * with FP32 accumulation for forward and backward, FP32 master weights, Adam.
- * No counterpart in the reference.  Parameters are one flat FP32 vector: W1[256x4]
- * b1 W2[256x256] b2 W3[256x256] b3 W4[17x256] b4 (W row-major [out][in]). */
+/* MLP 4 -> (fixed Fourier encoding, 128) -> 256 -> 256 -> 256 -> 17 (SiLU):
+ * output 0 = normalised LLE, outputs 1..16 = logits of the 16-way peak-count
+ * regime class.  The 4 inputs are (system code, two swept parameters in [-1, 1],
+ * third parameter / 10); the encoding keeps them and adds sin(2 pi s p_k),
+ * cos(2 pi s p_k) of p_k = b_k0 x1 + b_k1 x2 for 62 fixed frequencies b_k and the
+ * network's frequency scale s (cbf_mlp_set_encoding_scale, default 1).  BF16
+ * tensor-core products (tcgen05) with FP32 accumulation for forward and
+ * backward, FP32 master weights, Adam.  No counterpart in the reference.
+ * Parameters are one flat FP32 vector: W1[256x128] b1 W2[256x256] b2
+ * W3[256x256] b3 W4[17x256] b4 (W row-major [out][in]). */
 typedef struct cbf_mlp cbf_mlp;
 int64_t cbf_mlp_num_params(void);
 cbf_status cbf_mlp_create(int32_t batch, uint64_t seed, cbf_mlp** mlp);
 void cbf_mlp_destroy(cbf_mlp* mlp);
 cbf_status cbf_mlp_get_params(cbf_mlp* mlp, float* host, int64_t n);
 cbf_status cbf_mlp_set_params(cbf_mlp* mlp, const float* host, int64_t n);
+/* Frequency scale of the input encoding, a power of two in [2^-8, 16] (else
+ * CBF_ERR_INVALID_ARG).  The frequencies a network can learn from must stay well
+ * below what its labels resolve: the surrogate map sets (coarseSide / 512) rounded
+ * to a power of two. */
+cbf_status cbf_mlp_set_encoding_scale(cbf_mlp* mlp, float scale);
 /* One forward and backward pass on n <= batch host rows (features x[n*4], LLE
  * targets, classes) with loss = wLle*MSE(out0) + CE(out1..16), both batch means;
  * returns loss, the flat gradient and the raw outputs (each optional). */

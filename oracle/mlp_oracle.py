@@ -82,16 +82,17 @@ def fourier_freqs(seed=0x5EED):
     return b
 
 
-def encode(x):
+def encode(x, scale=1.0):
     """First-layer inputs of raw rows x (n, 4): the 4 values, then for each
-    frequency k, sin(2 pi p_k) and cos(2 pi p_k), p_k = fl(fl(b_k0 x1) + fl(b_k1 x2))
-    in float32 (the kernels' operation order; the sines and cosines are evaluated
-    here in float64 and rounded to float32, the kernels' sincospif is within
-    about an ulp of that)."""
+    frequency k, sin(2 pi s p_k) and cos(2 pi s p_k), p_k = fl(fl(b_k0 x1) +
+    fl(b_k1 x2)) in float32 (the kernels' operation order), s the network's
+    frequency scale (a power of two: the scaling is exact); the sines and cosines
+    are evaluated here in float64 and rounded to float32, the kernels' sincospif
+    is within about an ulp of that."""
     x = np.asarray(x, np.float32).reshape(-1, K_RAW)
     b = fourier_freqs()
     p = (x[:, 1:2] * b[None, :, 0]) + (x[:, 2:3] * b[None, :, 1])  # float32 products and sum
-    v = np.pi * (2.0 * p.astype(np.float64))
+    v = np.pi * ((2.0 * scale) * p.astype(np.float64))
     e = np.empty((len(x), K_IN), np.float32)
     e[:, :K_RAW] = x
     e[:, K_RAW::2] = np.sin(v).astype(np.float32)
@@ -108,13 +109,13 @@ def _silu_grad(z):
     return s * (1.0 + z * (1.0 - s))
 
 
-def forward_backward(params, x, y_lle, y_cls, w_lle, bf16_round=True):
+def forward_backward(params, x, y_lle, y_cls, w_lle, bf16_round=True, scale=1.0):
     """Returns (loss, grads[NUM_PARAMS], out[n, 17]) for the batch of raw rows
     (x [n, 4], y_lle, y_cls)."""
     r = bf16 if bf16_round else (lambda a: np.asarray(a, np.float64))
     P = unpack(params)
     W = {k: r(P[k]) for k in ("W1", "W2", "W3", "W4")}
-    x = r(encode(x).astype(np.float64))
+    x = r(encode(x, scale).astype(np.float64))
     n = x.shape[0]
     z1 = x @ W["W1"].T + P["b1"]
     h1 = r(_silu(z1))
@@ -213,12 +214,13 @@ def grid_features(system, nPts, ranges, idxMut, values, grid_values):
     return x
 
 
-def predict(params, x, lle_mean, lle_std):
+def predict(params, x, lle_mean, lle_std, scale=1.0):
     """Forward pass with the kernels' BF16 rounding points (exact accumulation):
     (LLE = out0 * std + mean, class = argmax of out1..16, softmax maximum,
     the raw outputs (n, 17), the gap between the two largest logits)."""
     n = len(x)
-    _, _, out = forward_backward(params, x, np.zeros(n), np.zeros(n, np.int64), 1.0, bf16_round=True)
+    _, _, out = forward_backward(params, x, np.zeros(n), np.zeros(n, np.int64), 1.0, bf16_round=True,
+                                 scale=scale)
     logits = out[:, 1:]
     cls = logits.argmax(axis=1)
     srt = np.sort(logits, axis=1)

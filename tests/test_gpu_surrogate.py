@@ -38,14 +38,15 @@ def test_mlp_init_matches_oracle(cbf, gpu_ok):
     assert np.array_equal(net.get_params().astype(np.float64), M.init_params(11))
 
 
-@pytest.mark.parametrize("n", [37, 1000, 4096, 9000])
-def test_mlp_gradients_match_oracle(cbf, gpu_ok, n):
+@pytest.mark.parametrize("n,scale", [(37, 1.0), (1000, 0.125), (4096, 1.0), (9000, 1.0)])
+def test_mlp_gradients_match_oracle(cbf, gpu_ok, n, scale):
     """Every product on tcgen05 against the oracle.  n=37: one ragged 128-row
-    tile; n=1000: four K slices in the weight gradients; n=4096 (the training
-    batch): sixteen; n=9000: sixteen slices of 576 rows, each run in three
-    passes of at most four 64-row chunks."""
+    tile; n=1000: four K slices in the weight gradients (and the encoding at
+    frequency scale 1/8); n=4096 (the training batch): sixteen; n=9000: sixteen
+    slices of 576 rows, each run in three passes of at most four 64-row chunks."""
     rng = np.random.default_rng(n)
     net = cbf.Mlp(max(1024, n), seed=5)
+    net.set_encoding_scale(scale)
     p = M.init_params(5)
     off = M.offsets()
     for b in ("b1", "b2", "b3", "b4"):
@@ -55,7 +56,7 @@ def test_mlp_gradients_match_oracle(cbf, gpu_ok, n):
     net.set_params(p)
     x, yl, yc = _batch(rng, n)
     loss, g, out = net.forward_backward(x, yl, yc, 0.5)
-    wl, wg, wout = M.forward_backward(p.astype(np.float64), x, yl, yc, 0.5, bf16_round=True)
+    wl, wg, wout = M.forward_backward(p.astype(np.float64), x, yl, yc, 0.5, bf16_round=True, scale=scale)
     assert abs(loss - wl) <= 1e-4 * abs(wl)
     assert _rel(out, wout) < 1e-3
     for name, (o, shape) in off.items():
@@ -63,8 +64,17 @@ def test_mlp_gradients_match_oracle(cbf, gpu_ok, n):
         err = _rel(g[o:o + k], wg[o:o + k])
         assert err < 1e-2, (name, err)
     # and the BF16 gradients stay near the exact float64 ones
-    _, eg, _ = M.forward_backward(p.astype(np.float64), x, yl, yc, 0.5, bf16_round=False)
+    _, eg, _ = M.forward_backward(p.astype(np.float64), x, yl, yc, 0.5, bf16_round=False, scale=scale)
     assert _rel(g, eg) < 0.05
+
+
+def test_encoding_scale_must_be_a_power_of_two(cbf, gpu_ok):
+    net = cbf.Mlp(64, seed=1)
+    for bad in (0.0, 0.3, 3.0, 32.0, 2.0 ** -9, float("nan")):
+        with pytest.raises(Exception):
+            net.set_encoding_scale(bad)
+    for good in (2.0 ** -8, 0.125, 1.0, 16.0):
+        net.set_encoding_scale(good)
 
 
 def test_mlp_predict_matches_forward(cbf, gpu_ok):
