@@ -817,6 +817,8 @@ def main(argv=None) -> int:
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--nPts", type=int, default=None, help="override the grid side (testing)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--lle-variant", type=int, default=None,
+                    help="chen-lle2d-2048: run this LLE kernel shape instead of autotuning (profiling)")
     ap.add_argument("--plain-only", action="store_true",
                     help="chen-surrogate-8192: compute and time only the plain map (profiling)")
     ap.add_argument("--workload", default="chen-surrogate-8192",
@@ -854,7 +856,11 @@ def main(argv=None) -> int:
     spp = steps_per_point(w)
 
     probe = cbf.probe_fp64_peak(300.0)  # TFLOP/s, FMA = 2 flops
-    variant, trial_ms = cbf.autotune(job)  # picks the LLE kernel shape for this device
+    if args.lle_variant is None:
+        variant, trial_ms = cbf.autotune(job)  # picks the LLE kernel shape for this device
+    else:  # a fixed shape (profiling a chosen kernel): no autotuning launches
+        variant, trial_ms = args.lle_variant, []
+        cbf.set_lle_variant(w["system"], variant)
 
     stream = torch.cuda.Stream()
     out = torch.empty(n, dtype=torch.float64, device="cuda")

@@ -21,7 +21,6 @@
 #include <string.h>
 
 #include <algorithm>
-#include <type_traits>
 #include <vector>
 
 #include "bif_device.cuh"
@@ -158,18 +157,16 @@ __global__ void __launch_bounds__(kBatchThreads, 6) batch_kernel(
                 break;
             case CBF_SYS_ROSSLER: run_tile<Rossler, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err); break;
             case CBF_SYS_LORENZ:
-                if (J.scaledStep && FAM == kFamLle && J.unitStep)  // the map kernel's 8-instruction form
-                    run_tile<std::conditional_t<FAM == kFamLle, LorenzScaledU, LorenzScaled>, FAM>(
-                        J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err);
+                if (J.scaledStep && J.unitStep)  // the map kernels' 8-instruction form
+                    run_tile<LorenzScaledU, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err);
                 else if (J.scaledStep)
                     run_tile<LorenzScaled, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err);
                 else
                     run_tile<Lorenz, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err);
                 break;
             case CBF_SYS_CHEN:
-                if (J.scaledStep && FAM == kFamLle && J.unitStep)  // the map kernel's 8-instruction form
-                    run_tile<std::conditional_t<FAM == kFamLle, ChenScaledU, ChenScaled>, FAM>(
-                        J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err);
+                if (J.scaledStep && J.unitStep)  // the map kernels' 8-instruction form
+                    run_tile<ChenScaledU, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err);
                 else if (J.scaledStep)
                     run_tile<ChenScaled, FAM>(J, out, aux, p0, lane, slotPk, slotIv, stride, L, Sb, so, err);
                 else

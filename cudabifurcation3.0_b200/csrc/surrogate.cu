@@ -464,7 +464,7 @@ void cbf_surrogate_config_init(cbf_surrogate_config* c)
     c->refine = 1;
     c->seed = 20240101ull;
     c->expandRadius = -1;
-    c->maxWaves = 20;
+    c->maxWaves = 12;
 }
 
 cbf_status cbf_lle_map_surrogate(const cbf_job* job, const cbf_surrogate_config* cfg, double* dLle,

@@ -268,7 +268,7 @@ typedef struct cbf_surrogate_config {
                                 differs from the prediction are recomputed next; -1 (default):
                                 ceil(nPts / 8192); 0: no expansion */
     int32_t maxWaves;        /* rounds that expand: the labels and the points computed in
-                                the first maxWaves rounds mark their neighbours (20) */
+                                the first maxWaves rounds mark their neighbours (12) */
     int32_t predictor;       /* 0: the trained network (default); 1: no network -- every
                                 point takes the class and LLE of its nearest coarse-grid
                                 label, confidence 1 (the ablation that measures what the

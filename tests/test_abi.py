@@ -278,11 +278,11 @@ def test_surrogate_config_defaults(cbf):
     """The defaults of cbf_surrogate_config_init (host code) are the measured
     operating point that include/cbf.h documents: 512^2 coarse labels plus 65 536
     random points, 1500 Adam steps on minibatches of 4096, confidence threshold
-    0.4, 1 % audit, automatic expansion radius, 20 rounds."""
+    0.4, 1 % audit, automatic expansion radius, 12 expanding rounds."""
     c = cbf.surrogate_config()
     assert (c.coarseSide, c.randomPoints, c.batch, c.trainSteps) == (512, 65536, 4096, 1500)
     assert c.confThreshold == pytest.approx(0.4) and c.auditFraction == pytest.approx(0.01)
-    assert (c.boundaryRadius, c.expandRadius, c.maxWaves, c.refine) == (1, -1, 20, 1)
+    assert (c.boundaryRadius, c.expandRadius, c.maxWaves, c.refine) == (1, -1, 12, 1)
     assert (c.predictor, c.auditFill, c.idleRadius) == (0, 0, 0)
     with pytest.raises(AttributeError):
         cbf.surrogate_config(noSuchField=1)
