@@ -68,6 +68,10 @@ FP64_INSTR_PER_STEP = {"chen": 14, "lorenz": 14, "rossler": 10, "memristive5": 5
 # cbf_job_scaled_step
 SCALED_COST = {2: (14, 8, "rescaled 8-instruction CD step (s = 1/2)"), 1: (15, 9, "rescaled 9-instruction CD step")}
 FP64_LANES_PER_SM = 64
+# the same Chen CD step written unfused, as the formula reads (each add, sub, mul
+# and div of the explicit half z, y, x and the implicit half x, y, z counted once,
+# parameter-only factors hoisted): 5 + 7 + 3 + 3 + 6 + 4 = 28
+UNFUSED_CD_FLOPS_PER_STEP = {"chen": 28}
 
 # The other measured configurations (printed as their own JSON lines with
 # --workload NAME; the default run is the LLE map above).
@@ -319,7 +323,7 @@ def step_cost(cbf, job, system: str):
 
 
 def fp64_roofline(torch, device: int, cost, n_points: int, spp: int, mean_ms: float,
-                  clocks: dict, probe_tflops: float) -> dict:
+                  clocks: dict, probe_tflops: float, system: str = "chen") -> dict:
     """FP64 roofline of one map: algorithmic flops and FP64-pipe instructions;
     cost = step_cost(...)."""
     flops_step, instr_step, form = cost
@@ -338,7 +342,17 @@ def fp64_roofline(torch, device: int, cost, n_points: int, spp: int, mean_ms: fl
                            "probe measured in this run); MEASURED_PEAKS.json has no FP64 figure",
             "peak_nominal": nominal, "peak_probe": probe_tflops, "flops_per_launch": flops,
             "flops_per_step": flops_step, "fp64_instr_per_step": instr_step, "step_form": form,
-            "fp64_pipe_frac": pipe}
+            "fp64_pipe_frac": pipe, **unfused_cd(system, n_points, spp, mean_ms, peak)}
+
+
+def unfused_cd(system: str, n_points: int, spp: int, mean_ms: float, peak: float) -> dict:
+    """The same map's rate counted with the unfused formula of the CD step (the
+    work of the method as written, whatever form computes it)."""
+    f = UNFUSED_CD_FLOPS_PER_STEP.get(system)
+    if not f:
+        return {}
+    achieved = float(n_points) * spp * f / (mean_ms / 1e3) / 1e12
+    return {"unfused_cd_flops_per_step": f, "unfused_cd_achieved": achieved, "unfused_cd_frac": achieved / peak}
 
 
 def cpu_baseline(w: dict, target_s: float = 15.0) -> dict:
@@ -509,7 +523,7 @@ def run_secondary(args, name: str) -> int:
     clocks = sampler.stop()
     t = statistics.mean(ms)
     probe = cbf.probe_fp64_peak(300.0)
-    roof = fp64_roofline(torch, 0, step_cost(cbf, job, w["system"]), n, spp, t, clocks, probe)
+    roof = fp64_roofline(torch, 0, step_cost(cbf, job, w["system"]), n, spp, t, clocks, probe, w["system"])
     roof["traffic"] = None
     roof["note"] = ("integration flops only (base + perturbed trajectories); Gram-Schmidt and log "
                     "per interval on top") if task == cbf.TASK_LS else \
@@ -756,6 +770,8 @@ def run_surrogate(args) -> int:
             "steps_per_point": spp,
             "plain_points_in_step": plain_points, "plain_phase_ms": plain_phase_ms,
             "plain_map_achieved": plain_achieved, "plain_map_frac": plain_achieved / peak,
+            **unfused_cd("chen", plain_points, spp, plain_phase_ms, peak),
+            "plain_map_unfused_cd_frac": unfused_cd("chen", n, spp, plain_ms, peak).get("unfused_cd_frac"),
             "traffic": regime_traffic(plain_points)}
 
     ok = agree_min >= 0.995 and exact and e2e_same
@@ -930,7 +946,7 @@ def main(argv=None) -> int:
     same = np.array_equal(res, out.cpu().numpy(), equal_nan=True)
 
     roof = fp64_roofline(torch, local, step_cost(cbf, job, w["system"]), n, spp, statistics.mean(kernel_ms),
-                         clocks, probe)
+                         clocks, probe, w["system"])
     roof["traffic"] = traffic_from_profiles()
 
     if rank == 0:

@@ -47,7 +47,7 @@ constexpr long long kW4 = kB3 + kHid, kB4 = kW4 + kOut * kHid;
 constexpr long long kNumParams = kB4 + kOut;
 
 // Tensor-core operand copies of the weights: seven 256 x 256 BF16 slots (row
-// pitch 256), zero outside the weights: W1 (256 x 4, K padded to 16), W2, W3,
+// pitch 256), zero outside the weights: W1 (256 x 128), W2, W3,
 // W4 (17 x 256, rows padded), W2^T, W3^T, W4^T (256 x 17, K padded to 32).
 constexpr long long kSlot = (long long)kHid * kHid;
 enum { kSlotW1 = 0, kSlotW2, kSlotW3, kSlotW4, kSlotW2T, kSlotW3T, kSlotW4T, kNumSlots };

@@ -321,3 +321,19 @@ def test_step_form_choice_matches_oracle(cbf, orc, kw, want):
     o = orc.make_job(**base)
     assert got == want
     assert O.orc_scaled_step(C.addressof(o)) == want
+
+
+def test_bench_step_cost_tables():
+    """The bench's flop accounting: the rescaled forms keyed by
+    cbf_job_scaled_step (8 instructions / 14 flops at s = 1/2, 9 / 15 otherwise)
+    and the unfused CD formula's count for Chen, applied per point and step."""
+    import importlib.util
+    from pathlib import Path
+    spec = importlib.util.spec_from_file_location("bench_for_test", Path(__file__).resolve().parents[1] / "bench.py")
+    b = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(b)
+    assert b.SCALED_COST[2][:2] == (14, 8) and b.SCALED_COST[1][:2] == (15, 9)
+    r = b.unfused_cd("chen", 1000, 2000, 1000.0, 1.0)
+    assert r["unfused_cd_flops_per_step"] == 28
+    assert r["unfused_cd_achieved"] == pytest.approx(1000 * 2000 * 28 / 1.0 / 1e12)
+    assert b.unfused_cd("lorenz", 1, 1, 1.0, 1.0) == {}
