@@ -872,6 +872,10 @@ def main(argv=None) -> int:
     spp = steps_per_point(w)
 
     probe = cbf.probe_fp64_peak(300.0)  # TFLOP/s, FMA = 2 flops
+    # the same step and divergence tracking as a bare instruction stream (two
+    # chains per thread, six blocks of 128 per SM): the issue rate the map kernel
+    # is compared with
+    step_stream = cbf.probe_fp64_step(2, True, 6, 300.0)
     if args.lle_variant is None:
         variant, trial_ms = cbf.autotune(job)  # picks the LLE kernel shape for this device
     else:  # a fixed shape (profiling a chosen kernel): no autotuning launches
@@ -948,6 +952,11 @@ def main(argv=None) -> int:
     roof = fp64_roofline(torch, local, step_cost(cbf, job, w["system"]), n, spp, statistics.mean(kernel_ms),
                          clocks, probe, w["system"])
     roof["traffic"] = traffic_from_profiles()
+    sm_props = torch.cuda.get_device_properties(local)
+    roof["step_stream_fp64_pipe_frac"] = step_stream / (
+        sm_props.multi_processor_count * FP64_LANES_PER_SM * (clocks.get("sm_mhz") or 1965.0) * 1e6)
+    roof["step_stream_note"] = ("FP64 issue rate of the same 8-instruction step and divergence tracking alone "
+                                "(2 chains per thread, 6 blocks of 128 per SM; cbf_probe_fp64_step)")
 
     if rank == 0:
         base = None

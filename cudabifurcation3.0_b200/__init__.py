@@ -40,7 +40,7 @@ EXPORTS = [
     "cbf_bifurcation1d", "cbf_bifurcation1d_ic", "cbf_bifurcation2d_kde",
     "cbf_bifurcation2d_kde_ic", "cbf_bifurcation2d_dbscan", "cbf_bifurcation2d_dbscan_ic",
     "cbf_lle1d", "cbf_lle1d_ic", "cbf_lle2d", "cbf_lle2d_ic", "cbf_run_host",
-    "cbf_grid_coordinates", "cbf_probe_fp64_peak", "cbf_probe_expf_zero",
+    "cbf_grid_coordinates", "cbf_probe_fp64_peak", "cbf_probe_fp64_step", "cbf_probe_expf_zero",
     "cbf_divergence_threshold", "cbf_lle_seeds", "cbf_autotune", "cbf_set_lle_variant",
     "cbf_get_lle_variant", "cbf_batch_create", "cbf_batch_destroy", "cbf_batch_points",
     "cbf_batch_blocks_per_sm", "cbf_batch_run", "cbf_batch_capture", "cbf_batch_launch",
@@ -214,6 +214,7 @@ def lib():
         L.cbf_lle_seeds.argtypes = [C.POINTER(Job), _dp]
         L.cbf_lle_seeds.restype = C.c_int32
         L.cbf_probe_fp64_peak.argtypes = [C.c_double, _dp]
+        L.cbf_probe_fp64_step.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_double, _dp]
         L.cbf_probe_expf_zero.argtypes = [C.c_float, C.POINTER(C.c_uint64)]
         L.cbf_divergence_threshold.argtypes = [C.c_double, _ip, _dp]
         bif1d = [C.c_int32, C.c_double, C.c_int32, C.c_double, C.c_int32, _dp, _dp, _ip,
@@ -236,7 +237,7 @@ def lib():
         for f in ("cbf_lle1d", "cbf_lle1d_ic", "cbf_lle2d", "cbf_lle2d_ic", "cbf_ls1d", "cbf_ls2d"):
             getattr(L, f).argtypes = lle
         for f in ("cbf_device_count", "cbf_set_device", "cbf_validate", "cbf_run", "cbf_run_host",
-                  "cbf_grid_coordinates", "cbf_probe_fp64_peak", "cbf_probe_expf_zero",
+                  "cbf_grid_coordinates", "cbf_probe_fp64_peak", "cbf_probe_fp64_step", "cbf_probe_expf_zero",
                   "cbf_divergence_threshold", "cbf_bifurcation1d", "cbf_bifurcation1d_ic",
                   "cbf_bifurcation2d_kde", "cbf_bifurcation2d_kde_ic", "cbf_bifurcation2d_dbscan",
                   "cbf_bifurcation2d_dbscan_ic", "cbf_lle1d", "cbf_lle1d_ic", "cbf_lle2d",
@@ -634,6 +635,13 @@ def probe_fp64_peak(ms: float = 200.0) -> float:
     t = C.c_double(0.0)
     check(lib().cbf_probe_fp64_peak(ms, C.byref(t)))
     return t.value
+
+
+def probe_fp64_step(chains: int = 2, tracking: bool = True, blocks_per_sm: int = 6, ms: float = 200.0) -> float:
+    """FP64 lane instructions per second of the map kernels' step stream alone."""
+    r = C.c_double(0.0)
+    check(lib().cbf_probe_fp64_step(chains, 1 if tracking else 0, blocks_per_sm, ms, C.byref(r)))
+    return r.value
 
 
 def probe_expf_zero(threshold: float) -> int:

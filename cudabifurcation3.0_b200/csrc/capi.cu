@@ -16,6 +16,7 @@ namespace cbf {
 
 cudaError_t probe_fp64_peak(double ms, double* tflops);
 cudaError_t probe_expf_zero(float threshold, unsigned long long* count);
+cudaError_t probe_fp64_step(int chains, bool track, int blocksPerSm, double ms, double* instrPerSec);
 
 namespace {
 
@@ -929,6 +930,17 @@ cbf_status cbf_probe_fp64_peak(double ms, double* tflops)
     if (!tflops || !(ms > 0)) return fail(CBF_ERR_INVALID_ARG, "bad probe arguments");
     cudaError_t e = probe_fp64_peak(ms, tflops);
     if (e != cudaSuccess) return cuda_fail(e, "fp64 probe");
+    return CBF_OK;
+}
+
+cbf_status cbf_probe_fp64_step(int32_t chains, int32_t tracking, int32_t blocksPerSm, double ms,
+                               double* fp64InstrPerSec)
+{
+    if (!fp64InstrPerSec) return fail(CBF_ERR_INVALID_ARG, "null output");
+    if ((chains != 1 && chains != 2 && chains != 4) || blocksPerSm < 1 || blocksPerSm > 16 || !(ms > 0))
+        return fail(CBF_ERR_INVALID_ARG, "chains must be 1, 2 or 4, blocksPerSm in [1, 16], ms > 0");
+    cudaError_t e = probe_fp64_step(chains, tracking != 0, blocksPerSm, ms, fp64InstrPerSec);
+    if (e != cudaSuccess) return cuda_fail(e, "FP64 step probe");
     return CBF_OK;
 }
 

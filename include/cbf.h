@@ -529,6 +529,14 @@ cbf_status cbf_grid_coordinates(const cbf_job* job, double* out_host);
 cbf_status cbf_lle_seeds(const cbf_job* job, double* out_host);
 /* FP64 FMA throughput of this GPU (TFLOP/s, 2 flops per FMA) over ~`ms` ms. */
 cbf_status cbf_probe_fp64_peak(double ms, double* tflops);
+/* The rate at which the map kernels' instruction stream issues FP64 instructions
+ * with nothing else around it: `chains` (1, 2 or 4) independent copies per thread
+ * of the rescaled 8-instruction Chen step, with the divergence tracking when
+ * `tracking` != 0, blocksPerSm blocks of 128 threads per SM, about `ms` ms.
+ * *fp64InstrPerSec = FP64 lane instructions per second (divide by SMs x 64 x
+ * clock for the pipe fraction).  No counterpart in the reference. */
+cbf_status cbf_probe_fp64_step(int32_t chains, int32_t tracking, int32_t blocksPerSm, double ms,
+                               double* fp64InstrPerSec);
 /* Exhaustive device check that expf(x) == 0 for every float x <= threshold;
  * *count receives the number of floats that violate it. */
 cbf_status cbf_probe_expf_zero(float threshold, uint64_t* count);
