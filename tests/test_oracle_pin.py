@@ -209,3 +209,38 @@ def test_lyapunov_spectrum_oracle_is_physical(orc):
     # seeds: unit rows
     z = orc.ls_seeds(job, [0, 5, 12345])
     assert np.allclose(np.linalg.norm(z, axis=2), 1.0, atol=1e-15)
+
+
+@pytest.mark.parametrize("system", ["chen", "lorenz"])
+@pytest.mark.parametrize("s", [0.5, 0.3])
+def test_rescaled_step_is_the_cd_step(orc, system, s):
+    """The rescaled Chen/Lorenz step (state (x, sy*y, sz*z)) is the same CD step
+    as the 14-instruction form: from the same physical states, ten steps of each
+    agree to rounding error in physical units.  The GPU tests compare the kernels
+    with the oracle form by form; this pins the algebra of the rescaled form
+    itself.  sy = r1 A h cy, sz = (1 - kB) sy / k as the library defines them."""
+    L = orc.lib()
+    sid = orc.SYSTEMS[system]
+    h = 0.002 if system == "chen" else 0.005
+    rng = np.random.default_rng(11)
+    lorenz = system == "lorenz"
+    for _ in range(20):
+        if lorenz:
+            v = np.array([s, rng.uniform(5, 20), rng.uniform(20, 200), 8.0 / 3.0])
+            A, B, cy = v[1], v[3], 1.0 - h * s
+        else:
+            v = np.array([s, rng.uniform(30, 45), 3.0, rng.uniform(20, 30)])
+            A, B, cy = v[1], v[2], 1.0 + h * s * v[3]
+        k, h1 = h * s, h * (1.0 - s)
+        r1 = 1.0 / (1.0 + h1 * A)
+        sy = (r1 * A) * h * cy
+        sz = ((1.0 - k * B) * sy) / k
+        x = rng.uniform(-20, 20, 3)
+        a = x.copy()
+        b = np.array([x[0], x[1] * sy, x[2] * sz])
+        vv = np.ascontiguousarray(v)
+        for _ in range(10):
+            L.orc_model_step(sid, a, vv, h)
+            L.orc_model_step(sid | 0x100, b, vv, h)
+        phys = np.array([b[0], b[1] / sy, b[2] / sz])
+        assert np.allclose(phys, a, rtol=1e-13, atol=1e-13), (system, s, v, a, phys)
