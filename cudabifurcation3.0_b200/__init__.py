@@ -47,7 +47,8 @@ EXPORTS = [
     "cbf_batch_run_sequential", "cbf_batch_check", "cbf_batch_autotune", "cbf_bifurcation2d_dbscan_noalloc",
     "cbf_csv_write_map", "cbf_csv_write_peaks", "cbf_csv_write_pairs",
     "cbf_mlp_num_params", "cbf_mlp_create", "cbf_mlp_destroy", "cbf_mlp_get_params",
-    "cbf_mlp_set_params", "cbf_mlp_set_encoding_scale", "cbf_mlp_forward_backward", "cbf_mlp_train",
+    "cbf_mlp_set_params", "cbf_mlp_set_encoding_scale", "cbf_mlp_encoding_frequencies",
+    "cbf_mlp_forward_backward", "cbf_mlp_train",
     "cbf_mlp_predict",
     "cbf_mlp_predict_grid", "cbf_mlp_grid_features",
     "cbf_surrogate_config_init", "cbf_lle_map_surrogate", "cbf_surrogate_release", "cbf_ls1d", "cbf_ls2d",
@@ -265,6 +266,8 @@ def lib():
             getattr(L, f).argtypes = [C.c_void_p, _fp, C.c_int64]
             getattr(L, f).restype = C.c_int32
         L.cbf_mlp_set_encoding_scale.argtypes = [C.c_void_p, C.c_float]
+        L.cbf_mlp_encoding_frequencies.argtypes = [_fp, C.c_int32]
+        L.cbf_mlp_encoding_frequencies.restype = C.c_int32
         L.cbf_mlp_set_encoding_scale.restype = C.c_int32
         L.cbf_mlp_forward_backward.argtypes = [C.c_void_p, _fp, _fp, _ip, C.c_int32, C.c_float, _fp,
                                                _fp, _fp]

@@ -793,6 +793,19 @@ cbf_status cbf_mlp_set_params(cbf_mlp* m, const float* host, int64_t n)
     return upload_params(m, host);
 }
 
+// The encoding's frequency table (kFreq x 2 floats, row-major), as the kernels
+// hold it in constant memory; n must be kFreq * 2.
+cbf_status cbf_mlp_encoding_frequencies(float* out, int32_t n)
+{
+    if (!out || n != kFreq * 2) return report_error(CBF_ERR_INVALID_ARG, "the table holds 124 floats");
+    constexpr FreqTable tab = make_freqs();
+    for (int k = 0; k < kFreq; ++k) {
+        out[2 * k] = tab.b[k][0];
+        out[2 * k + 1] = tab.b[k][1];
+    }
+    return CBF_OK;
+}
+
 // Frequency scale of the input encoding: a power of two in [2^-8, 16].
 cbf_status cbf_mlp_set_encoding_scale(cbf_mlp* m, float scale)
 {

@@ -215,6 +215,9 @@ cbf_status cbf_mlp_set_params(cbf_mlp* mlp, const float* host, int64_t n);
  * below what its labels resolve: the surrogate map sets (coarseSide / 512) rounded
  * to a power of two. */
 cbf_status cbf_mlp_set_encoding_scale(cbf_mlp* mlp, float scale);
+/* The encoding's 62 frequencies (b_k0, b_k1 for k = 0..61, cycles per unit of the
+ * [-1, 1] axes) into out[0..124); n must be 124.  Host-only, needs no GPU. */
+cbf_status cbf_mlp_encoding_frequencies(float* out, int32_t n);
 /* One forward and backward pass on n <= batch host rows (features x[n*4], LLE
  * targets, classes) with loss = wLle*MSE(out0) + CE(out1..16), both batch means;
  * returns loss, the flat gradient and the raw outputs (each optional). */

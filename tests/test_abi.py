@@ -337,3 +337,17 @@ def test_bench_step_cost_tables():
     assert r["unfused_cd_flops_per_step"] == 28
     assert r["unfused_cd_achieved"] == pytest.approx(1000 * 2000 * 28 / 1.0 / 1e12)
     assert b.unfused_cd("lorenz", 1, 1, 1.0, 1.0) == {}
+
+
+def test_encoding_frequencies_match_the_oracle(cbf):
+    """The network's Fourier-encoding table, built at compile time for the
+    kernels' constant memory, equals the oracle's table bit for bit (host call,
+    no GPU)."""
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1] / "oracle"))
+    import mlp_oracle as M
+    out = np.zeros(124, np.float32)
+    assert cbf.lib().cbf_mlp_encoding_frequencies(out.ctypes.data_as(C.POINTER(C.c_float)), 124) == 0
+    assert np.array_equal(out.reshape(62, 2), M.fourier_freqs())
+    assert cbf.lib().cbf_mlp_encoding_frequencies(out.ctypes.data_as(C.POINTER(C.c_float)), 10) != 0
